@@ -1,0 +1,46 @@
+"""The CPU oracle against the reference's own outputs (no GPU).
+
+* the notebook's recorded known answer (``CPU_GPU_Wigner2D.ipynb:557,577``);
+* golden fixtures produced by running the reference's own code
+  (``tests/golden/make_golden.py``).
+Tolerances: relative L2 1e-10 on the final state, observable columns to 1e-10
+of the column's scale (the parity bar for the complex128 path).
+"""
+import numpy as np
+import pytest
+
+from oracle.common import rel_l2
+from oracle.strang_notebook import StrangNotebook, KNOWN_MIN_W, KNOWN_NORM
+from oracle.wigner2d import WignerOracle
+from oracle.dirac2d import DiracOracle
+from golden_cases import WIGNER_NAMES, DIRAC_NAMES, wigner_case, dirac_case, obs_close
+
+TOL = 1e-10
+
+
+def test_notebook_known_answer():
+    s = StrangNotebook()
+    W = s.run(s.initial_state(), 500)
+    assert abs(np.min(W) - KNOWN_MIN_W) <= 1e-10 * abs(KNOWN_MIN_W)
+    assert abs(np.sum(W) * s.dX * s.dP - KNOWN_NORM) <= 1e-12
+
+
+@pytest.mark.parametrize('name', WIGNER_NAMES)
+def test_wigner_oracle_matches_reference(name):
+    g, prm, W0, steps = wigner_case(name)
+    assert np.allclose([W0.sum(), (W0 * W0).sum()], g['init_sum'], rtol=1e-14, atol=0)
+    o = WignerOracle(prm)
+    obs, W = o.run(W0, steps + 1)
+    assert obs_close(obs[:steps + 1, 1:], g['obs'], TOL) < TOL
+    assert rel_l2(W.real[::2, ::2], g['end_dec']) < TOL
+    Wr = W.real
+    assert np.allclose([Wr.sum(), (Wr * Wr).sum()], g['end_sums'], rtol=1e-10, atol=1e-14)
+
+
+@pytest.mark.parametrize('name', DIRAC_NAMES)
+def test_dirac_oracle_matches_reference(name):
+    g, prm, psi0, steps = dirac_case(name)
+    assert np.allclose([np.sum(np.abs(p) ** 2) for p in psi0], g['init_sum'], rtol=1e-14)
+    obs, P = DiracOracle(prm).run(psi0, steps)
+    assert obs_close(obs[:, :7], g['obs'], TOL) < TOL
+    assert rel_l2(P[:, ::2, ::2], g['end_dec']) < TOL
