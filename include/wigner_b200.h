@@ -1,0 +1,202 @@
+/*
+ * wigner_b200.h -- C ABI of the B200 (sm_100a) Wigner2D / Dirac2D
+ * split-operator propagators.
+ *
+ * The reference (cabrer7/PyWignerCUDA) drives its kernels from Python through
+ * PyCUDA and a ctypes binding of cuFFT (cufft_wrapper.py:78-145).  This library
+ * is the native layer under the Python drop-in classes
+ * (pywignercuda_b200.GPU_Wigner2D_FFT / GPU_Wigner2D_ODM2 / GPU_Dirac2D): one
+ * handle per propagator instance; expression strings are JIT-compiled by NVRTC
+ * into the fused kernels the way the reference's SourceModule pastes them into
+ * its kernel sources.
+ *
+ * Conventions
+ *   - Plain C types only; device buffers are raw pointers owned by the caller
+ *     (16-byte aligned, contiguous); scratch and tables are owned by the handle.
+ *   - Every call returns an int status (WIG_OK or WIG_ERR_*); wig_last_error()
+ *     gives the message of the calling thread's last failure.  No exception
+ *     crosses the ABI.  (Replaces cufftCheckStatus, cufft_wrapper.py:67-75.)
+ *   - One handle per stream; no internal host threads.
+ *   - Grids: powers of two, Wigner n_x, n_p in [16, 4096], Dirac n_x, n_y in
+ *     [16, 2048] (one fused pass holds a full line of the grid -- four spinor
+ *     components for Dirac -- in shared memory).
+ *   - Layout: (rows, cols) = (n_p, n_x) for Wigner, (n_y, n_x) per spinor
+ *     component for Dirac, row-major, FFT-shifted (index 0 holds coordinate 0),
+ *     complex128 interleaved -- the reference's layout
+ *     (GPU_Wigner2D_FFT.py:577-581, GPU_Dirac2D.py:331-332).
+ */
+#ifndef WIGNER_B200_H
+#define WIGNER_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WIG_ABI_VERSION 1
+
+enum wig_status {
+  WIG_OK = 0,
+  WIG_ERR_ARG = 1,         /* invalid descriptor / size / pointer            */
+  WIG_ERR_NVRTC = 2,       /* expression strings failed to compile           */
+  WIG_ERR_CUDA = 3,        /* CUDA runtime / driver error                    */
+  WIG_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up             */
+  WIG_ERR_NONFINITE = 5,   /* a recorded observable or norm became NaN / Inf */
+  WIG_ERR_UNSUPPORTED = 6, /* valid request this build does not implement    */
+  WIG_ERR_NOMEM = 7        /* device allocation failed                       */
+};
+
+enum wig_damping {
+  WIG_DAMP_NONE = 0,
+  WIG_DAMP_CALDEIRA_LEGGETT = 1, /* dampingFunction = 'CaldeiraLeggett' */
+  WIG_DAMP_ODM = 2               /* dampingFunction = 'ODM'             */
+};
+
+enum wig_constants {
+  WIG_CONST_CUDA_F = 0, /* kernel constants rounded by '%f' as the reference does */
+  WIG_CONST_EXACT = 1   /* full double precision                                 */
+};
+
+enum wig_precision { WIG_PREC_C128 = 0 };
+
+/* wig_run / dirac_run flags */
+#define WIG_RUN_CONTINUE 1u /* W continues an earlier call: skip the entry normalisation */
+#define WIG_RUN_PROFILE 2u  /* time every x-pass / p-pass launch with CUDA events (wig_profile) */
+
+#define WIG_NOBS 11   /* norm, <x>, <x^2>, <p>, <p^2>, <xp>, <V'>, <pV'>, <xV'>, <H>, negative area */
+#define DIRAC_NOBS 10 /* <x>, <y>, <alpha1>, <alpha2>, <beta>, <K>, <A0>, <px>, <py>, norm_kept */
+
+typedef struct wig_handle wig_handle;
+typedef struct dirac_handle dirac_handle;
+
+/* Wigner2D instance description: the constructor arguments of
+ * GPU_Wigner2D_FFT / GPU_Wigner2D_ODM2 (GPU_Wigner2D_FFT.py:1718-1720,1981-1984)
+ * plus the attributes an instance sets before construction. */
+typedef struct wig_desc {
+  int32_t abi_version;         /* WIG_ABI_VERSION                                   */
+  int32_t n_x, n_p;            /* X_gridDIM, P_gridDIM                              */
+  int32_t damping;             /* wig_damping; used only when gamma != 0 (Run :1901) */
+  int32_t kinetic_from_string; /* 0: p*lambda/mass phase (GPU_Wigner2D_FFT.Run)
+                                  1: kinetic string phase (GPU_Wigner2D_ODM2.Run)    */
+  int32_t constants;           /* wig_constants                                     */
+  int32_t precision;           /* wig_precision                                     */
+  int32_t n_lindblad;          /* ODM: 1 (GPU_Wigner2D_FFT) or 2 (GPU_Wigner2D_ODM2)  */
+  double x_amplitude, p_amplitude;
+  double hbar, mass, dt;
+  double d_theta, d_lambda, gamma;
+  double epsilon, l_material;  /* ODM (SetA_ODM :1206)                              */
+  double weight1, weight2;     /* ODM2 Lindblad weights (:2169-2176)                 */
+  const char* potential;       /* potentialString, C expression in (t, x)           */
+  const char* kinetic;         /* kinematicString, C expression in p                */
+  const char* fp_damping;      /* fp_Damping_String, C expression in p              */
+  /* Exact host tables of the observables (Run :1785-1792, :1747); NULL -> built
+   * by the library (shifted linspace grids; zeros for dV / V0). */
+  const double* x_table;       /* [n_x] */
+  const double* p_table;       /* [n_p] */
+  const double* theta_table;   /* [n_p] */
+  const double* lambda_table;  /* [n_x] */
+  const double* dv_table;      /* [n_x] dPotential(0, x) */
+  const double* v0_table;      /* [n_x] Potential(0, x)  */
+} wig_desc;
+
+/* Replaces GPU_Wigner2D_FFT.__init__ (:1718-1751): SetPhaseSpaceBox2D,
+ * SetCUDA_Constants (:833-842), SetFFT_Plans (:859-865), SetCUDA_Functions
+ * (:869-906, NVRTC instead of SourceModule). */
+int wig_create(const wig_desc* desc, wig_handle** out);
+
+/* The hot loop of GPU_Wigner2D_FFT.Run / GPU_Wigner2D_ODM2.Run (:1843-1914):
+ * normalises W (as Run does on entry, :1779-1780), then performs n_prop
+ * propagations starting at time index t_index0 (t = t_index * dt), in place on
+ * the device array W ((n_p, n_x) complex128).  flags & WIG_RUN_CONTINUE: W is
+ * the state an earlier call returned; no entry normalisation.  obs_host (may be NULL) receives
+ * (n_prop + 1) x WIG_NOBS doubles: sample k is taken before propagation k, the
+ * last one after the final propagation.  Run(timeSteps) == n_prop = timeSteps+1
+ * keeping the first timeSteps+1 samples.  stream: a cudaStream_t (NULL = legacy
+ * default stream).  Returns after the stream is synchronised when obs_host is
+ * given, otherwise asynchronously. */
+int wig_run(wig_handle* h, void* W_dev, int64_t t_index0, int64_t n_prop, uint32_t flags,
+            double* obs_host, void* stream);
+
+/* wig_run on host buffers: W_in (host, complex128) is copied to the device,
+ * propagated, and copied back into W_out (host, may alias W_in); the run's
+ * device buffer is owned by the handle.  (Run's W_init upload :1778 and W_end
+ * download :1954.) Synchronous. */
+int wig_run_host(wig_handle* h, const void* W_in_host, void* W_out_host, int64_t t_index0,
+                 int64_t n_prop, uint32_t flags, double* obs_host, void* stream);
+
+/* wig_run over `count` independent instances (each with its own handle and W)
+ * stepped in lock-step on one stream: step k of every instance is launched
+ * before step k+1 of any.  obs_host may be NULL or hold per-instance pointers
+ * (NULL entries allowed).  The reference runs one instance per Run()
+ * (GPU_Wigner2D_FFT.py:1843); this batches that loop. */
+int wig_run_many(wig_handle* const* handles, void* const* W_dev, int64_t count, int64_t t_index0,
+                 int64_t n_prop, uint32_t flags, double* const* obs_host, void* stream);
+
+/* Per-kernel device time of the handle's last run made with WIG_RUN_PROFILE:
+ * ms_out[0] = summed x-pass milliseconds, ms_out[1] = summed p-pass
+ * milliseconds, *launches = launches of each.  Synchronises on the events.
+ * (No counterpart in the reference, which times whole runs with %time.) */
+int wig_profile(wig_handle* h, double* ms_out, int64_t* launches);
+
+/* Replaces the cufftDestroy calls at the end of Run (:1960-1962). */
+int wig_destroy(wig_handle* h);
+
+/* Dirac2D instance: GPU_Dirac2D(gridDIM, amplitude, dt, ...) and the attributes
+ * mass, c, hBar, Potential_{0..3}_String (GPU_Dirac2D.py:306,356-380). */
+typedef struct dirac_desc {
+  int32_t abi_version;
+  int32_t n_x, n_y;
+  int32_t constants;           /* wig_constants */
+  int32_t precision;           /* wig_precision */
+  int32_t reserved;
+  double x_amplitude, y_amplitude;
+  double mass, c, hbar, dt;
+  const char* a0;              /* Potential_0_String, C expression in (t, x, y) */
+  const char* a1;
+  const char* a2;
+  const char* a3;
+  const double* x_table;       /* [n_x] shifted X  (NULL -> built) */
+  const double* y_table;       /* [n_y] shifted Y  */
+  const double* px_table;      /* [n_x] shifted Px */
+  const double* py_table;      /* [n_y] shifted Py */
+} dirac_desc;
+
+/* Replaces GPU_Dirac2D.__init__ (GPU_Dirac2D.py:306-392). */
+int dirac_create(const dirac_desc* desc, dirac_handle** out);
+
+/* GPU_Dirac2D.Run's loop (:1040-1111): n_steps >= 1 propagations at
+ * t = (t_index0 + k) * dt, k = 1..n_steps, in place on the device spinor psi
+ * ((4, n_y, n_x) complex128), which holds the normalised final spinor on
+ * return (Normalize_X, :1103).  obs_host (may be NULL) receives
+ * n_steps x DIRAC_NOBS doubles, sample k taken before propagation k + 1, as
+ * Run records them. */
+int dirac_run(dirac_handle* h, void* psi_dev, int64_t t_index0, int64_t n_steps,
+              double* obs_host, void* stream);
+
+/* dirac_run on host buffers (Psi_init upload :1002-1005, Psi_end download :1119). */
+int dirac_run_host(dirac_handle* h, const void* psi_in_host, void* psi_out_host, int64_t t_index0,
+                   int64_t n_steps, double* obs_host, void* stream);
+
+int dirac_destroy(dirac_handle* h);
+
+/* Compile-only check of an instance's kernels: builds the JIT source the way
+ * wig_create / dirac_create do and compiles it with NVRTC for sm_100a without
+ * loading it (no GPU needed).  log (may be NULL) receives the NVRTC log with
+ * the ptxas register / spill report, or the error.  The compile step of the
+ * reference's SourceModule calls (GPU_Wigner2D_FFT.py:869-906,
+ * GPU_Dirac2D.py:369-388). */
+int wig_jit_check(const wig_desc* desc, char* log, int64_t log_cap);
+int dirac_jit_check(const dirac_desc* desc, char* log, int64_t log_cap);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* wig_last_error(void);
+
+/* WIG_ABI_VERSION of the loaded library. */
+int wig_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WIGNER_B200_H */

@@ -1,0 +1,916 @@
+// C ABI of the B200 Wigner2D / Dirac2D propagators (see include/wigner_b200.h).
+//
+// Host side: descriptor validation, the instance's kernel constants (the
+// reference's '%f' formatting, GPU_Wigner2D_FFT.py:833-842 /
+// GPU_Dirac2D.py:358-367), NVRTC compilation of the fused kernels with the
+// user's expression strings pasted in (the reference's SourceModule calls,
+// GPU_Wigner2D_FFT.py:869-906 / GPU_Dirac2D.py:369-388), per-instance tables,
+// and the launch sequence of the hot loop (GPU_Wigner2D_FFT.Run :1843-1914,
+// GPU_Dirac2D.Run :1055-1111).
+//
+// The library links the CUDA runtime statically and reaches the driver API
+// and NVRTC only at run time (cudaGetDriverEntryPointByVersion, dlopen), so it
+// loads on machines without a GPU driver.
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <nvrtc.h>
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/wigner_b200.h"
+#include "wig_dirac.cuh"
+#include "wig_device_src.inc"   // kJitWignerSource, kJitDiracSource (generated by build.py)
+
+namespace {
+
+// ------------------------------------------------------------------ errors
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[2048];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define WIG_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(e_ == cudaErrorMemoryAllocation ? WIG_ERR_NOMEM : WIG_ERR_CUDA,       \
+                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+// ------------------------------------------------------------------ driver API
+struct Driver {
+  PFN_cuModuleLoadData load = nullptr;
+  PFN_cuModuleGetFunction getf = nullptr;
+  PFN_cuLaunchKernel launch = nullptr;
+  PFN_cuFuncSetAttribute setattr = nullptr;
+  PFN_cuGetErrorString errstr = nullptr;
+  bool ok = false;
+};
+
+std::mutex g_mu;
+Driver g_drv;
+
+template <class F>
+bool entry(const char* name, F& fn) {
+  cudaDriverEntryPointQueryResult q;
+  void* p = nullptr;
+  if (cudaGetDriverEntryPointByVersion(name, &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !p)
+    return false;
+  fn = reinterpret_cast<F>(p);
+  return true;
+}
+
+int driver(Driver** out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_drv.ok) {
+    if (!(entry("cuModuleLoadData", g_drv.load) && entry("cuModuleGetFunction", g_drv.getf) &&
+          entry("cuLaunchKernel", g_drv.launch) && entry("cuFuncSetAttribute", g_drv.setattr) &&
+          entry("cuGetErrorString", g_drv.errstr)))
+      return fail(WIG_ERR_CUDA, "CUDA driver entry points unavailable (no GPU driver?)");
+    g_drv.ok = true;
+  }
+  *out = &g_drv;
+  return WIG_OK;
+}
+
+const char* cu_err(CUresult r) {
+  const char* s = nullptr;
+  if (g_drv.errstr) g_drv.errstr(r, &s);
+  return s ? s : "unknown CUDA driver error";
+}
+
+// ------------------------------------------------------------------ NVRTC
+struct Nvrtc {
+  decltype(&nvrtcCreateProgram) create = nullptr;
+  decltype(&nvrtcCompileProgram) compile = nullptr;
+  decltype(&nvrtcGetProgramLogSize) logsize = nullptr;
+  decltype(&nvrtcGetProgramLog) log = nullptr;
+  decltype(&nvrtcGetCUBINSize) cubinsize = nullptr;
+  decltype(&nvrtcGetCUBIN) cubin = nullptr;
+  decltype(&nvrtcDestroyProgram) destroy = nullptr;
+  bool ok = false;
+};
+Nvrtc g_nvrtc;
+
+int nvrtc(Nvrtc** out) {
+  // caller holds g_mu
+  if (!g_nvrtc.ok) {
+    const char* names[] = {"libnvrtc.so.12", "/usr/local/cuda/lib64/libnvrtc.so.12", "libnvrtc.so"};
+    void* h = nullptr;
+    for (const char* n : names)
+      if ((h = dlopen(n, RTLD_NOW | RTLD_LOCAL))) break;
+    if (!h) return fail(WIG_ERR_NVRTC, "cannot load libnvrtc.so.12: %s", dlerror());
+#define WIG_SYM(f, s)                                                                    \
+  g_nvrtc.f = reinterpret_cast<decltype(g_nvrtc.f)>(dlsym(h, s));                        \
+  if (!g_nvrtc.f) return fail(WIG_ERR_NVRTC, "libnvrtc: missing symbol %s", s);
+    WIG_SYM(create, "nvrtcCreateProgram")
+    WIG_SYM(compile, "nvrtcCompileProgram")
+    WIG_SYM(logsize, "nvrtcGetProgramLogSize")
+    WIG_SYM(log, "nvrtcGetProgramLog")
+    WIG_SYM(cubinsize, "nvrtcGetCUBINSize")
+    WIG_SYM(cubin, "nvrtcGetCUBIN")
+    WIG_SYM(destroy, "nvrtcDestroyProgram")
+#undef WIG_SYM
+    g_nvrtc.ok = true;
+  }
+  *out = &g_nvrtc;
+  return WIG_OK;
+}
+
+// Compiled modules, keyed by (device, source); kept for the process lifetime.
+std::map<std::string, CUmodule> g_modules;
+
+// NVRTC: source -> sm_100a CUBIN (no GPU needed).  Caller holds g_mu.
+int nvrtc_compile(const std::string& src, std::vector<char>* cubin, std::string* log, bool verbose) {
+  Nvrtc* nv;
+  if (int rc = nvrtc(&nv)) return rc;
+  nvrtcProgram prog;
+  if (nv->create(&prog, src.c_str(), "wig_jit.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
+    return fail(WIG_ERR_NVRTC, "nvrtcCreateProgram failed");
+  std::vector<const char*> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo"};
+  if (verbose) opts.push_back("--ptxas-options=-v");
+  nvrtcResult cr = nv->compile(prog, (int)opts.size(), opts.data());
+  size_t ls = 0;
+  nv->logsize(prog, &ls);
+  log->assign(ls, '\0');
+  if (ls) nv->log(prog, &(*log)[0]);
+  if (cr != NVRTC_SUCCESS) {
+    nv->destroy(&prog);
+    return fail(WIG_ERR_NVRTC, "expression strings failed to compile:\n%s", log->c_str());
+  }
+  size_t n = 0;
+  nv->cubinsize(prog, &n);
+  cubin->resize(n);
+  nv->cubin(prog, cubin->data());
+  nv->destroy(&prog);
+  return WIG_OK;
+}
+
+bool env_verbose() {
+  const char* v = getenv("WIG_JIT_VERBOSE");
+  return v && *v && *v != '0';
+}
+
+int get_module(const std::string& src, int device, CUmodule* mod) {
+  Driver* drv;
+  if (int rc = driver(&drv)) return rc;
+  std::lock_guard<std::mutex> lk(g_mu);
+  const std::string key = std::to_string(device) + "\n" + src;
+  auto it = g_modules.find(key);
+  if (it != g_modules.end()) { *mod = it->second; return WIG_OK; }
+  std::vector<char> cubin;
+  std::string log;
+  const bool verbose = env_verbose();
+  if (int rc = nvrtc_compile(src, &cubin, &log, verbose)) return rc;
+  if (verbose) fprintf(stderr, "[wigner_b200 jit]\n%s\n", log.c_str());
+  CUresult r = drv->load(mod, cubin.data());
+  if (r != CUDA_SUCCESS) return fail(WIG_ERR_CUDA, "cuModuleLoadData: %s", cu_err(r));
+  g_modules[key] = *mod;
+  return WIG_OK;
+}
+
+int copy_log(const std::string& log, char* out, int64_t cap) {
+  if (out && cap > 0) {
+    const size_t n = std::min((size_t)(cap - 1), log.size());
+    memcpy(out, log.data(), n);
+    out[n] = '\0';
+  }
+  return WIG_OK;
+}
+
+int get_fn(CUmodule mod, const char* name, CUfunction* f, int dyn_smem) {
+  CUresult r = g_drv.getf(f, mod, name);
+  if (r != CUDA_SUCCESS) return fail(WIG_ERR_CUDA, "cuModuleGetFunction(%s): %s", name, cu_err(r));
+  if (dyn_smem > 48 * 1024) {
+    r = g_drv.setattr(*f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, dyn_smem);
+    if (r != CUDA_SUCCESS) return fail(WIG_ERR_CUDA, "cuFuncSetAttribute(%s): %s", name, cu_err(r));
+  }
+  return WIG_OK;
+}
+
+int launch(CUfunction f, unsigned grid, unsigned block, unsigned smem, cudaStream_t st, void** args) {
+  CUresult r = g_drv.launch(f, grid, 1, 1, block, 1, 1, smem, (CUstream)st, args, nullptr);
+  if (r != CUDA_SUCCESS) return fail(WIG_ERR_CUDA, "cuLaunchKernel: %s", cu_err(r));
+  return WIG_OK;
+}
+
+// ------------------------------------------------------------------ helpers
+bool pow2_in_range(int n) { return n >= 16 && n <= 4096 && (n & (n - 1)) == 0; }
+int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+int round_warp(int v) { return ((v + 31) / 32) * 32; }
+
+// '%f' formatting of the reference (or exact), and the value the kernel sees.
+std::string fmt_const(double v, int mode) {
+  char b[64];
+  snprintf(b, sizeof(b), mode == WIG_CONST_EXACT ? "%.17g" : "%f", v);
+  return b;
+}
+double kval(double v, int mode) { return strtod(fmt_const(v, mode).c_str(), nullptr); }
+
+// numpy linspace(-a, a - 2a/n, n) put through fftshift (GPU_Wigner2D_FFT.py:568-581)
+std::vector<double> shifted_range(double amp, int n) {
+  const double d = 2. * amp / (double)n;
+  const double start = -amp, stop = amp - d;
+  const double step = (stop - start) / (double)(n - 1);
+  std::vector<double> y(n), out(n);
+  for (int i = 0; i < n; ++i) y[i] = (double)i * step + start;
+  y[n - 1] = stop;
+  for (int k = 0; k < n; ++k) out[k] = y[(k + n / 2) % n];
+  return out;
+}
+
+// tw[m] = exp(-2 pi i m / n), extended precision, exact zeros on the axes
+std::vector<double2> twiddles(int n) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  std::vector<double2> t(n);
+  for (int m = 0; m < n; ++m) {
+    const long double a = 2.0L * pi * (long double)m / (long double)n;
+    double c = (double)cosl(a), s = (double)(-sinl(a));
+    if (fabs(c) < 1e-18) c = 0.;
+    if (fabs(s) < 1e-18) s = 0.;
+    t[m] = make_double2(c, s);
+  }
+  return t;
+}
+
+std::string expr_or(const char* s, const char* dflt) {
+  if (!s) return dflt;
+  std::string e(s);
+  if (e.find_first_not_of(" \t\r\n") == std::string::npos) return dflt;
+  return e;
+}
+
+bool safe_expr(const std::string& e) {
+  // the expression is pasted between parentheses inside a function body: refuse
+  // text that could close it or start a preprocessor directive
+  int depth = 0;
+  for (char ch : e) {
+    if (ch == '(') ++depth;
+    else if (ch == ')') { if (--depth < 0) return false; }
+    else if (ch == ';' || ch == '{' || ch == '}' || ch == '#' || ch == '"' || ch == '\\') return false;
+  }
+  return depth == 0;
+}
+
+const char* kMathPrelude =
+    "#ifndef M_PI\n#define M_PI 3.14159265358979323846\n#endif\n"
+    "#ifndef M_E\n#define M_E 2.7182818284590452354\n#endif\n";
+
+template <class T>
+int dev_upload(T** dst, const T* src, size_t n) {
+  WIG_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));
+  if (src) WIG_CUDA(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return WIG_OK;
+}
+
+struct DevBuf {
+  std::vector<void*> ptrs;
+  template <class T> int alloc(T** p, size_t n, const T* src = nullptr) {
+    int rc = dev_upload(p, src, n);
+    if (rc == WIG_OK) ptrs.push_back((void*)*p);
+    return rc;
+  }
+  void free_all() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+};
+
+}  // namespace
+
+// ======================================================================== Wigner
+struct wig_handle {
+  int device = 0;
+  wig_desc d{};
+  wig::WigArgs a{};
+  CUfunction f_x = nullptr, f_p = nullptr, f_r = nullptr, f_fin = nullptr, f_scale = nullptr;
+  int xrows = 1, xnt = 256, pc = 1, pnt = 256, rnt = 256;
+  int n_cta_x = 1, n_cta_p = 1, n_cta_r = 1;
+  int smem_x = 0, smem_p = 0;
+  DevBuf bufs;
+  double* obs = nullptr;
+  size_t obs_cap = 0;
+  double2* scale = nullptr;
+  double2* W_host_stage = nullptr;   // device copy used by wig_run_host
+  std::vector<cudaEvent_t> ev;       // WIG_RUN_PROFILE: 3 events per step
+  size_t ev_used = 0;
+};
+
+// Validation, tiling and the JIT source of one Wigner instance (no CUDA calls).
+struct WigPlan {
+  int xrows, xnt, pc, pnt, rnt, n_cta_x, n_cta_p, n_cta_r, smem_x, smem_p, damp;
+  double dX, dP, dTheta, dLambda;
+  std::string src;
+};
+
+static int wig_plan(const wig_desc* d, WigPlan* P) {
+  if (!d) return fail(WIG_ERR_ARG, "wig: null descriptor");
+  if (d->abi_version != WIG_ABI_VERSION)
+    return fail(WIG_ERR_ARG, "wig: abi_version %d != %d", d->abi_version, WIG_ABI_VERSION);
+  if (!pow2_in_range(d->n_x) || !pow2_in_range(d->n_p))
+    return fail(WIG_ERR_ARG, "grid %d x %d: n_x and n_p must be powers of two in [16, 4096]", d->n_x,
+                d->n_p);
+  if (!(d->x_amplitude > 0) || !(d->p_amplitude > 0) || !(d->hbar != 0) || !(d->mass != 0) ||
+      !std::isfinite(d->dt))
+    return fail(WIG_ERR_ARG, "amplitudes must be > 0, hbar and mass nonzero, dt finite");
+  if (d->constants != WIG_CONST_CUDA_F && d->constants != WIG_CONST_EXACT)
+    return fail(WIG_ERR_ARG, "unknown constants mode %d", d->constants);
+  if (d->precision != WIG_PREC_C128) return fail(WIG_ERR_UNSUPPORTED, "precision %d not available", d->precision);
+  const bool damped = d->gamma != 0.;
+  if (damped && d->damping == WIG_DAMP_ODM)
+    return fail(WIG_ERR_UNSUPPORTED, "ODM Lindblad damping is not available in this build");
+  const std::string V = expr_or(d->potential, "0."), K = expr_or(d->kinetic, "0.5*p*p"),
+                    F = expr_or(d->fp_damping, "fabs(p)");
+  if (!safe_expr(V) || !safe_expr(K) || !safe_expr(F))
+    return fail(WIG_ERR_ARG, "expression strings may not contain ; { } # quotes or unbalanced ()");
+  const int NX = d->n_x, NP = d->n_p, cm = d->constants;
+  P->damp = (damped && d->damping == WIG_DAMP_CALDEIRA_LEGGETT) ? 1 : 0;
+
+  // ---- tiling
+  P->xrows = clampi(2048 / NX, 1, NP);
+  P->xnt = round_warp(clampi(P->xrows * NX / 8, 32, 256));
+  P->pc = clampi(2048 / NP, 1, NX);
+  P->pnt = round_warp(clampi(P->pc * NP / 8, 32, 256));
+  P->rnt = 256;
+  P->n_cta_x = NP / P->xrows;
+  P->n_cta_p = NX / P->pc;
+  P->n_cta_r = clampi(NX * NP / (4 * P->rnt), 1, 296);
+  P->smem_x = P->xrows * (NX + (NX >> 3)) * (int)sizeof(double2);
+  P->smem_p = (P->damp ? 2 : 1) * P->pc * NP * (int)sizeof(double2);
+
+  // ---- JIT source
+  P->dX = 2. * d->x_amplitude / (double)NX;
+  P->dP = 2. * d->p_amplitude / (double)NP;
+  P->dTheta = 2. * M_PI / (2. * d->p_amplitude);
+  P->dLambda = 2. * M_PI / (2. * d->x_amplitude);
+  struct { const char* name; double v; } consts[] = {
+      {"dt", d->dt}, {"dx", P->dX}, {"dp", P->dP}, {"dtheta", P->dTheta}, {"dlambda", P->dLambda},
+      {"mass", d->mass}, {"hBar", d->hbar}, {"D_Theta", d->d_theta}, {"D_Lambda", d->d_lambda}};
+  std::string src = kMathPrelude;
+  for (auto& c : consts) src += "__constant__ double " + std::string(c.name) + "=" + fmt_const(c.v, cm) + ";";
+  src += "\nstruct UserPhys {\n";
+  src += "  __device__ __forceinline__ double Potential(double t, double x) const { return (" + V + "); }\n";
+  src += "  __device__ __forceinline__ double KineticEnergy(double p) const { return (" + K + "); }\n";
+  src += "  __device__ __forceinline__ double f(double p) const { return (" + F + "); }\n};\n";
+  char macros[512];
+  snprintf(macros, sizeof(macros),
+           "#define WIG_NX %d\n#define WIG_NP %d\n#define WIG_XROWS %d\n#define WIG_XNT %d\n"
+           "#define WIG_XPAD 3\n#define WIG_KIN_STRING %d\n#define WIG_PC %d\n#define WIG_PNT %d\n"
+           "#define WIG_DAMP %d\n#define WIG_RNT %d\n",
+           NX, NP, P->xrows, P->xnt, d->kinetic_from_string ? 1 : 0, P->pc, P->pnt, P->damp, P->rnt);
+  src += macros;
+  src += kJitWignerSource;
+  P->src.swap(src);
+  return WIG_OK;
+}
+
+extern "C" int wig_jit_check(const wig_desc* d, char* log, int64_t log_cap) {
+  WigPlan P;
+  if (int rc = wig_plan(d, &P)) { copy_log(g_last_error, log, log_cap); return rc; }
+  std::lock_guard<std::mutex> lk(g_mu);
+  std::vector<char> cubin;
+  std::string lg;
+  int rc = nvrtc_compile(P.src, &cubin, &lg, true);
+  copy_log(rc ? g_last_error : lg, log, log_cap);
+  return rc;
+}
+
+extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
+  if (!out) return fail(WIG_ERR_ARG, "wig_create: null argument");
+  *out = nullptr;
+  WigPlan P;
+  if (int rc = wig_plan(d, &P)) return rc;
+  int device = 0;
+  WIG_CUDA(cudaGetDevice(&device));
+  WIG_CUDA(cudaFree(0));
+  wig_handle* h = new wig_handle();
+  h->d = *d;
+  h->device = device;
+  const int NX = d->n_x, NP = d->n_p, cm = d->constants;
+  h->xrows = P.xrows; h->xnt = P.xnt; h->pc = P.pc; h->pnt = P.pnt; h->rnt = P.rnt;
+  h->n_cta_x = P.n_cta_x; h->n_cta_p = P.n_cta_p; h->n_cta_r = P.n_cta_r;
+  h->smem_x = P.smem_x; h->smem_p = P.smem_p;
+  const double dX = P.dX, dP = P.dP, dTheta = P.dTheta, dLambda = P.dLambda;
+  const std::string& src = P.src;
+  CUmodule mod;
+  int rc = get_module(src, h->device, &mod);
+  if (!rc) rc = get_fn(mod, "wig_xpass", &h->f_x, h->smem_x);
+  if (!rc) rc = get_fn(mod, "wig_ppass", &h->f_p, h->smem_p);
+  if (!rc) rc = get_fn(mod, "wig_reduce", &h->f_r, 0);
+  if (!rc) rc = get_fn(mod, "wig_finalize", &h->f_fin, 0);
+  if (!rc) rc = get_fn(mod, "wig_scale", &h->f_scale, 0);
+  CUfunction f_setup = nullptr;
+  if (!rc) rc = get_fn(mod, "wig_setup", &f_setup, 0);
+  if (rc) { delete h; return rc; }
+
+  // ---- kernel arguments and tables
+  wig::WigArgs& a = h->a;
+  a.dt = kval(d->dt, cm); a.dx = kval(dX, cm); a.dp = kval(dP, cm);
+  a.dtheta = kval(dTheta, cm); a.dlambda = kval(dLambda, cm); a.mass = kval(d->mass, cm);
+  a.hbar = kval(d->hbar, cm); a.D_theta = kval(d->d_theta, cm); a.D_lambda = kval(d->d_lambda, cm);
+  a.dX = dX; a.dP = dP; a.mass_exact = d->mass;
+  {
+    // CaldeiraDissipatorOrder3 (:1145-1157) coefficients c1 = 2/3 i dt gamma,
+    // c2 = i dt gamma, c3 = 2 i dt gamma; Horner: k1 = c1 c2/(c1 + c2), k12 = c1 + c2
+    const double g = d->dt * d->gamma;
+    const double c1 = 2. / 3. * g, c2 = 2. / 2. * g, c3 = 2. * g;   // imaginary parts
+    // c1 c2 / (c1 + c2) with c1 = i u, c2 = i v:  (i u)(i v)/(i (u+v)) = i u v/(u+v)
+    const double k1 = (c1 + c2) != 0. ? c1 * c2 / (c1 + c2) : 0.;
+    a.cl_k1 = make_double2(0., k1);
+    a.cl_k12 = make_double2(0., c1 + c2);
+    a.cl_c3 = make_double2(0., c3);
+  }
+  std::vector<double> xt = d->x_table ? std::vector<double>(d->x_table, d->x_table + NX) : shifted_range(d->x_amplitude, NX);
+  std::vector<double> pt = d->p_table ? std::vector<double>(d->p_table, d->p_table + NP) : shifted_range(d->p_amplitude, NP);
+  std::vector<double> tht = d->theta_table ? std::vector<double>(d->theta_table, d->theta_table + NP)
+                                           : shifted_range(dTheta * NP / 2., NP);
+  std::vector<double> ths(NP);
+  for (int i = 0; i < NP; ++i) ths[i] = tht[i] * (1.0 / (double)NP);
+  std::vector<double> dv(NX, 0.), v0(NX, 0.);
+  if (d->dv_table) dv.assign(d->dv_table, d->dv_table + NX);
+  if (d->v0_table) v0.assign(d->v0_table, d->v0_table + NX);
+  std::vector<double2> twx = twiddles(NX), twp = twiddles(NP);
+  double *x_d, *p_d, *dv_d, *v0_d, *ths_d, *rl_d, *rt_d, *m1_d, *m2_d, *sfp_d, *part_d;
+  double2 *twx_d, *twp_d;
+  const int nparts = std::max(std::max(h->n_cta_x, h->n_cta_p), h->n_cta_r);
+  DevBuf& B = h->bufs;
+  rc = B.alloc(&x_d, NX, xt.data());
+  if (!rc) rc = B.alloc(&p_d, NP, pt.data());
+  if (!rc) rc = B.alloc(&dv_d, NX, dv.data());
+  if (!rc) rc = B.alloc(&v0_d, NX, v0.data());
+  if (!rc) rc = B.alloc(&ths_d, NP, ths.data());
+  if (!rc) rc = B.alloc(&rl_d, NX);
+  if (!rc) rc = B.alloc(&rt_d, NP);
+  if (!rc) rc = B.alloc(&m1_d, NX);
+  if (!rc) rc = B.alloc(&m2_d, NX);
+  if (!rc) rc = B.alloc(&sfp_d, NP);
+  if (!rc) rc = B.alloc(&twx_d, NX, twx.data());
+  if (!rc) rc = B.alloc(&twp_d, NP, twp.data());
+  if (!rc) rc = B.alloc(&part_d, (size_t)nparts * wig::NACC);
+  if (!rc) rc = B.alloc(&h->scale, 1);
+  if (rc) { B.free_all(); delete h; return rc; }
+  a.x_tab = x_d; a.p_tab = p_d; a.dV_tab = dv_d; a.V0_tab = v0_d; a.theta_s = ths_d;
+  a.r_lambda = rl_d; a.r_theta = rt_d; a.mask1 = m1_d; a.mask2s = m2_d; a.sfp = sfp_d;
+  a.tw_x = twx_d; a.tw_p = twp_d; a.partials = part_d; a.n_partials = 0;
+  {
+    void* args[] = {&rl_d, &rt_d, &m1_d, &m2_d, &sfp_d};
+    rc = launch(f_setup, 8, 256, 0, 0, args);
+    if (!rc) {
+      cudaError_t e = cudaDeviceSynchronize();
+      if (e != cudaSuccess) rc = fail(WIG_ERR_CUDA, "wig_setup: %s", cudaGetErrorString(e));
+    }
+    if (rc) { B.free_all(); delete h; return rc; }
+  }
+  *out = h;
+  return WIG_OK;
+}
+
+static int ensure_obs(double** buf, size_t* cap, size_t need) {
+  if (need <= *cap) return WIG_OK;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  WIG_CUDA(cudaMalloc((void**)buf, need * sizeof(double)));
+  *cap = need;
+  return WIG_OK;
+}
+
+static int check_finite(const double* v, size_t n, const char* what) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(v[i])) return fail(WIG_ERR_NONFINITE, "%s: non-finite value at index %zu", what, i);
+  return WIG_OK;
+}
+
+// ---- one run, split so that several instances can be stepped in lock-step
+struct WigRunState {
+  wig::WigArgs a;
+  double2* W;
+  int64_t t_index0, n_prop;
+  uint32_t flags;
+  bool damped;
+};
+
+static int wig_run_check(wig_handle* h, void* W_dev, int64_t n_prop) {
+  if (!h || !W_dev) return fail(WIG_ERR_ARG, "wig_run: null handle or W");
+  if (((uintptr_t)W_dev & 15) != 0) return fail(WIG_ERR_ARG, "wig_run: W must be 16-byte aligned");
+  if (n_prop < 0) return fail(WIG_ERR_ARG, "wig_run: n_prop < 0");
+  int cur;
+  WIG_CUDA(cudaGetDevice(&cur));
+  if (cur != h->device) return fail(WIG_ERR_ARG, "wig_run: current device %d != handle device %d", cur, h->device);
+  if (int rc = ensure_obs(&h->obs, &h->obs_cap, (size_t)(n_prop + 1) * WIG_NOBS)) return rc;
+  return WIG_OK;
+}
+
+static int wig_profile_prepare(wig_handle* h, int64_t n_prop) {
+  const size_t need = 3 * (size_t)n_prop;
+  while (h->ev.size() < need) {
+    cudaEvent_t e;
+    WIG_CUDA(cudaEventCreate(&e));
+    h->ev.push_back(e);
+  }
+  h->ev_used = need;
+  return WIG_OK;
+}
+
+static int wig_run_begin(wig_handle* h, WigRunState* S, void* W_dev, int64_t t_index0, int64_t n_prop,
+                         uint32_t flags, cudaStream_t st) {
+  S->a = h->a;
+  S->W = (double2*)W_dev;
+  S->t_index0 = t_index0;
+  S->n_prop = n_prop;
+  S->flags = flags;
+  S->damped = h->d.gamma != 0.;
+  if (flags & WIG_RUN_PROFILE) {
+    if (int rc = wig_profile_prepare(h, n_prop)) return rc;
+  } else {
+    h->ev_used = 0;
+  }
+  void* args[] = {&S->a, &S->W};
+  if (int rc = launch(h->f_r, h->n_cta_r, h->rnt, 0, st, args)) return rc;
+  S->a.n_partials = h->n_cta_r;
+  return WIG_OK;
+}
+
+static int wig_run_step(wig_handle* h, WigRunState* S, int64_t n, cudaStream_t st) {
+  const int first = (S->flags & WIG_RUN_CONTINUE) ? 0 : 1;
+  int mode = (n == 0) ? first : (S->damped ? 2 : 0);
+  double* obs_row = h->obs + (size_t)n * WIG_NOBS;
+  const bool prof = h->ev_used != 0;
+  if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n], st));
+  void* xargs[] = {&S->a, &S->W, &mode, &obs_row};
+  if (int rc = launch(h->f_x, h->n_cta_x, h->xnt, h->smem_x, st, xargs)) return rc;
+  if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 1], st));
+  double t = (double)(S->t_index0 + n) * h->d.dt;
+  void* pargs[] = {&S->a, &S->W, &t};
+  if (int rc = launch(h->f_p, h->n_cta_p, h->pnt, h->smem_p, st, pargs)) return rc;
+  if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 2], st));
+  S->a.n_partials = h->n_cta_p;
+  return WIG_OK;
+}
+
+static int wig_run_end(wig_handle* h, WigRunState* S, cudaStream_t st) {
+  int fmode = (S->n_prop == 0) ? ((S->flags & WIG_RUN_CONTINUE) ? 0 : 1) : (S->damped ? 2 : 0);
+  double* last_row = h->obs + (size_t)S->n_prop * WIG_NOBS;
+  void* args[] = {&S->a, &fmode, &last_row, &h->scale};
+  if (int rc = launch(h->f_fin, 1, h->rnt, 0, st, args)) return rc;
+  if (fmode != 0) {
+    long n = (long)h->d.n_x * h->d.n_p;
+    void* sargs[] = {&S->W, &n, &h->scale};
+    if (int rc = launch(h->f_scale, clampi((int)(n / (4 * h->rnt)), 1, 592), h->rnt, 0, st, sargs)) return rc;
+  }
+  return WIG_OK;
+}
+
+static int wig_copy_obs(wig_handle* h, int64_t n_prop, double* obs_host, cudaStream_t st) {
+  const size_t nobs = (size_t)(n_prop + 1) * WIG_NOBS;
+  WIG_CUDA(cudaMemcpyAsync(obs_host, h->obs, nobs * sizeof(double), cudaMemcpyDeviceToHost, st));
+  return WIG_OK;
+}
+
+extern "C" int wig_run(wig_handle* h, void* W_dev, int64_t t_index0, int64_t n_prop, uint32_t flags,
+                       double* obs_host, void* stream) {
+  if (int rc = wig_run_check(h, W_dev, n_prop)) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  WigRunState S;
+  if (int rc = wig_run_begin(h, &S, W_dev, t_index0, n_prop, flags, st)) return rc;
+  for (int64_t n = 0; n < n_prop; ++n)
+    if (int rc = wig_run_step(h, &S, n, st)) return rc;
+  if (int rc = wig_run_end(h, &S, st)) return rc;
+  if (obs_host) {
+    if (int rc = wig_copy_obs(h, n_prop, obs_host, st)) return rc;
+    WIG_CUDA(cudaStreamSynchronize(st));
+    return check_finite(obs_host, (size_t)(n_prop + 1) * WIG_NOBS, "wig_run observables");
+  }
+  return WIG_OK;
+}
+
+extern "C" int wig_run_many(wig_handle* const* hs, void* const* Ws, int64_t count, int64_t t_index0,
+                            int64_t n_prop, uint32_t flags, double* const* obs_host, void* stream) {
+  if (!hs || !Ws || count < 1) return fail(WIG_ERR_ARG, "wig_run_many: empty batch");
+  for (int64_t i = 0; i < count; ++i) {
+    if (int rc = wig_run_check(hs[i], Ws[i], n_prop)) return rc;
+    for (int64_t j = 0; j < i; ++j)
+      if (hs[j] == hs[i]) return fail(WIG_ERR_ARG, "wig_run_many: a handle appears twice");
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<WigRunState> S((size_t)count);
+  for (int64_t i = 0; i < count; ++i)
+    if (int rc = wig_run_begin(hs[i], &S[i], Ws[i], t_index0, n_prop, flags, st)) return rc;
+  for (int64_t n = 0; n < n_prop; ++n)
+    for (int64_t i = 0; i < count; ++i)
+      if (int rc = wig_run_step(hs[i], &S[i], n, st)) return rc;
+  for (int64_t i = 0; i < count; ++i)
+    if (int rc = wig_run_end(hs[i], &S[i], st)) return rc;
+  if (obs_host) {
+    for (int64_t i = 0; i < count; ++i)
+      if (obs_host[i])
+        if (int rc = wig_copy_obs(hs[i], n_prop, obs_host[i], st)) return rc;
+    WIG_CUDA(cudaStreamSynchronize(st));
+    for (int64_t i = 0; i < count; ++i)
+      if (obs_host[i])
+        if (int rc = check_finite(obs_host[i], (size_t)(n_prop + 1) * WIG_NOBS, "wig_run_many observables"))
+          return rc;
+  }
+  return WIG_OK;
+}
+
+extern "C" int wig_profile(wig_handle* h, double* ms_out, int64_t* launches) {
+  if (!h || !ms_out) return fail(WIG_ERR_ARG, "wig_profile: null argument");
+  ms_out[0] = ms_out[1] = 0.;
+  const size_t steps = h->ev_used / 3;
+  for (size_t n = 0; n < steps; ++n) {
+    float a = 0.f, b = 0.f;
+    WIG_CUDA(cudaEventSynchronize(h->ev[3 * n + 2]));
+    WIG_CUDA(cudaEventElapsedTime(&a, h->ev[3 * n], h->ev[3 * n + 1]));
+    WIG_CUDA(cudaEventElapsedTime(&b, h->ev[3 * n + 1], h->ev[3 * n + 2]));
+    ms_out[0] += a;
+    ms_out[1] += b;
+  }
+  if (launches) *launches = (int64_t)steps;
+  return WIG_OK;
+}
+
+extern "C" int wig_run_host(wig_handle* h, const void* W_in, void* W_out, int64_t t_index0, int64_t n_prop,
+                            uint32_t flags, double* obs_host, void* stream) {
+  if (!h || !W_in || !W_out) return fail(WIG_ERR_ARG, "wig_run_host: null argument");
+  const size_t bytes = (size_t)h->d.n_x * h->d.n_p * sizeof(double2);
+  if (!h->W_host_stage) {
+    void* p = nullptr;
+    WIG_CUDA(cudaMalloc(&p, bytes));
+    h->W_host_stage = (double2*)p;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  WIG_CUDA(cudaMemcpyAsync(h->W_host_stage, W_in, bytes, cudaMemcpyHostToDevice, st));
+  int rc = wig_run(h, h->W_host_stage, t_index0, n_prop, flags, nullptr, stream);
+  if (rc) return rc;
+  WIG_CUDA(cudaMemcpyAsync(W_out, h->W_host_stage, bytes, cudaMemcpyDeviceToHost, st));
+  const size_t nobs = (size_t)(n_prop + 1) * WIG_NOBS;
+  if (obs_host) WIG_CUDA(cudaMemcpyAsync(obs_host, h->obs, nobs * sizeof(double), cudaMemcpyDeviceToHost, st));
+  WIG_CUDA(cudaStreamSynchronize(st));
+  if (obs_host) return check_finite(obs_host, nobs, "wig_run_host observables");
+  return WIG_OK;
+}
+
+extern "C" int wig_destroy(wig_handle* h) {
+  if (!h) return WIG_OK;
+  cudaDeviceSynchronize();
+  for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  h->bufs.free_all();
+  if (h->obs) cudaFree(h->obs);
+  if (h->W_host_stage) cudaFree(h->W_host_stage);
+  delete h;
+  return WIG_OK;
+}
+
+// ======================================================================== Dirac
+struct dirac_handle {
+  int device = 0;
+  dirac_desc d{};
+  wig::DiracArgs a{};
+  CUfunction f_row = nullptr, f_col = nullptr, f_fin = nullptr, f_scale = nullptr;
+  int rows = 1, rnt = 256, cc = 1, cnt = 256, snt = 256;
+  int n_row = 1, n_col = 1, smem_row = 0, smem_col = 0;
+  DevBuf bufs;
+  double* obs = nullptr;
+  size_t obs_cap = 0;
+  double2* scale = nullptr;
+  double2* psi_host_stage = nullptr;
+};
+
+struct DiracPlan {
+  int rows, rnt, cc, cnt, snt, n_row, n_col, smem_row, smem_col;
+  double dX, dY, Pxa, Pya, dPx, dPy;
+  std::string src;
+};
+
+static int dirac_plan(const dirac_desc* d, DiracPlan* P) {
+  if (!d) return fail(WIG_ERR_ARG, "dirac: null descriptor");
+  if (d->abi_version != WIG_ABI_VERSION)
+    return fail(WIG_ERR_ARG, "dirac: abi_version %d != %d", d->abi_version, WIG_ABI_VERSION);
+  if (!pow2_in_range(d->n_x) || !pow2_in_range(d->n_y) || d->n_x > 2048 || d->n_y > 2048)
+    return fail(WIG_ERR_ARG, "grid %d x %d: n_x and n_y must be powers of two in [16, 2048]", d->n_x, d->n_y);
+  if (!(d->x_amplitude > 0) || !(d->y_amplitude > 0) || !std::isfinite(d->dt) || !std::isfinite(d->c))
+    return fail(WIG_ERR_ARG, "amplitudes must be > 0, dt and c finite");
+  if (d->constants != WIG_CONST_CUDA_F && d->constants != WIG_CONST_EXACT)
+    return fail(WIG_ERR_ARG, "unknown constants mode %d", d->constants);
+  if (d->precision != WIG_PREC_C128) return fail(WIG_ERR_UNSUPPORTED, "precision %d not available", d->precision);
+  const std::string A0 = expr_or(d->a0, "0."), A1 = expr_or(d->a1, "0."), A2 = expr_or(d->a2, "0."),
+                    A3 = expr_or(d->a3, "0.");
+  if (!safe_expr(A0) || !safe_expr(A1) || !safe_expr(A2) || !safe_expr(A3))
+    return fail(WIG_ERR_ARG, "expression strings may not contain ; { } # quotes or unbalanced ()");
+  const int NX = d->n_x, NY = d->n_y, cm = d->constants;
+  P->rows = clampi(512 / NX, 1, NY);
+  P->rnt = round_warp(clampi(4 * P->rows * NX / 8, 32, 256));
+  P->cc = clampi(1024 / NY, 1, NX);
+  P->cnt = round_warp(clampi(4 * P->cc * NY / 8, 32, 256));
+  P->snt = 256;
+  P->n_row = NY / P->rows;
+  P->n_col = NX / P->cc;
+  P->smem_row = 4 * P->rows * (NX + (NX >> 3)) * (int)sizeof(double2);
+  P->smem_col = 4 * P->cc * NY * (int)sizeof(double2);
+  // GPU_Dirac2D.py:312-346
+  P->dX = 2. * d->x_amplitude / (double)NX;
+  P->dY = 2. * d->y_amplitude / (double)NY;
+  P->Pxa = M_PI / P->dX;
+  P->Pya = M_PI / P->dY;
+  P->dPx = 2 * P->Pxa / NX;
+  P->dPy = 2 * P->Pya / NY;
+  struct { const char* name; double v; } consts[] = {{"mass", d->mass}, {"c", d->c}, {"dt", d->dt},
+                                                      {"dX", P->dX},    {"dY", P->dY}, {"dPx", P->dPx},
+                                                      {"dPy", P->dPy}};
+  std::string src = kMathPrelude;
+  for (auto& c : consts) src += "__constant__ double " + std::string(c.name) + "=" + fmt_const(c.v, cm) + ";";
+  src += "\nstruct UserPhys {\n";
+  const std::string* As[4] = {&A0, &A1, &A2, &A3};
+  for (int i = 0; i < 4; ++i)
+    src += "  __device__ __forceinline__ double A" + std::to_string(i) +
+           "(double t, double x, double y) const { return (" + *As[i] + "); }\n";
+  src += "};\n";
+  char macros[512];
+  snprintf(macros, sizeof(macros),
+           "#define DIR_NX %d\n#define DIR_NY %d\n#define DIR_ROWS %d\n#define DIR_RNT %d\n"
+           "#define DIR_PAD 3\n#define DIR_C %d\n#define DIR_CNT %d\n#define DIR_SNT %d\n",
+           NX, NY, P->rows, P->rnt, P->cc, P->cnt, P->snt);
+  src += macros;
+  src += kJitDiracSource;
+  P->src.swap(src);
+  return WIG_OK;
+}
+
+extern "C" int dirac_jit_check(const dirac_desc* d, char* log, int64_t log_cap) {
+  DiracPlan P;
+  if (int rc = dirac_plan(d, &P)) { copy_log(g_last_error, log, log_cap); return rc; }
+  std::lock_guard<std::mutex> lk(g_mu);
+  std::vector<char> cubin;
+  std::string lg;
+  int rc = nvrtc_compile(P.src, &cubin, &lg, true);
+  copy_log(rc ? g_last_error : lg, log, log_cap);
+  return rc;
+}
+
+extern "C" int dirac_create(const dirac_desc* d, dirac_handle** out) {
+  if (!out) return fail(WIG_ERR_ARG, "dirac_create: null argument");
+  *out = nullptr;
+  DiracPlan P;
+  if (int rc = dirac_plan(d, &P)) return rc;
+  int device = 0;
+  WIG_CUDA(cudaGetDevice(&device));
+  WIG_CUDA(cudaFree(0));
+  dirac_handle* h = new dirac_handle();
+  h->d = *d;
+  h->device = device;
+  const int NX = d->n_x, NY = d->n_y, cm = d->constants;
+  h->rows = P.rows; h->rnt = P.rnt; h->cc = P.cc; h->cnt = P.cnt; h->snt = P.snt;
+  h->n_row = P.n_row; h->n_col = P.n_col; h->smem_row = P.smem_row; h->smem_col = P.smem_col;
+  const double dX = P.dX, dY = P.dY, Pxa = P.Pxa, Pya = P.Pya, dPx = P.dPx, dPy = P.dPy;
+  const std::string& src = P.src;
+  CUmodule mod;
+  int rc = get_module(src, h->device, &mod);
+  if (!rc) rc = get_fn(mod, "dirac_rowpass", &h->f_row, h->smem_row);
+  if (!rc) rc = get_fn(mod, "dirac_colpass", &h->f_col, h->smem_col);
+  if (!rc) rc = get_fn(mod, "dirac_final", &h->f_fin, 0);
+  if (!rc) rc = get_fn(mod, "dirac_scale", &h->f_scale, 0);
+  CUfunction f_setup = nullptr;
+  if (!rc) rc = get_fn(mod, "dirac_setup", &f_setup, 0);
+  if (rc) { delete h; return rc; }
+
+  wig::DiracArgs& a = h->a;
+  a.mass = kval(d->mass, cm); a.c = kval(d->c, cm); a.dt = kval(d->dt, cm);
+  a.dX = kval(dX, cm); a.dY = kval(dY, cm); a.dPx = kval(dPx, cm); a.dPy = kval(dPy, cm);
+  a.dX_e = dX; a.dY_e = dY; a.dPx_e = dPx; a.dPy_e = dPy; a.mass_e = d->mass; a.c_e = d->c;
+  std::vector<double> xt = d->x_table ? std::vector<double>(d->x_table, d->x_table + NX) : shifted_range(d->x_amplitude, NX);
+  std::vector<double> yt = d->y_table ? std::vector<double>(d->y_table, d->y_table + NY) : shifted_range(d->y_amplitude, NY);
+  std::vector<double> pxt = d->px_table ? std::vector<double>(d->px_table, d->px_table + NX) : shifted_range(Pxa, NX);
+  std::vector<double> pyt = d->py_table ? std::vector<double>(d->py_table, d->py_table + NY) : shifted_range(Pya, NY);
+  std::vector<double2> twx = twiddles(NX), twy = twiddles(NY);
+  double *x_d, *y_d, *px_d, *py_d, *bx_d, *by_d, *pr0, *pr1, *pc;
+  double2 *twx_d, *twy_d;
+  DevBuf& B = h->bufs;
+  rc = B.alloc(&x_d, NX, xt.data());
+  if (!rc) rc = B.alloc(&y_d, NY, yt.data());
+  if (!rc) rc = B.alloc(&px_d, NX, pxt.data());
+  if (!rc) rc = B.alloc(&py_d, NY, pyt.data());
+  if (!rc) rc = B.alloc(&bx_d, 2 * (size_t)NX);
+  if (!rc) rc = B.alloc(&by_d, 2 * (size_t)NY);
+  if (!rc) rc = B.alloc(&twx_d, NX, twx.data());
+  if (!rc) rc = B.alloc(&twy_d, NY, twy.data());
+  if (!rc) rc = B.alloc(&pr0, (size_t)h->n_row * wig::DNR);
+  if (!rc) rc = B.alloc(&pr1, (size_t)h->n_row * wig::DNR);
+  if (!rc) rc = B.alloc(&pc, (size_t)h->n_col * wig::DNC);
+  if (!rc) rc = B.alloc(&h->scale, 1);
+  if (rc) { B.free_all(); delete h; return rc; }
+  a.x_tab = x_d; a.y_tab = y_d; a.px_tab = px_d; a.py_tab = py_d; a.bx = bx_d; a.by = by_d;
+  a.tw_x = twx_d; a.tw_y = twy_d; a.part_row[0] = pr0; a.part_row[1] = pr1; a.part_col = pc;
+  a.n_row_cta = h->n_row; a.n_col_cta = h->n_col;
+  {
+    void* args[] = {&bx_d, &by_d};
+    rc = launch(f_setup, 8, 256, 0, 0, args);
+    if (!rc) {
+      cudaError_t e = cudaDeviceSynchronize();
+      if (e != cudaSuccess) rc = fail(WIG_ERR_CUDA, "dirac_setup: %s", cudaGetErrorString(e));
+    }
+    if (rc) { B.free_all(); delete h; return rc; }
+  }
+  *out = h;
+  return WIG_OK;
+}
+
+extern "C" int dirac_run(dirac_handle* h, void* psi_dev, int64_t t_index0, int64_t n_steps, double* obs_host,
+                         void* stream) {
+  if (!h || !psi_dev) return fail(WIG_ERR_ARG, "dirac_run: null handle or psi");
+  if (((uintptr_t)psi_dev & 15) != 0) return fail(WIG_ERR_ARG, "dirac_run: psi must be 16-byte aligned");
+  if (n_steps < 1) return fail(WIG_ERR_ARG, "dirac_run: n_steps must be >= 1");
+  int cur;
+  WIG_CUDA(cudaGetDevice(&cur));
+  if (cur != h->device) return fail(WIG_ERR_ARG, "dirac_run: current device %d != handle device %d", cur, h->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t nobs = (size_t)n_steps * DIRAC_NOBS;
+  if (int rc = ensure_obs(&h->obs, &h->obs_cap, nobs)) return rc;
+  double2* psi = (double2*)psi_dev;
+  wig::DiracArgs a = h->a;
+  const double dt = h->d.dt;
+  int rc;
+  {
+    int mode = 0, parity = 0;
+    double t_step = 0., t_obs = dt * (double)(t_index0 + 1);
+    double* obs_row = nullptr;
+    void* args[] = {&a, &psi, &mode, &parity, &t_step, &t_obs, &obs_row};
+    if ((rc = launch(h->f_row, h->n_row, h->rnt, h->smem_row, st, args))) return rc;
+  }
+  for (int64_t n = 0; n < n_steps; ++n) {
+    void* cargs[] = {&a, &psi};
+    if ((rc = launch(h->f_col, h->n_col, h->cnt, h->smem_col, st, cargs))) return rc;
+    int mode = (n == n_steps - 1) ? 2 : 1, parity = (int)((n + 1) & 1);
+    double t_step = dt * (double)(t_index0 + n + 1), t_obs = dt * (double)(t_index0 + n + 2);
+    double* obs_row = h->obs + (size_t)n * DIRAC_NOBS;
+    void* args[] = {&a, &psi, &mode, &parity, &t_step, &t_obs, &obs_row};
+    if ((rc = launch(h->f_row, h->n_row, h->rnt, h->smem_row, st, args))) return rc;
+  }
+  {
+    int parity = (int)(n_steps & 1);
+    void* args[] = {&a, &parity, &h->scale};
+    if ((rc = launch(h->f_fin, 1, h->snt, 0, st, args))) return rc;
+    long n = 4L * h->d.n_x * h->d.n_y;
+    void* sargs[] = {&psi, &n, &h->scale};
+    if ((rc = launch(h->f_scale, clampi((int)(n / (4 * h->snt)), 1, 592), h->snt, 0, st, sargs))) return rc;
+  }
+  if (obs_host) {
+    WIG_CUDA(cudaMemcpyAsync(obs_host, h->obs, nobs * sizeof(double), cudaMemcpyDeviceToHost, st));
+    WIG_CUDA(cudaStreamSynchronize(st));
+    return check_finite(obs_host, nobs, "dirac_run observables");
+  }
+  return WIG_OK;
+}
+
+extern "C" int dirac_run_host(dirac_handle* h, const void* psi_in, void* psi_out, int64_t t_index0,
+                              int64_t n_steps, double* obs_host, void* stream) {
+  if (!h || !psi_in || !psi_out) return fail(WIG_ERR_ARG, "dirac_run_host: null argument");
+  const size_t bytes = 4 * (size_t)h->d.n_x * h->d.n_y * sizeof(double2);
+  if (!h->psi_host_stage) {
+    void* p = nullptr;
+    WIG_CUDA(cudaMalloc(&p, bytes));
+    h->psi_host_stage = (double2*)p;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  WIG_CUDA(cudaMemcpyAsync(h->psi_host_stage, psi_in, bytes, cudaMemcpyHostToDevice, st));
+  int rc = dirac_run(h, h->psi_host_stage, t_index0, n_steps, nullptr, stream);
+  if (rc) return rc;
+  WIG_CUDA(cudaMemcpyAsync(psi_out, h->psi_host_stage, bytes, cudaMemcpyDeviceToHost, st));
+  const size_t nobs = (size_t)n_steps * DIRAC_NOBS;
+  if (obs_host) WIG_CUDA(cudaMemcpyAsync(obs_host, h->obs, nobs * sizeof(double), cudaMemcpyDeviceToHost, st));
+  WIG_CUDA(cudaStreamSynchronize(st));
+  if (obs_host) return check_finite(obs_host, nobs, "dirac_run_host observables");
+  return WIG_OK;
+}
+
+extern "C" int dirac_destroy(dirac_handle* h) {
+  if (!h) return WIG_OK;
+  cudaDeviceSynchronize();
+  h->bufs.free_all();
+  if (h->obs) cudaFree(h->obs);
+  if (h->psi_host_stage) cudaFree(h->psi_host_stage);
+  delete h;
+  return WIG_OK;
+}
+
+extern "C" const char* wig_last_error(void) { return g_last_error.c_str(); }
+extern "C" int wig_abi_version(void) { return WIG_ABI_VERSION; }

@@ -1,0 +1,168 @@
+// Shared-memory batched Stockham FFT for sm_100a (double and float).
+//
+// One CTA transforms NB independent sequences of length N (power of two) that
+// live in shared memory.  The element layout is a template functor ("Map") so
+// that the same code serves contiguous rows (x-pass: sequence = one grid row)
+// and interleaved column tiles (p-pass: sequence = one grid column, the tile
+// stored row-major, so element k of column c sits at k*NB + c).
+//
+// Stockham autosort, mixed radix 8/4/2: stage s combines R sub-transforms of
+// length Ns into length Ns*R.  Butterfly j (0 <= j < N/R) reads elements
+// j + r*N/R, applies twiddles W_{Ns R}^{(j mod Ns) r}, does an R-point DFT and
+// writes to (j/Ns)*Ns*R + (j mod Ns) + r*Ns.  Output is in natural order.
+// Each stage is done in place through registers: every thread loads all of
+// its butterflies' inputs, the CTA synchronises, then every thread writes.
+//
+// Twiddles come from a table tw[m] = exp(-2 pi i m / N), m < N, computed on
+// the host in extended precision; the inverse transform uses the conjugates.
+// Forward = exp(-i ...), inverse unnormalised (the callers fold 1/N into a
+// pointwise factor, which is exact because N is a power of two).
+#pragma once
+
+namespace wig {
+
+template <class T> struct V2;
+template <> struct V2<double> { typedef double2 t; };
+template <> struct V2<float>  { typedef float2 t;  };
+
+__device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2  mk(float a, float b)   { return make_float2(a, b); }
+
+template <class C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <class C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+// (a.x + i a.y)(b.x + i b.y), the textbook formula (same as pycuda::complex)
+template <class C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+template <class C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+template <class C, class T> __device__ __forceinline__ C cscale(C a, T s) { a.x *= s; a.y *= s; return a; }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV, class C> __device__ __forceinline__ C mul_mi(C a) {
+  C r;
+  if (INV) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+  return r;
+}
+
+// ---------------------------------------------------------------- R-point DFTs
+template <bool INV, class C> __device__ __forceinline__ void dft2(C& a, C& b) {
+  C t = a; a = cadd(t, b); b = csub(t, b);
+}
+
+template <bool INV, class C> __device__ __forceinline__ void dft4(C& v0, C& v1, C& v2, C& v3) {
+  C a0 = cadd(v0, v2), a1 = csub(v0, v2), a2 = cadd(v1, v3), a3 = mul_mi<INV>(csub(v1, v3));
+  v0 = cadd(a0, a2); v2 = csub(a0, a2); v1 = cadd(a1, a3); v3 = csub(a1, a3);
+}
+
+template <bool INV, class C> __device__ __forceinline__ void dft8(C* v) {
+  typedef decltype(v[0].x) T;
+  const T h = (T)0.70710678118654752440084436210485;   // sqrt(1/2)
+  C a[4], b[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) { a[k] = cadd(v[k], v[k + 4]); b[k] = csub(v[k], v[k + 4]); }
+  // b_k *= W8^k  (W8 = exp(-+ 2 pi i / 8))
+  {
+    C t = b[1];
+    if (INV) { b[1].x = h * (t.x - t.y); b[1].y = h * (t.x + t.y); }
+    else     { b[1].x = h * (t.x + t.y); b[1].y = h * (t.y - t.x); }
+    b[2] = mul_mi<INV>(b[2]);
+    t = b[3];
+    if (INV) { b[3].x = -h * (t.x + t.y); b[3].y = h * (t.x - t.y); }
+    else     { b[3].x = h * (t.y - t.x); b[3].y = -h * (t.x + t.y); }
+  }
+  dft4<INV>(a[0], a[1], a[2], a[3]);
+  dft4<INV>(b[0], b[1], b[2], b[3]);
+#pragma unroll
+  for (int m = 0; m < 4; ++m) { v[2 * m] = a[m]; v[2 * m + 1] = b[m]; }
+}
+
+template <int R, bool INV, class C> __device__ __forceinline__ void dft(C* v) {
+  if (R == 2) dft2<INV>(v[0], v[1]);
+  else if (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+  else dft8<INV>(v);
+}
+
+// ---------------------------------------------------------------- layouts
+// Contiguous rows: sequence b, element k at b*(N + pad) + k + pad(k);
+// PADSH > 0 inserts one slot every 2^PADSH elements (bank-conflict relief for
+// the stride-R writes of the first stage).
+template <int N, int PADSH> struct RowMap {
+  static constexpr int stride = N + (PADSH > 0 ? (N >> PADSH) : 0);
+  __device__ __forceinline__ static int padded(int k) { return PADSH > 0 ? k + (k >> PADSH) : k; }
+  __device__ __forceinline__ static int idx(int b, int k) { return b * stride + padded(k); }
+  // butterfly q -> (sequence, butterfly-in-sequence): consecutive q walk along a row
+  template <int NBF> __device__ __forceinline__ static void split(int q, int& b, int& j) { b = q / NBF; j = q % NBF; }
+};
+
+// Column tile stored row-major: sequence (column) b, element k at k*NB + b.
+template <int NB> struct ColMap {
+  __device__ __forceinline__ static int idx(int b, int k) { return k * NB + b; }
+  template <int NBF> __device__ __forceinline__ static void split(int q, int& b, int& j) { b = q % NB; j = q / NB; }
+};
+
+template <int N, int NS> struct Radix {
+  static constexpr int rem = N / NS;
+  static constexpr int value = rem >= 8 ? 8 : (rem >= 4 ? 4 : 2);
+};
+
+// One Stockham stage over all NB sequences.
+template <class C, int N, int NS, int NB, int NT, bool INV, class Map>
+__device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
+  constexpr int R = Radix<N, NS>::value;
+  constexpr int NBF = N / R;                 // butterflies per sequence
+  constexpr int TOT = NB * NBF;              // butterflies per stage
+  constexpr int PER = (TOT + NT - 1) / NT;   // per thread
+  const int tid = threadIdx.x;
+  C v[PER][R];
+#pragma unroll
+  for (int m = 0; m < PER; ++m) {
+    const int q = tid + m * NT;
+    if ((TOT % NT) == 0 || q < TOT) {
+      int b, j;
+      Map::template split<NBF>(q, b, j);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[m][r] = s[Map::idx(b, j + r * NBF)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < PER; ++m) {
+    const int q = tid + m * NT;
+    if ((TOT % NT) == 0 || q < TOT) {
+      int b, j;
+      Map::template split<NBF>(q, b, j);
+      const int k = j & (NS - 1);
+      if (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          C w = tw[(k * r) * (N / (NS * R))];
+          if (INV) w = cconj(w);
+          v[m][r] = cmul(v[m][r], w);
+        }
+      }
+      dft<R, INV>(v[m]);
+      const int d = (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[Map::idx(b, d + r * NS)] = v[m][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <class C, int N, int NS, int NB, int NT, bool INV, class Map> struct FftRun {
+  __device__ __forceinline__ static void run(C* s, const C* __restrict__ tw) {
+    fft_stage<C, N, NS, NB, NT, INV, Map>(s, tw);
+    FftRun<C, N, NS * Radix<N, NS>::value, NB, NT, INV, Map>::run(s, tw);
+  }
+};
+template <class C, int N, int NB, int NT, bool INV, class Map> struct FftRun<C, N, N, NB, NT, INV, Map> {
+  __device__ __forceinline__ static void run(C*, const C* __restrict__) {}
+};
+
+// Batched FFT of NB sequences of length N in shared memory (caller has
+// synchronised before; the CTA is synchronised on return).
+template <class C, int N, int NB, int NT, bool INV, class Map>
+__device__ __forceinline__ void cta_fft(C* s, const C* __restrict__ tw) {
+  FftRun<C, N, 1, NB, NT, INV, Map>::run(s, tw);
+}
+
+}  // namespace wig

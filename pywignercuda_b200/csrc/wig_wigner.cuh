@@ -1,0 +1,297 @@
+// Wigner2D split-operator step for sm_100a: two fused passes per step.
+//
+// Layout: W is (N_p, N_x) complex128, row-major, x contiguous, FFT-shifted in
+// both axes (array index 0 holds coordinate 0) -- the reference's layout
+// (GPU_Wigner2D_FFT.py:577-581).
+//
+//  x-pass (one CTA = ROWS contiguous rows):
+//      prologue: deferred normalisation W <- W * s, s = 1/(dX dP sum W) taken
+//                from the previous pass's per-CTA partial sums;
+//      row FFT x->lambda, kinetic factor, row IFFT (1/N_x folded in).
+//      (expPLambda_source :131-158 / expPLambdaKinetic_source :162-200 between
+//       Fourier_X_To_Lambda_GPU and Fourier_Lambda_To_X_GPU, :1885-1888)
+//  p-pass (one CTA = a tile of C columns x all N_p rows):
+//      column FFT p->theta, Moyal potential factor, diffusion factor and the
+//      two absorbing masks, column IFFT (1/N_p folded in)
+//      (expPotential_source :80-126, :1891-1899);
+//      Caldeira-Leggett order 3 (CaldeiraDissipatorOrder3 :1145-1157) on the
+//      tile still in shared memory;
+//      epilogue: store W' and this CTA's partial sums of the 10 observables
+//      plus sum W (Run :1857-1878,1912).
+//
+// Each pass reads and writes W once (64 B per grid point per step).
+#pragma once
+#include "wig_fft.cuh"
+
+namespace wig {
+
+constexpr int NACC = 12;   // sumRe, sumIm, x, x^2, p, p^2, xp, V', pV', xV', H, negative
+constexpr int NOBS = 11;   // norm, x, x^2, p, p^2, xp, V', pV', xV', H, negative area
+
+struct WigArgs {
+  // kernel constants exactly as the reference's kernels see them
+  // (SetCUDA_Constants :833-842: '%f'-rounded unless exact mode is asked for)
+  double dt, dx, dp, dtheta, dlambda, mass, hbar, D_theta, D_lambda;
+  // host-side exact values (the reference's observable tables and sums)
+  double dX, dP, mass_exact;
+  // Caldeira-Leggett polynomial W + c3 D(W + c12 D(W + c1 D W)) (Horner form of
+  // W + a(1 + a/2)(1 + a/3)W, a = 2 i gamma dt D)
+  double2 cl_k1, cl_k12, cl_c3;
+  // 1-D device tables
+  const double* x_tab;     // [n_x] shifted X (exact)
+  const double* p_tab;     // [n_p] shifted P (exact)
+  const double* dV_tab;    // [n_x] dPotential(0, x)
+  const double* V0_tab;    // [n_x] Potential(0, x)
+  const double* theta_s;   // [n_p] exact shifted Theta / n_p
+  const double* r_lambda;  // [n_x] exp(-D_Lambda lambda^2)       (per frequency)
+  const double* r_theta;   // [n_p] exp(-D_Theta theta^2 dt)      (per frequency)
+  const double* mask1;     // [n_x] 1 - exp(-(x - x_max)^2/(10 dx)^2)
+  const double* mask2s;    // [n_x] (1 - exp(-(x + x_max)^2/(10 dx)^2)) / n_p
+  const double* sfp;       // [n_p] sign(p) f(p)   (theta_fp_source :399-431)
+  const double2* tw_x;     // [n_x] exp(-2 pi i m / n_x)
+  const double2* tw_p;     // [n_p]
+  double* partials;        // [n_cta][NACC]
+  int n_partials;          // CTAs that wrote `partials`
+};
+
+// ------------------------------------------------------------------ reductions
+template <int NT, int NV>
+__device__ __forceinline__ void block_sum(double (&acc)[NV], double (*red)[NV]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double x = acc[v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    acc[v] = x;
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) red[warp][v] = acc[v];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double s = 0.;
+    for (int w = 0; w < NT / 32; ++w) s += red[w][threadIdx.x];
+    red[0][threadIdx.x] = s;     // only lane threadIdx.x < NV reads/writes column threadIdx.x
+  }
+  __syncthreads();
+}
+
+// numpy's complex reciprocal 1/(a + i b) (Smith's method)
+__device__ __forceinline__ double2 crecip(double2 z) {
+  double2 r;
+  if (fabs(z.x) >= fabs(z.y)) {
+    const double rat = z.y / z.x, scl = 1.0 / (z.x + z.y * rat);
+    r.x = scl; r.y = -rat * scl;
+  } else {
+    const double rat = z.x / z.y, scl = 1.0 / (z.y + z.x * rat);
+    r.x = rat * scl; r.y = -scl;
+  }
+  return r;
+}
+
+// Scale modes: 0 = none; 1 = the initial normalisation of Run (:1779-1780,
+// norm = (sum W * dX) * dP); 2 = the per-step one (:1912-1913,
+// norm = sum W * (dX * dP)).  Reduces the previous pass's partials, returns
+// s = 1/norm (or 1) and, when obs_row != nullptr, writes that sample's 11
+// observables.
+template <int NT>
+__device__ __forceinline__ double2 consume_partials(const WigArgs& a, int mode, double* obs_row,
+                                                    double (*red)[NACC]) {
+  double acc[NACC];
+#pragma unroll
+  for (int v = 0; v < NACC; ++v) acc[v] = 0.;
+  const int ncol = obs_row ? NACC : 2;
+  for (int i = threadIdx.x; i < a.n_partials; i += NT) {
+    const double* p = a.partials + (size_t)i * NACC;
+#pragma unroll
+    for (int v = 0; v < NACC; ++v)
+      if (v < ncol) acc[v] += p[v];
+  }
+  block_sum<NT, NACC>(acc, red);
+  const double2 S = make_double2(red[0][0], red[0][1]);
+  double2 s = make_double2(1., 0.);
+  if (mode == 1) s = crecip(make_double2(S.x * a.dX * a.dP, S.y * a.dX * a.dP));
+  else if (mode == 2) { const double d = a.dX * a.dP; s = crecip(make_double2(S.x * d, S.y * d)); }
+  if (obs_row && threadIdx.x < NOBS) {
+    const double dXdP = a.dX * a.dP;
+    double val;
+    if (threadIdx.x == 0) val = (s.x * S.x - s.y * S.y) * dXdP;
+    else val = s.x * (dXdP * red[0][threadIdx.x + 1]);
+    obs_row[threadIdx.x] = val;
+  }
+  __syncthreads();   // red[] is reused by the caller
+  return s;
+}
+
+__device__ __forceinline__ void accumulate_obs(double (&acc)[NACC], double2 v, double x, double p,
+                                               double dV, double V0, double mass_exact) {
+  const double w = v.x;
+  acc[0] += v.x;
+  acc[1] += v.y;
+  acc[2] += w * x;
+  acc[3] += w * (x * x);
+  acc[4] += w * p;
+  acc[5] += w * (p * p);
+  acc[6] += w * (p * x);
+  acc[7] += w * dV;
+  acc[8] += w * (p * dV);
+  acc[9] += w * (dV * x);
+  acc[10] += w * ((p * p) / (2. * mass_exact) + V0);
+  acc[11] += (w < 0.) ? w : 0.;
+}
+
+// ------------------------------------------------------------------ kernels
+// Partial sums over the whole grid (initial state, or any state): grid-stride.
+template <int NX, int NP, int NT>
+__device__ __forceinline__ void reduce_body(const WigArgs& a, const double2* __restrict__ W,
+                                            double* __restrict__ partials) {
+  __shared__ double red[NT / 32][NACC];
+  double acc[NACC];
+#pragma unroll
+  for (int v = 0; v < NACC; ++v) acc[v] = 0.;
+  for (int e = blockIdx.x * NT + threadIdx.x; e < NX * NP; e += gridDim.x * NT) {
+    const int i = e / NX, j = e - i * NX;
+    accumulate_obs(acc, W[e], a.x_tab[j], a.p_tab[i], a.dV_tab[j], a.V0_tab[j], a.mass_exact);
+  }
+  block_sum<NT, NACC>(acc, red);
+  if (threadIdx.x < NACC) partials[(size_t)blockIdx.x * NACC + threadIdx.x] = red[0][threadIdx.x];
+}
+
+// One CTA: the last sample's observables and the final scale.
+template <int NT>
+__device__ __forceinline__ void finalize_body(const WigArgs& a, int mode, double* obs_row,
+                                              double2* scale_out) {
+  __shared__ double red[NT / 32][NACC];
+  const double2 s = consume_partials<NT>(a, mode, obs_row, red);
+  if (threadIdx.x == 0) *scale_out = s;
+}
+
+template <int NT>
+__device__ __forceinline__ void scale_body(double2* __restrict__ W, long n, const double2* s_ptr) {
+  const double2 s = *s_ptr;
+  for (long e = (long)blockIdx.x * NT + threadIdx.x; e < n; e += (long)gridDim.x * NT)
+    W[e] = cmul(W[e], s);
+}
+
+// x-pass: ROWS rows per CTA.
+template <class Phys, int NX, int NP, int ROWS, int NT, int PAD, bool KIN_STRING>
+__device__ __forceinline__ void xpass_body(const WigArgs& a, const Phys& ph, double2* __restrict__ W,
+                                           int scale_mode, double* obs_row) {
+  typedef RowMap<NX, PAD> M;
+  extern __shared__ double2 sm[];
+  __shared__ double red[NT / 32][NACC];
+  double2 s = make_double2(1., 0.);
+  if (scale_mode != 0 || (obs_row != nullptr && blockIdx.x == 0))
+    s = consume_partials<NT>(a, scale_mode, blockIdx.x == 0 ? obs_row : nullptr, red);
+
+  const int row0 = blockIdx.x * ROWS;
+  double2* Wb = W + (size_t)row0 * NX;
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    double2 v = Wb[e];
+    if (scale_mode != 0) v = cmul(v, s);
+    sm[M::idx(r, k)] = v;
+  }
+  __syncthreads();
+  cta_fft<double2, NX, ROWS, NT, false, M>(sm, a.tw_x);
+  const double inv_n = 1.0 / (double)NX;
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    const int ii = (row0 + r + NP / 2) % NP;
+    const int jj = (k + NX / 2) % NX;
+    const double lambda = a.dlambda * (jj - 0.5 * NX);
+    const double p = a.dp * (ii - 0.5 * NP);
+    double phase;
+    if (KIN_STRING)
+      phase = a.dt * ((ph.KineticEnergy(p + a.hbar * lambda / 2.) -
+                       ph.KineticEnergy(p - a.hbar * lambda / 2.)) / a.hbar);
+    else
+      phase = a.dt * lambda * p / a.mass;
+    const double rr = a.r_lambda[k] * inv_n;
+    double sn, cs;
+    sincos(phase, &sn, &cs);
+    const int id = M::idx(r, k);
+    sm[id] = cmul(sm[id], make_double2(rr * cs, -rr * sn));
+  }
+  __syncthreads();
+  cta_fft<double2, NX, ROWS, NT, true, M>(sm, a.tw_x);
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    Wb[e] = sm[M::idx(r, k)];
+  }
+}
+
+// D(B) = IFFT_p[theta FFT_p(sign(p) f(p) B)] / n_p, in place on the tile.
+template <int NP, int C, int NT>
+__device__ __forceinline__ void cl_apply_D(const WigArgs& a, double2* B) {
+  typedef ColMap<C> M;
+  for (int e = threadIdx.x; e < C * NP; e += NT) B[e] = cscale(B[e], a.sfp[e / C]);
+  __syncthreads();
+  cta_fft<double2, NP, C, NT, false, M>(B, a.tw_p);
+  for (int e = threadIdx.x; e < C * NP; e += NT) B[e] = cscale(B[e], a.theta_s[e / C]);
+  __syncthreads();
+  cta_fft<double2, NP, C, NT, true, M>(B, a.tw_p);
+}
+
+// p-pass: a tile of C columns x NP rows per CTA.  DAMP: 0 none, 1 Caldeira-Leggett.
+template <class Phys, int NX, int NP, int C, int NT, int DAMP>
+__device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, double2* __restrict__ W,
+                                           double t, double* __restrict__ partials) {
+  typedef ColMap<C> M;
+  extern __shared__ double2 sm[];
+  __shared__ double red[NT / 32][NACC];
+  double2* A = sm;
+  double2* B = sm + C * NP;
+  const int col0 = blockIdx.x * C;
+  for (int e = threadIdx.x; e < C * NP; e += NT) {
+    const int k = e / C, c = e - k * C;
+    A[e] = W[(size_t)k * NX + col0 + c];
+  }
+  __syncthreads();
+  cta_fft<double2, NP, C, NT, false, M>(A, a.tw_p);
+  for (int e = threadIdx.x; e < C * NP; e += NT) {
+    const int k = e / C, c = e - k * C;
+    const int col = col0 + c;
+    const int ii = (k + NP / 2) % NP;
+    const int jj = (col + NX / 2) % NX;
+    const double x = a.dx * (jj - 0.5 * NX);
+    const double theta = a.dtheta * (ii - 0.5 * NP);
+    const double phase = a.dt * ((ph.Potential(t, x - a.hbar * theta / 2.) -
+                                  ph.Potential(t, x + a.hbar * theta / 2.)) / a.hbar);
+    const double r = a.r_theta[k];
+    double sn, cs;
+    sincos(phase, &sn, &cs);
+    double2 v = cmul(A[e], make_double2(r * cs, -r * sn));
+    v = cscale(v, a.mask1[col]);
+    v = cscale(v, a.mask2s[col]);
+    A[e] = v;
+  }
+  __syncthreads();
+  cta_fft<double2, NP, C, NT, true, M>(A, a.tw_p);
+  if (DAMP == 1) {
+    for (int e = threadIdx.x; e < C * NP; e += NT) B[e] = A[e];
+    cl_apply_D<NP, C, NT>(a, B);
+    for (int e = threadIdx.x; e < C * NP; e += NT) B[e] = cadd(A[e], cmul(a.cl_k1, B[e]));
+    cl_apply_D<NP, C, NT>(a, B);
+    for (int e = threadIdx.x; e < C * NP; e += NT) B[e] = cadd(A[e], cmul(a.cl_k12, B[e]));
+    cl_apply_D<NP, C, NT>(a, B);
+    for (int e = threadIdx.x; e < C * NP; e += NT) A[e] = cadd(A[e], cmul(a.cl_c3, B[e]));
+    __syncthreads();
+  }
+  double acc[NACC];
+#pragma unroll
+  for (int v = 0; v < NACC; ++v) acc[v] = 0.;
+  for (int e = threadIdx.x; e < C * NP; e += NT) {
+    const int k = e / C, c = e - k * C;
+    const int col = col0 + c;
+    const double2 v = A[e];
+    W[(size_t)k * NX + col] = v;
+    accumulate_obs(acc, v, a.x_tab[col], a.p_tab[k], a.dV_tab[col], a.V0_tab[col], a.mass_exact);
+  }
+  block_sum<NT, NACC>(acc, red);
+  if (threadIdx.x < NACC) partials[(size_t)blockIdx.x * NACC + threadIdx.x] = red[0][threadIdx.x];
+}
+
+}  // namespace wig

@@ -1,0 +1,362 @@
+"""Drop-in Wigner2D propagators: ``GPU_Wigner2D_FFT`` and ``GPU_Wigner2D_ODM2``.
+
+Same construction protocol as the reference (``GPU_Wigner2D_FFT.py:529-1964``):
+an instance subclass sets ``dampingFunction``, ``grossPitaevskiiCoefficient``,
+``fp_Damping_String`` (and ``epsilon`` / ``L_material`` for ODM), calls
+``SetTimeTrack(dt, timeSteps, skipFrames, fileName)`` and then the class
+constructor with the grid, amplitudes, hbar, mass, diffusion, damping and the
+potential / derivative / kinetic expression strings; it sets ``W_init`` (FFT-
+shifted (P_gridDIM, X_gridDIM) array) and calls ``Run()``.  ``Run()`` returns 0
+and leaves ``timeRange``, ``X_average``, ``X2_average``, ``P_average``,
+``P2_average``, ``XP_average``, ``dPotentialdX_average``,
+``PdPotentialdX_average``, ``XdPotentialdX_average``, ``Hamiltonian_average``,
+``negativeArea`` and ``W_end`` on the instance (``:1918-1954``), plus
+``Norm_average`` (dX dP sum W of each sample) and ``frames`` (the W saved every
+``skipFrames`` steps, ``save_Frame`` :660-663; written to HDF5 as the reference
+does when h5py is importable and ``fileName`` is set).
+
+The propagation runs on the GPU through ``libwigner_b200.so``; device memory
+and the stream come from PyTorch.  There is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import WigDesc, check, dptr
+
+try:                                   # HDF5 output is optional (h5py may be absent)
+    import h5py as _h5py
+except ImportError:                    # pragma: no cover - depends on the image
+    _h5py = None
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise _lib.WignerCudaError('no CUDA device: the propagators run on the GPU only')
+    return torch
+
+
+def _eval(expr, **variables):
+    """The reference's host-side evaluation of expression strings
+    (``eval(s, np.__dict__, locals())`` with ``pow = np.power``, :674-692)."""
+    ns = dict(np.__dict__)
+    ns.update(pow=np.power, atan=np.arctan, M_E=np.e, sqrt=np.sqrt, exp=np.exp, fabs=np.fabs)
+    ns.update(variables)
+    return eval(expr, ns)
+
+
+class Propagator_Base:
+    """Grid, helpers and initial states of the reference's ``Propagator_Base``
+    (``GPU_Wigner2D_FFT.py:529-1705``) that instances use on the host."""
+
+    constants_mode = _lib.CONST_CUDA_F     # '%f' kernel constants, as the reference
+
+    def SetTimeTrack(self, dt, timeSteps=128, skipFrames=1, fileName='', compression=None):
+        self.runTime = float(dt) * timeSteps
+        self.timeSteps = timeSteps
+        self.dt = dt
+        self.skipFrames = skipFrames
+        self.fileName = fileName
+        self.compression = compression
+
+    def SetPhaseSpaceBox2D(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude):
+        self.X_gridDIM = X_gridDIM
+        self.P_gridDIM = P_gridDIM
+        self.X_amplitude = X_amplitude
+        self.P_amplitude = P_amplitude
+        self.dX = 2. * X_amplitude / float(X_gridDIM)
+        self.dP = 2. * P_amplitude / float(P_gridDIM)
+        self.dTheta = 2. * np.pi / (2. * P_amplitude)
+        self.Theta_amplitude = self.dTheta * P_gridDIM / 2.
+        self.dLambda = 2. * np.pi / (2. * X_amplitude)
+        self.Lambda_amplitude = self.dLambda * X_gridDIM / 2.
+        self.SetPhaseSpaceGrid2D()
+
+    def SetPhaseSpaceGrid2D(self):
+        self.X_range = np.linspace(-self.X_amplitude, self.X_amplitude - self.dX, self.X_gridDIM)
+        self.Lambda_range = np.linspace(-self.Lambda_amplitude, self.Lambda_amplitude - self.dLambda,
+                                        self.X_gridDIM)
+        self.Theta_range = np.linspace(-self.Theta_amplitude, self.Theta_amplitude - self.dTheta,
+                                       self.P_gridDIM)
+        self.P_range = np.linspace(-self.P_amplitude, self.P_amplitude - self.dP, self.P_gridDIM)
+        self.X = np.fft.fftshift(self.X_range)[np.newaxis, :]
+        self.Theta = np.fft.fftshift(self.Theta_range)[:, np.newaxis]
+        self.Lambda = np.fft.fftshift(self.Lambda_range)[np.newaxis, :]
+        self.P = np.fft.fftshift(self.P_range)[:, np.newaxis]
+
+    # ---- expression strings evaluated on the host (:674-692, :1674-1681)
+    def Potential(self, t, x):
+        return _eval(self.potentialString, t=t, x=x)
+
+    def dPotential(self, t, x):
+        return _eval(self.dPotentialString, t=t, x=x)
+
+    def fp_Damping(self, p):
+        return _eval(self.fp_Damping_String, p=p)
+
+    # ---- helpers
+    def fft_shift2D(self, X):
+        return np.fft.fftshift(np.fft.fftshift(X, axes=1), axes=0)
+
+    def WignerMarginal_Probability_x(self, W):
+        return np.sum(W, axis=0) * self.dP
+
+    def WignerMarginal_Probability_p(self, W):
+        return np.sum(W, axis=1) * self.dX
+
+    def Fourier_Theta_To_P_CPU(self, W):
+        return np.fft.ifft(W, axis=0)
+
+    def Fourier_P_To_Theta_CPU(self, W):
+        return np.fft.fft(W, axis=0)
+
+    def Fourier_X_To_Lambda_CPU(self, W):
+        return np.fft.fft(W, axis=1)
+
+    def Fourier_Lambda_To_X_CPU(self, W):
+        return np.fft.ifft(W, axis=1)
+
+    # ---- initial states (:715-771)
+    def Wigner_HarmonicOscillator(self, n, omega, x, p):
+        from scipy.special import eval_laguerre
+        self.representation = 'x_p'
+        r2 = self.mass * omega ** 2 * ((self.X - x)) ** 2 + ((self.P - p)) ** 2 / self.mass
+        W = (-1) ** (n) * eval_laguerre(n, 2 * r2) * np.exp(-r2)
+        norm = np.sum(W) * self.dX * self.dP
+        return W / norm
+
+    def Heaviside(self, x):
+        return 0.5 * (np.sign(x) + 1.)
+
+    def Psi_Half_HarmonicOscillator(self, n, omega, x0, p0, X):
+        from scipy.special import eval_legendre
+        k = np.sqrt(self.mass * omega / self.hBar)
+        return (np.exp(1j * p0) * np.exp(-0.5 * k ** 2 * (X - x0) ** 2) * eval_legendre(n, k * (X - x0))
+                * self.Heaviside(-(X - x0)))
+
+    def Wigner_Half_HarmonicOscillator(self, n, omega, x0, p0):
+        X_minus = self.X_range[np.newaxis, :] - 0.5 * self.hBar * self.Theta_range[:, np.newaxis]
+        X_plus = self.X_range[np.newaxis, :] + 0.5 * self.hBar * self.Theta_range[:, np.newaxis]
+        W = (self.Psi_Half_HarmonicOscillator(n, omega, x0, p0, X_minus)
+             * self.Psi_Half_HarmonicOscillator(n, omega, x0, p0, X_plus).conj())
+        W = self.Fourier_Theta_To_P_CPU(np.fft.fftshift(W))
+        return W / (np.sum(W) * self.dX * self.dP)
+
+    def Wigner_FromWavefunction(self, psi):
+        """Wigner function of a wave-function callable psi(x), by the same discrete
+        transform as ``Wigner_Half_HarmonicOscillator`` (psi(x - hbar theta/2)
+        psi*(x + hbar theta/2), IFFT over theta), shifted layout, normalised."""
+        X_minus = self.X_range[np.newaxis, :] - 0.5 * self.hBar * self.Theta_range[:, np.newaxis]
+        X_plus = self.X_range[np.newaxis, :] + 0.5 * self.hBar * self.Theta_range[:, np.newaxis]
+        W = psi(X_minus) * np.conj(psi(X_plus))
+        W = self.Fourier_Theta_To_P_CPU(np.fft.fftshift(W))
+        return W / (np.sum(W) * self.dX * self.dP)
+
+    # ---- classical reference trajectories (:597-657)
+    def symplecticExpK(self, mass, dt, c, Z):
+        return Z + np.array([dt * c * Z[1] / mass, 0])
+
+    def symplecticExpV(self, mass, dt, d, dVdx, Z):
+        return Z + np.array([0, -dt * d * dVdx(0., Z[0])])
+
+    def symplecticExpKExpV2(self, mass, dt, dVdx, Z0):
+        Z = self.symplecticExpK(mass, dt, 0.5, self.symplecticExpV(mass, dt, 1.0, dVdx, Z0))
+        return self.symplecticExpK(mass, dt, 0.5, self.symplecticExpV(mass, dt, 0.0, dVdx, Z))
+
+    def SymplecticPropagator(self, dt, n_iterations, Z0, gammaDamping):
+        Z = np.asarray(Z0, dtype=float)
+        trajectory = []
+        for i in range(n_iterations):
+            trajectory.append(np.append(Z, dt * (i + 1)))
+            Z = self.symplecticExpKExpV2(self.mass, dt, self.dPotential, Z)
+            Z[1] = np.exp(-2. * gammaDamping * dt) * Z[1]
+        return np.array(trajectory)
+
+
+class GPU_Wigner2D_FFT(Propagator_Base):
+    """Wigner propagator with diffusion and Caldeira-Leggett / ODM damping
+    (``GPU_Wigner2D_FFT.py:1713-1964``)."""
+
+    _odm2 = False
+
+    def __init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass, D_Theta, D_Lambda,
+                 gammaDamping, potentialString, dPotentialString, kinematicString, normalization='Wigner'):
+        self.normalization = normalization
+        self.D_Theta = D_Theta
+        self.D_Lambda = D_Lambda
+        self.gammaDamping = gammaDamping
+        self.potentialString = potentialString
+        self.dPotentialString = dPotentialString
+        self.kinematicString = kinematicString
+        self.SetPhaseSpaceBox2D(X_gridDIM, P_gridDIM, X_amplitude, P_amplitude)
+        self.hBar = hBar
+        self.mass = mass
+        self._build()
+
+    def _damping_code(self):
+        kind = getattr(self, 'dampingFunction', 'CaldeiraLeggett')
+        if kind == 'CaldeiraLeggett':
+            return _lib.DAMP_CALDEIRA_LEGGETT
+        if kind == 'ODM':
+            return _lib.DAMP_ODM
+        return _lib.DAMP_NONE
+
+    def _build(self):
+        if getattr(self, 'grossPitaevskiiCoefficient', 0.) != 0.:
+            raise _lib.WignerUnsupportedError('the Gross-Pitaevskii term is not part of this propagator')
+        if not hasattr(self, 'fp_Damping_String'):
+            self.fp_Damping_String = 'fabs(p)'
+        for name in ('dt', 'timeSteps'):
+            if not hasattr(self, name):
+                raise _lib.WignerArgumentError('call SetTimeTrack(dt, timeSteps, ...) before the constructor')
+        lib = _lib.load()
+        # host tables of Run (:1747, :1785-1792), evaluated with numpy like the reference
+        self._x_tab = np.ascontiguousarray(self.X[0], dtype=np.float64)
+        self._p_tab = np.ascontiguousarray(self.P[:, 0], dtype=np.float64)
+        self._theta_tab = np.ascontiguousarray(self.Theta[:, 0], dtype=np.float64)
+        self._lambda_tab = np.ascontiguousarray(self.Lambda[0], dtype=np.float64)
+        self._dv_tab = np.ascontiguousarray(
+            np.broadcast_to(self.dPotential(0., self.X), self.X.shape)[0], dtype=np.float64)
+        self._v0_tab = np.ascontiguousarray(
+            np.broadcast_to(self.Potential(0, self.X), self.X.shape)[0], dtype=np.float64)
+        self.Hamiltonian = self.fft_shift2D(self.P ** 2 / (2. * self.mass) + self.Potential(0, self.X))
+        d = WigDesc()
+        d.abi_version = _lib.ABI_VERSION
+        d.n_x, d.n_p = int(self.X_gridDIM), int(self.P_gridDIM)
+        d.damping = self._damping_code()
+        d.kinetic_from_string = 1 if self._odm2 else 0
+        d.constants = self.constants_mode
+        d.precision = _lib.PREC_C128
+        d.n_lindblad = 2 if self._odm2 else 1
+        d.x_amplitude, d.p_amplitude = float(self.X_amplitude), float(self.P_amplitude)
+        d.hbar, d.mass, d.dt = float(self.hBar), float(self.mass), float(self.dt)
+        d.d_theta, d.d_lambda, d.gamma = float(self.D_Theta), float(self.D_Lambda), float(self.gammaDamping)
+        d.epsilon = float(getattr(self, 'epsilon', 0.5))
+        d.l_material = float(getattr(self, 'L_material', 1.0))
+        d.weight1 = float(getattr(self, 'weightLindbland1', 1.0))
+        d.weight2 = float(getattr(self, 'weightLindbland2', 0.0))
+        self._strings = [s.encode() for s in (self.potentialString, self.kinematicString,
+                                              self.fp_Damping_String)]
+        d.potential, d.kinetic, d.fp_damping = self._strings
+        d.x_table, d.p_table = dptr(self._x_tab), dptr(self._p_tab)
+        d.theta_table, d.lambda_table = dptr(self._theta_tab), dptr(self._lambda_tab)
+        d.dv_table, d.v0_table = dptr(self._dv_tab), dptr(self._v0_tab)
+        self._desc = d
+        torch = _torch()
+        self._device = torch.cuda.current_device()
+        h = ctypes.c_void_p()
+        check(lib.wig_create(d, h), 'wig_create')
+        self._handle = h
+
+    def __del__(self):
+        h = getattr(self, '_handle', None)
+        if h is not None and h.value:
+            try:
+                _lib.load().wig_destroy(h)
+            except Exception:
+                pass
+            h.value = None
+
+    # ------------------------------------------------------------------ run
+    def propagate(self, W, n_prop, t_index0=0, continue_run=False, stream=None):
+        """Advance the device array ``W`` (torch complex128 (P, X), in place) by
+        ``n_prop`` propagations; returns the (n_prop+1, 11) observables
+        (norm, x, x^2, p, p^2, xp, V', pV', xV', H, negative area)."""
+        torch = _torch()
+        if W.dtype != torch.complex128 or not W.is_cuda or not W.is_contiguous() or \
+                tuple(W.shape) != (self.P_gridDIM, self.X_gridDIM):
+            raise _lib.WignerArgumentError('W must be a contiguous CUDA complex128 tensor of shape (P, X)')
+        obs = np.empty((n_prop + 1, _lib.WIG_NOBS))
+        st = stream if stream is not None else torch.cuda.current_stream(W.device)
+        flags = _lib.WIG_RUN_CONTINUE if continue_run else 0
+        check(_lib.load().wig_run(self._handle, W.data_ptr(), t_index0, n_prop, flags, dptr(obs),
+                                  st.cuda_stream), 'wig_run')
+        return obs
+
+    def _frame_sink(self):
+        if _h5py is not None and self.fileName:
+            import os
+            try:
+                os.remove(self.fileName)
+            except OSError:
+                pass
+            f = _h5py.File(self.fileName, 'w')
+            f['dx'], f['dtheta'], f['dp'], f['dlambda'] = self.dX, self.dTheta, self.dP, self.dLambda
+            f['x_gridDIM'], f['p_gridDIM'] = self.X_gridDIM, self.P_gridDIM
+            f['dt'], f['timeSteps'], f['skipFrames'] = self.dt, self.timeSteps, self.skipFrames
+            return f
+        return None
+
+    def Run(self):
+        torch = _torch()
+        W0 = np.ascontiguousarray(self.W_init, dtype=np.complex128)
+        if W0.shape != (self.P_gridDIM, self.X_gridDIM):
+            raise _lib.WignerArgumentError('W_init must have shape (P_gridDIM, X_gridDIM)')
+        dev = torch.device('cuda', self._device)
+        with torch.cuda.device(dev):
+            W = torch.from_numpy(W0.copy()).to(dev)
+            n_total = int(self.timeSteps) + 1             # Run :1776 loops over 0..timeSteps
+            skip = max(int(self.skipFrames), 1)
+            obs = np.empty((n_total + 1, _lib.WIG_NOBS))
+            self.frames = {}
+            sink = self._frame_sink()
+            saved = []
+            t, cont = 0, False
+            while t < n_total:
+                if t % skip == 0 and t <= self.timeSteps:
+                    if not cont:                           # W must be normalised first
+                        obs[0] = self.propagate(W, 0)[0]
+                        cont = True
+                    frame = W.cpu().numpy()
+                    self.frames[t] = frame
+                    saved.append(t)
+                    if sink is not None:
+                        sink.create_dataset(str(t), data=frame)
+                nxt = min(n_total, (t // skip + 1) * skip)
+                o = self.propagate(W, nxt - t, t_index0=t, continue_run=cont)
+                obs[t:nxt + 1] = o
+                t, cont = nxt, True
+            W_end = W.cpu().numpy()
+        n = int(self.timeSteps) + 1
+        self.timeRange = np.arange(n) * self.dt
+        self.timeRangeIndexSaved = saved
+        self.Norm_average = obs[:n, 0].copy()
+        (self.X_average, self.X2_average, self.P_average, self.P2_average, self.XP_average,
+         self.dPotentialdX_average, self.PdPotentialdX_average, self.XdPotentialdX_average,
+         self.Hamiltonian_average, self.negativeArea) = [obs[:n, k].copy() for k in range(1, 11)]
+        self.W_end_complex = W_end
+        self.W_end = W_end.real.copy()
+        if sink is not None:
+            sink['timeRange'] = self.timeRange
+            sink['timeRangeIndexSaved'] = saved
+            for key, arr in (('X_Ehrenfest', self.X_average), ('X2_Ehrenfest', self.X2_average),
+                             ('P_Ehrenfest', self.P_average), ('P2_Ehrenfest', self.P2_average),
+                             ('XP_Ehrenfest', self.XP_average),
+                             ('dPotentialdX_Ehrenfest', self.dPotentialdX_average),
+                             ('PdPotentialdX_average', self.PdPotentialdX_average),
+                             ('XdPotentialdX_average', self.XdPotentialdX_average),
+                             ('Hamiltonian_average', self.Hamiltonian_average)):
+                sink['/Ehrenfest/' + key] = arr
+            sink['W_init'] = np.asarray(self.W_init).real
+            sink['W_end'] = self.W_end
+            sink['negativeArea'] = self.negativeArea
+            sink.close()
+        return 0
+
+
+class GPU_Wigner2D_ODM2(GPU_Wigner2D_FFT):
+    """Kinetic phase from the kinetic string and two Lindblad terms, one damping
+    and one pumping (``GPU_Wigner2D_FFT.py:1973-2230``)."""
+
+    _odm2 = True
+
+    def __init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass, D_Theta, D_Lambda,
+                 gammaDamping, weightLindbland1, weightLindbland2, potentialString, dPotentialString,
+                 kinematicString, normalization='Wigner'):
+        self.weightLindbland1 = weightLindbland1
+        self.weightLindbland2 = weightLindbland2
+        GPU_Wigner2D_FFT.__init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass,
+                                  D_Theta, D_Lambda, gammaDamping, potentialString, dPotentialString,
+                                  kinematicString, normalization)

@@ -1,0 +1,110 @@
+"""The C-ABI library without a GPU: it loads, exports every symbol the header
+declares, validates descriptors on the host, and its JIT source compiles with
+NVRTC for sm_100a (compile only)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from pywignercuda_b200 import _lib
+from pywignercuda_b200._lib import WigDesc, DiracDesc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, 'include', 'wigner_b200.h')).read()
+    return sorted(set(re.findall(r'^\s*(?:int|const char\*)\s+(\w+)\s*\(', src, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    syms = header_symbols()
+    assert len(syms) >= 12
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert {n for n, _, _ in _lib.SIGNATURES} == set(syms)
+    assert lib.wig_abi_version() == _lib.ABI_VERSION
+
+
+def wig_desc(nx=256, npp=256, **kw):
+    d = WigDesc()
+    d.abi_version = _lib.ABI_VERSION
+    d.n_x, d.n_p = nx, npp
+    d.damping = kw.get('damping', _lib.DAMP_CALDEIRA_LEGGETT)
+    d.x_amplitude = d.p_amplitude = 10.
+    d.hbar = d.mass = 1.
+    d.dt = 0.01
+    d.gamma = kw.get('gamma', 0.1)
+    d.d_theta = 0.1
+    d.potential = kw.get('potential', b'0.05*pow(x,4) - pow(x,2)')
+    d.kinetic = b'0.5*p*p'
+    d.fp_damping = kw.get('fp', b'fabs(p)')
+    return d
+
+
+def jit(d, fn='wig_jit_check'):
+    buf = ctypes.create_string_buffer(1 << 16)
+    rc = getattr(_lib.load(), fn)(d, buf, len(buf))
+    return rc, buf.value.decode()
+
+
+@pytest.mark.parametrize('n', [16, 256, 1024, 4096])
+def test_wigner_jit_compiles(n):
+    rc, log = jit(wig_desc(n, n))
+    assert rc == 0, log
+    assert 'wig_xpass' in log and 'wig_ppass' in log
+    assert '0 bytes spill stores' in log
+
+
+def test_dirac_jit_compiles():
+    d = DiracDesc()
+    d.abi_version = _lib.ABI_VERSION
+    d.n_x = d.n_y = 512
+    d.x_amplitude = d.y_amplitude = 12.
+    d.mass, d.c, d.hbar, d.dt = 1., 137.036, 1., 1e-4
+    d.a0 = b'-1./sqrt(x*x+y*y+0.5)'
+    rc, log = jit(d, 'dirac_jit_check')
+    assert rc == 0, log
+    assert 'dirac_rowpass' in log and 'dirac_colpass' in log
+
+
+@pytest.mark.parametrize('nx,npp', [(100, 256), (256, 8), (8192, 256), (0, 0)])
+def test_bad_grid_rejected_on_host(nx, npp):
+    rc, log = jit(wig_desc(nx, npp))
+    assert rc == 1 and 'powers of two' in log
+
+
+def test_bad_expression_reports_compile_error():
+    rc, log = jit(wig_desc(potential=b'0.5*pow(x,2) + undefined_name'))
+    assert rc == 2 and 'undefined_name' in log
+
+
+@pytest.mark.parametrize('expr', [b'x); } __global__ void k() { (x', b'x;', b'#define', b'((x)'])
+def test_expression_injection_refused(expr):
+    rc, log = jit(wig_desc(potential=expr))
+    assert rc == 1
+
+
+def test_odm_reported_unsupported_when_missing():
+    rc, log = jit(wig_desc(damping=_lib.DAMP_ODM))
+    assert rc in (0, 6)
+
+
+def test_python_classes_fail_loudly_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip('GPU present')
+    from pywignercuda_b200 import GPU_Wigner2D_FFT, WignerCudaError
+
+    class Inst(GPU_Wigner2D_FFT):
+        def __init__(self):
+            self.dampingFunction = 'CaldeiraLeggett'
+            self.grossPitaevskiiCoefficient = 0.
+            self.fp_Damping_String = 'fabs(p)'
+            self.SetTimeTrack(0.01, 10, 100)
+            GPU_Wigner2D_FFT.__init__(self, 256, 256, 10., 10., 1., 1., 0., 0., 0., '0.5*pow(x,2)', 'x',
+                                      '0.5*p*p')
+    with pytest.raises(WignerCudaError):
+        Inst()
