@@ -299,6 +299,63 @@ def run_ours(args, world, rank, local):
     del insts
 
 
+def make_dirac_instance(time_steps):
+    from pywignercuda_b200 import GPU_Dirac2D
+
+    class Coulomb(GPU_Dirac2D):
+        def __init__(self):
+            self.mass, self.c, self.hBar = 1., 137.036, 1.
+            self.Potential_0_String = '-1./sqrt(x*x+y*y+0.5)'
+            self.Potential_1_String = self.Potential_2_String = self.Potential_3_String = '0.'
+            self.fileName = ''
+            GPU_Dirac2D.__init__(self, (512, 512), (12., 12.), 1e-4, time_steps, 10 ** 9)
+    return Coulomb()
+
+
+def run_dirac(args, world, rank, local):
+    """Dirac2D 512x512, c = 137.036, softened Coulomb, packet p0 = (5, 0), dt = 1e-4,
+    complex128, R replicas in lock-step (dirac_run_many)."""
+    import ctypes
+    import torch
+    from pywignercuda_b200 import _lib
+    lib = _lib.load()
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    R = args.replicas
+    insts = [make_dirac_instance(args.steps) for _ in range(R)]
+    P0 = insts[0].Spinor_Particle_SpinUp((5., 0.), lambda x, y: np.exp(-(x * x + y * y) / 2.))
+    Ps = [torch.from_numpy(np.ascontiguousarray(P0, dtype=np.complex128)).to(dev) for _ in range(R)]
+    stream = torch.cuda.current_stream(dev)
+    hs = (ctypes.c_void_p * R)(*[i._handle.value for i in insts])
+    ps = (ctypes.c_void_p * R)(*[p.data_ptr() for p in Ps])
+    _lib.check(lib.dirac_run_many(hs, ps, R, 0, args.warmup, None, stream.cuda_stream), 'warm-up')
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        _lib.check(lib.dirac_run_many(hs, ps, R, args.warmup, args.steps, None, stream.cuda_stream), 'timed')
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = barrier_max(world, e0.elapsed_time(e1))
+    value = world * R * 512 * 512 * args.steps / (ms / 1e3)
+    peak, peak_kind = peaks()
+    achieved = 2 * 512 * 512 * 128 / (ms / 1e3 / (R * args.steps)) / 1e9   # 2 passes x 128 B per point
+    line = {'metric': 'Dirac2D spinor-pt-steps/s', 'value': value, 'unit': 'spinor-pt-steps/s',
+            'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c128',
+            'data': 'synthetic',
+            'config': {'workload': 'Dirac2D 512x512 c=137.036 softened Coulomb, p0=(5,0), dt=1e-4',
+                       'replicas_per_gpu': R,
+                       'l2': 'per-step working set %d MB > 126 MB L2' % (R * 16)},
+            'roofline': {'bound': 'hbm', 'kernel': 'dirac_rowpass+dirac_colpass (step average)',
+                         'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
+                         'peak_kind': peak_kind, 'traffic': None},
+            'gpu_launches': R * (2 * args.steps + 3), 'clocks': clk.summary()}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -307,12 +364,15 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--replicas', type=int, default=REPLICAS)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
+    ap.add_argument('--workload', default='wigner', choices=['wigner', 'dirac'])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
     try:
         if args.impl == 'reference':
             run_reference(args, world, rank)
+        elif args.workload == 'dirac':
+            run_dirac(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -174,6 +174,11 @@ int dirac_create(const dirac_desc* desc, dirac_handle** out);
 int dirac_run(dirac_handle* h, void* psi_dev, int64_t t_index0, int64_t n_steps,
               double* obs_host, void* stream);
 
+/* dirac_run over `count` independent instances stepped in lock-step on one
+ * stream (the Dirac counterpart of wig_run_many). */
+int dirac_run_many(dirac_handle* const* handles, void* const* psi_dev, int64_t count, int64_t t_index0,
+                   int64_t n_steps, double* const* obs_host, void* stream);
+
 /* dirac_run on host buffers (Psi_init upload :1002-1005, Psi_end download :1119). */
 int dirac_run_host(dirac_handle* h, const void* psi_in_host, void* psi_out_host, int64_t t_index0,
                    int64_t n_steps, double* obs_host, void* stream);

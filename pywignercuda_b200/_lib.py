@@ -94,6 +94,8 @@ SIGNATURES = [
     ('wig_destroy', c_int, [c_void_p]),
     ('dirac_create', c_int, [POINTER(DiracDesc), POINTER(c_void_p)]),
     ('dirac_run', c_int, [c_void_p, c_void_p, c_int64, c_int64, _DP, c_void_p]),
+    ('dirac_run_many', c_int, [POINTER(c_void_p), POINTER(c_void_p), c_int64, c_int64, c_int64,
+                               POINTER(_DP), c_void_p]),
     ('dirac_run_host', c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, _DP, c_void_p]),
     ('dirac_destroy', c_int, [c_void_p]),
     ('wig_jit_check', c_int, [POINTER(WigDesc), c_char_p, c_int64]),

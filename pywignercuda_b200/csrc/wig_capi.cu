@@ -303,6 +303,10 @@ struct wig_handle {
   wig_desc d{};
   wig::WigArgs a{};
   CUfunction f_x = nullptr, f_p = nullptr, f_r = nullptr, f_fin = nullptr, f_scale = nullptr;
+  CUfunction f_ox = nullptr, f_op = nullptr;   // ODM passes
+  int odm = 0, smem_odm_x = 0, smem_odm_p = 0;
+  double2* odm_T = nullptr;                    // 5 planes of ODM intermediates
+  double odm_coef[2] = {0., 0.}, odm_sign[2] = {1., -1.};
   int xrows = 1, xnt = 256, pc = 1, pnt = 256, rnt = 256;
   int n_cta_x = 1, n_cta_p = 1, n_cta_r = 1;
   int smem_x = 0, smem_p = 0;
@@ -318,6 +322,8 @@ struct wig_handle {
 // Validation, tiling and the JIT source of one Wigner instance (no CUDA calls).
 struct WigPlan {
   int xrows, xnt, pc, pnt, rnt, n_cta_x, n_cta_p, n_cta_r, smem_x, smem_p, damp;
+  int xminb, pminb;
+  int odm, smem_odm_x, smem_odm_p;
   double dX, dP, dTheta, dLambda;
   std::string src;
 };
@@ -336,26 +342,47 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
     return fail(WIG_ERR_ARG, "unknown constants mode %d", d->constants);
   if (d->precision != WIG_PREC_C128) return fail(WIG_ERR_UNSUPPORTED, "precision %d not available", d->precision);
   const bool damped = d->gamma != 0.;
-  if (damped && d->damping == WIG_DAMP_ODM)
-    return fail(WIG_ERR_UNSUPPORTED, "ODM Lindblad damping is not available in this build");
+  if (damped && d->damping == WIG_DAMP_ODM && (d->n_lindblad < 1 || d->n_lindblad > 2))
+    return fail(WIG_ERR_ARG, "n_lindblad must be 1 or 2");
+  if (damped && d->damping == WIG_DAMP_ODM && !(d->l_material > 0))
+    return fail(WIG_ERR_ARG, "ODM needs l_material > 0");
   const std::string V = expr_or(d->potential, "0."), K = expr_or(d->kinetic, "0.5*p*p"),
                     F = expr_or(d->fp_damping, "fabs(p)");
   if (!safe_expr(V) || !safe_expr(K) || !safe_expr(F))
     return fail(WIG_ERR_ARG, "expression strings may not contain ; { } # quotes or unbalanced ()");
   const int NX = d->n_x, NP = d->n_p, cm = d->constants;
   P->damp = (damped && d->damping == WIG_DAMP_CALDEIRA_LEGGETT) ? 1 : 0;
+  P->odm = (damped && d->damping == WIG_DAMP_ODM) ? 1 : 0;
 
-  // ---- tiling
+  // ---- tiling (defaults; WIG_TILING="xrows,xnt,xminb,pc,pnt,pminb" overrides for tuning runs)
   P->xrows = clampi(2048 / NX, 1, NP);
   P->xnt = round_warp(clampi(P->xrows * NX / 8, 32, 256));
+  P->xminb = 3;
   P->pc = clampi(2048 / NP, 1, NX);
   P->pnt = round_warp(clampi(P->pc * NP / 8, 32, 256));
+  P->pminb = P->damp ? 2 : 3;
+  if (const char* tv = getenv("WIG_TILING")) {
+    int v[6];
+    if (sscanf(tv, "%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]) == 6) {
+      if (v[0] > 0) P->xrows = clampi(v[0], 1, NP);
+      if (v[1] > 0) P->xnt = round_warp(clampi(v[1], 32, 1024));
+      if (v[2] > 0) P->xminb = v[2];
+      if (v[3] > 0) P->pc = clampi(v[3], 1, NX);
+      if (v[4] > 0) P->pnt = round_warp(clampi(v[4], 32, 1024));
+      if (v[5] > 0) P->pminb = v[5];
+    }
+  }
   P->rnt = 256;
   P->n_cta_x = NP / P->xrows;
   P->n_cta_p = NX / P->pc;
   P->n_cta_r = clampi(NX * NP / (4 * P->rnt), 1, 296);
-  P->smem_x = P->xrows * (NX + (NX >> 3)) * (int)sizeof(double2);
-  P->smem_p = (P->damp ? 2 : 1) * P->pc * NP * (int)sizeof(double2);
+  // shared layouts carry one padding slot per 8 elements (wig::padded_size)
+  const int tile_x = wig::padded_size(P->xrows * NX) * (int)sizeof(double2);
+  const int tile_p = wig::padded_size(P->pc * NP) * (int)sizeof(double2);
+  P->smem_x = tile_x;
+  P->smem_p = P->damp ? 2 * tile_p + 2 * NP * (int)sizeof(double) : tile_p;
+  P->smem_odm_x = 2 * tile_x;
+  P->smem_odm_p = 2 * tile_p;
 
   // ---- JIT source
   P->dX = 2. * d->x_amplitude / (double)NX;
@@ -374,9 +401,10 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
   char macros[512];
   snprintf(macros, sizeof(macros),
            "#define WIG_NX %d\n#define WIG_NP %d\n#define WIG_XROWS %d\n#define WIG_XNT %d\n"
-           "#define WIG_XPAD 3\n#define WIG_KIN_STRING %d\n#define WIG_PC %d\n#define WIG_PNT %d\n"
-           "#define WIG_DAMP %d\n#define WIG_RNT %d\n",
-           NX, NP, P->xrows, P->xnt, d->kinetic_from_string ? 1 : 0, P->pc, P->pnt, P->damp, P->rnt);
+           "#define WIG_KIN_STRING %d\n#define WIG_PC %d\n#define WIG_PNT %d\n"
+           "#define WIG_DAMP %d\n#define WIG_RNT %d\n#define WIG_XMINB %d\n#define WIG_PMINB %d\n",
+           NX, NP, P->xrows, P->xnt, d->kinetic_from_string ? 1 : 0, P->pc, P->pnt, P->damp, P->rnt,
+           P->xminb, P->pminb);
   src += macros;
   src += kJitWignerSource;
   P->src.swap(src);
@@ -409,6 +437,7 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   h->xrows = P.xrows; h->xnt = P.xnt; h->pc = P.pc; h->pnt = P.pnt; h->rnt = P.rnt;
   h->n_cta_x = P.n_cta_x; h->n_cta_p = P.n_cta_p; h->n_cta_r = P.n_cta_r;
   h->smem_x = P.smem_x; h->smem_p = P.smem_p;
+  h->odm = P.odm; h->smem_odm_x = P.smem_odm_x; h->smem_odm_p = P.smem_odm_p;
   const double dX = P.dX, dP = P.dP, dTheta = P.dTheta, dLambda = P.dLambda;
   const std::string& src = P.src;
   CUmodule mod;
@@ -420,6 +449,8 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   if (!rc) rc = get_fn(mod, "wig_scale", &h->f_scale, 0);
   CUfunction f_setup = nullptr;
   if (!rc) rc = get_fn(mod, "wig_setup", &f_setup, 0);
+  if (!rc && h->odm) rc = get_fn(mod, "wig_odm_xpass", &h->f_ox, h->smem_odm_x);
+  if (!rc && h->odm) rc = get_fn(mod, "wig_odm_ppass", &h->f_op, h->smem_odm_p);
   if (rc) { delete h; return rc; }
 
   // ---- kernel arguments and tables
@@ -467,7 +498,18 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   if (!rc) rc = B.alloc(&twp_d, NP, twp.data());
   if (!rc) rc = B.alloc(&part_d, (size_t)nparts * wig::NACC);
   if (!rc) rc = B.alloc(&h->scale, 1);
+  std::vector<double> lt = d->lambda_table ? std::vector<double>(d->lambda_table, d->lambda_table + NX)
+                                           : shifted_range(dLambda * NX / 2., NX);
+  double* lam_d = nullptr;
+  if (!rc) rc = B.alloc(&lam_d, NX, lt.data());
+  if (!rc && h->odm) rc = B.alloc(&h->odm_T, 5 * (size_t)NX * NP);
   if (rc) { B.free_all(); delete h; return rc; }
+  a.lambda_tab = lam_d;
+  a.hbar_exact = d->hbar;
+  a.L_material = d->l_material;
+  // _Lindbladian_ODM scale dt*2*gamma*weight/n (n = 1, Order1), with 1/n_p folded in
+  h->odm_coef[0] = d->dt * 2 * d->gamma * d->weight1 / 1. * (1.0 / (double)NP);
+  h->odm_coef[1] = d->dt * 2 * d->gamma * d->weight2 / 1. * (1.0 / (double)NP);
   a.x_tab = x_d; a.p_tab = p_d; a.dV_tab = dv_d; a.V0_tab = v0_d; a.theta_s = ths_d;
   a.r_lambda = rl_d; a.r_theta = rt_d; a.mask1 = m1_d; a.mask2s = m2_d; a.sfp = sfp_d;
   a.tw_x = twx_d; a.tw_p = twp_d; a.partials = part_d; a.n_partials = 0;
@@ -562,6 +604,17 @@ static int wig_run_step(wig_handle* h, WigRunState* S, int64_t n, cudaStream_t s
   double t = (double)(S->t_index0 + n) * h->d.dt;
   void* pargs[] = {&S->a, &S->W, &t};
   if (int rc = launch(h->f_p, h->n_cta_p, h->pnt, h->smem_p, st, pargs)) return rc;
+  if (h->odm) {
+    // Lindbladian_ODM_Order1 (:1637-1643); GPU_Wigner2D_ODM2 applies a damping
+    // (sign +1, weight1) then a pumping (sign -1, weight2) term (:2169-2176)
+    for (int j = 0; j < h->d.n_lindblad; ++j) {
+      void* oxargs[] = {&S->a, &S->W, &h->odm_T};
+      if (int rc = launch(h->f_ox, h->n_cta_x, h->xnt, h->smem_odm_x, st, oxargs)) return rc;
+      double coef = h->odm_coef[j], sign = h->odm_sign[j];
+      void* opargs[] = {&S->a, &S->W, &h->odm_T, &coef, &sign};
+      if (int rc = launch(h->f_op, h->n_cta_p, h->pnt, h->smem_odm_p, st, opargs)) return rc;
+    }
+  }
   if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 2], st));
   S->a.n_partials = h->n_cta_p;
   return WIG_OK;
@@ -725,8 +778,8 @@ static int dirac_plan(const dirac_desc* d, DiracPlan* P) {
   P->snt = 256;
   P->n_row = NY / P->rows;
   P->n_col = NX / P->cc;
-  P->smem_row = 4 * P->rows * (NX + (NX >> 3)) * (int)sizeof(double2);
-  P->smem_col = 4 * P->cc * NY * (int)sizeof(double2);
+  P->smem_row = wig::padded_size(4 * P->rows * NX) * (int)sizeof(double2);
+  P->smem_col = wig::padded_size(4 * P->cc * NY) * (int)sizeof(double2);
   // GPU_Dirac2D.py:312-346
   P->dX = 2. * d->x_amplitude / (double)NX;
   P->dY = 2. * d->y_amplitude / (double)NY;
@@ -748,7 +801,7 @@ static int dirac_plan(const dirac_desc* d, DiracPlan* P) {
   char macros[512];
   snprintf(macros, sizeof(macros),
            "#define DIR_NX %d\n#define DIR_NY %d\n#define DIR_ROWS %d\n#define DIR_RNT %d\n"
-           "#define DIR_PAD 3\n#define DIR_C %d\n#define DIR_CNT %d\n#define DIR_SNT %d\n",
+           "#define DIR_C %d\n#define DIR_CNT %d\n#define DIR_SNT %d\n",
            NX, NY, P->rows, P->rnt, P->cc, P->cnt, P->snt);
   src += macros;
   src += kJitDiracSource;
@@ -834,49 +887,99 @@ extern "C" int dirac_create(const dirac_desc* d, dirac_handle** out) {
   return WIG_OK;
 }
 
-extern "C" int dirac_run(dirac_handle* h, void* psi_dev, int64_t t_index0, int64_t n_steps, double* obs_host,
-                         void* stream) {
+struct DiracRunState {
+  wig::DiracArgs a;
+  double2* psi;
+  int64_t t_index0, n_steps;
+};
+
+static int dirac_run_check(dirac_handle* h, void* psi_dev, int64_t n_steps) {
   if (!h || !psi_dev) return fail(WIG_ERR_ARG, "dirac_run: null handle or psi");
   if (((uintptr_t)psi_dev & 15) != 0) return fail(WIG_ERR_ARG, "dirac_run: psi must be 16-byte aligned");
   if (n_steps < 1) return fail(WIG_ERR_ARG, "dirac_run: n_steps must be >= 1");
   int cur;
   WIG_CUDA(cudaGetDevice(&cur));
   if (cur != h->device) return fail(WIG_ERR_ARG, "dirac_run: current device %d != handle device %d", cur, h->device);
-  cudaStream_t st = (cudaStream_t)stream;
-  const size_t nobs = (size_t)n_steps * DIRAC_NOBS;
-  if (int rc = ensure_obs(&h->obs, &h->obs_cap, nobs)) return rc;
-  double2* psi = (double2*)psi_dev;
-  wig::DiracArgs a = h->a;
+  return ensure_obs(&h->obs, &h->obs_cap, (size_t)n_steps * DIRAC_NOBS);
+}
+
+static int dirac_run_begin(dirac_handle* h, DiracRunState* S, void* psi_dev, int64_t t_index0, int64_t n_steps,
+                           cudaStream_t st) {
+  S->a = h->a;
+  S->psi = (double2*)psi_dev;
+  S->t_index0 = t_index0;
+  S->n_steps = n_steps;
+  int mode = 0, parity = 0;
+  double t_step = 0., t_obs = h->d.dt * (double)(t_index0 + 1);
+  double* obs_row = nullptr;
+  void* args[] = {&S->a, &S->psi, &mode, &parity, &t_step, &t_obs, &obs_row};
+  return launch(h->f_row, h->n_row, h->rnt, h->smem_row, st, args);
+}
+
+static int dirac_run_step(dirac_handle* h, DiracRunState* S, int64_t n, cudaStream_t st) {
+  void* cargs[] = {&S->a, &S->psi};
+  if (int rc = launch(h->f_col, h->n_col, h->cnt, h->smem_col, st, cargs)) return rc;
   const double dt = h->d.dt;
-  int rc;
-  {
-    int mode = 0, parity = 0;
-    double t_step = 0., t_obs = dt * (double)(t_index0 + 1);
-    double* obs_row = nullptr;
-    void* args[] = {&a, &psi, &mode, &parity, &t_step, &t_obs, &obs_row};
-    if ((rc = launch(h->f_row, h->n_row, h->rnt, h->smem_row, st, args))) return rc;
-  }
-  for (int64_t n = 0; n < n_steps; ++n) {
-    void* cargs[] = {&a, &psi};
-    if ((rc = launch(h->f_col, h->n_col, h->cnt, h->smem_col, st, cargs))) return rc;
-    int mode = (n == n_steps - 1) ? 2 : 1, parity = (int)((n + 1) & 1);
-    double t_step = dt * (double)(t_index0 + n + 1), t_obs = dt * (double)(t_index0 + n + 2);
-    double* obs_row = h->obs + (size_t)n * DIRAC_NOBS;
-    void* args[] = {&a, &psi, &mode, &parity, &t_step, &t_obs, &obs_row};
-    if ((rc = launch(h->f_row, h->n_row, h->rnt, h->smem_row, st, args))) return rc;
-  }
-  {
-    int parity = (int)(n_steps & 1);
-    void* args[] = {&a, &parity, &h->scale};
-    if ((rc = launch(h->f_fin, 1, h->snt, 0, st, args))) return rc;
-    long n = 4L * h->d.n_x * h->d.n_y;
-    void* sargs[] = {&psi, &n, &h->scale};
-    if ((rc = launch(h->f_scale, clampi((int)(n / (4 * h->snt)), 1, 592), h->snt, 0, st, sargs))) return rc;
-  }
+  int mode = (n == S->n_steps - 1) ? 2 : 1, parity = (int)((n + 1) & 1);
+  double t_step = dt * (double)(S->t_index0 + n + 1), t_obs = dt * (double)(S->t_index0 + n + 2);
+  double* obs_row = h->obs + (size_t)n * DIRAC_NOBS;
+  void* args[] = {&S->a, &S->psi, &mode, &parity, &t_step, &t_obs, &obs_row};
+  return launch(h->f_row, h->n_row, h->rnt, h->smem_row, st, args);
+}
+
+static int dirac_run_end(dirac_handle* h, DiracRunState* S, cudaStream_t st) {
+  int parity = (int)(S->n_steps & 1);
+  void* args[] = {&S->a, &parity, &h->scale};
+  if (int rc = launch(h->f_fin, 1, h->snt, 0, st, args)) return rc;
+  long n = 4L * h->d.n_x * h->d.n_y;
+  void* sargs[] = {&S->psi, &n, &h->scale};
+  return launch(h->f_scale, clampi((int)(n / (4 * h->snt)), 1, 592), h->snt, 0, st, sargs);
+}
+
+extern "C" int dirac_run(dirac_handle* h, void* psi_dev, int64_t t_index0, int64_t n_steps, double* obs_host,
+                         void* stream) {
+  if (int rc = dirac_run_check(h, psi_dev, n_steps)) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  DiracRunState S;
+  if (int rc = dirac_run_begin(h, &S, psi_dev, t_index0, n_steps, st)) return rc;
+  for (int64_t n = 0; n < n_steps; ++n)
+    if (int rc = dirac_run_step(h, &S, n, st)) return rc;
+  if (int rc = dirac_run_end(h, &S, st)) return rc;
   if (obs_host) {
+    const size_t nobs = (size_t)n_steps * DIRAC_NOBS;
     WIG_CUDA(cudaMemcpyAsync(obs_host, h->obs, nobs * sizeof(double), cudaMemcpyDeviceToHost, st));
     WIG_CUDA(cudaStreamSynchronize(st));
     return check_finite(obs_host, nobs, "dirac_run observables");
+  }
+  return WIG_OK;
+}
+
+extern "C" int dirac_run_many(dirac_handle* const* hs, void* const* psis, int64_t count, int64_t t_index0,
+                              int64_t n_steps, double* const* obs_host, void* stream) {
+  if (!hs || !psis || count < 1) return fail(WIG_ERR_ARG, "dirac_run_many: empty batch");
+  for (int64_t i = 0; i < count; ++i) {
+    if (int rc = dirac_run_check(hs[i], psis[i], n_steps)) return rc;
+    for (int64_t j = 0; j < i; ++j)
+      if (hs[j] == hs[i]) return fail(WIG_ERR_ARG, "dirac_run_many: a handle appears twice");
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<DiracRunState> S((size_t)count);
+  for (int64_t i = 0; i < count; ++i)
+    if (int rc = dirac_run_begin(hs[i], &S[i], psis[i], t_index0, n_steps, st)) return rc;
+  for (int64_t n = 0; n < n_steps; ++n)
+    for (int64_t i = 0; i < count; ++i)
+      if (int rc = dirac_run_step(hs[i], &S[i], n, st)) return rc;
+  for (int64_t i = 0; i < count; ++i)
+    if (int rc = dirac_run_end(hs[i], &S[i], st)) return rc;
+  if (obs_host) {
+    const size_t nobs = (size_t)n_steps * DIRAC_NOBS;
+    for (int64_t i = 0; i < count; ++i)
+      if (obs_host[i])
+        WIG_CUDA(cudaMemcpyAsync(obs_host[i], hs[i]->obs, nobs * sizeof(double), cudaMemcpyDeviceToHost, st));
+    WIG_CUDA(cudaStreamSynchronize(st));
+    for (int64_t i = 0; i < count; ++i)
+      if (obs_host[i])
+        if (int rc = check_finite(obs_host[i], nobs, "dirac_run_many observables")) return rc;
   }
   return WIG_OK;
 }

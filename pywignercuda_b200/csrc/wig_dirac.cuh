@@ -134,11 +134,11 @@ __device__ __forceinline__ double dirac_p_scale(const DiracArgs& a, double (*red
 // Row pass.  mode 0: first (load x-space psi, x sums, row FFT); 1: mid
 // (row IFFT, A, boundary, x sums, row FFT); 2: last (row IFFT, A, boundary,
 // x sums, store x-space).  parity selects the row-sum buffer written.
-template <class Phys, int NX, int NY, int ROWS, int NT, int PAD>
+template <class Phys, int NX, int NY, int ROWS, int NT>
 __device__ __forceinline__ void dirac_row_body(const DiracArgs& a, const Phys& ph, double2* __restrict__ psi,
                                                int mode, int parity, double t_step, double t_obs,
                                                double* obs_row) {
-  typedef RowMap<NX, PAD> M;
+  typedef RowMap<NX> M;
   extern __shared__ double2 sm[];
   __shared__ double red[NT / 32][NACC];
   double scale = 1.0;
@@ -215,7 +215,7 @@ __device__ __forceinline__ void dirac_col_body(const DiracArgs& a, double2* __re
   for (int e = threadIdx.x; e < 4 * C * NY; e += NT) {
     const int k = e / (4 * C), q = e - k * (4 * C);
     const int m = q / C, c = q - m * C;
-    sm[e] = psi[m * comp + (size_t)k * NX + col0 + c];
+    sm[pad8(e)] = psi[m * comp + (size_t)k * NX + col0 + c];
   }
   __syncthreads();
   cta_fft<double2, NY, 4 * C, NT, false, M>(sm, a.tw_y);
@@ -226,8 +226,9 @@ __device__ __forceinline__ void dirac_col_body(const DiracArgs& a, double2* __re
   for (int e = threadIdx.x; e < C * NY; e += NT) {
     const int k = e / C, c = e - k * C;
     const int col = col0 + c;
-    double2* base = sm + k * (4 * C) + c;
-    double2 q1 = base[0], q2 = base[C], q3 = base[2 * C], q4 = base[3 * C];
+    const int i1 = pad8(k * (4 * C) + c), i2 = pad8(k * (4 * C) + C + c);
+    const int i3 = pad8(k * (4 * C) + 2 * C + c), i4 = pad8(k * (4 * C) + 3 * C + c);
+    double2 q1 = sm[i1], q2 = sm[i2], q3 = sm[i3], q4 = sm[i4];
     const double pxe = a.px_tab[col], pye = a.py_tab[k];
     const double r2 = n2(q1) + n2(q2) + n2(q3) + n2(q4);
     acc[0] += r2;
@@ -247,10 +248,10 @@ __device__ __forceinline__ void dirac_col_body(const DiracArgs& a, double2* __re
     cs *= inv_ny;
     const double2 pplus = make_double2(py * sdt, px * sdt);    // (py + i px) sdt
     const double2 pminus = make_double2(py * sdt, -px * sdt);  // (py - i px) sdt
-    base[0] = csub(cscale(q1, cs), cmul(pplus, q4));
-    base[C] = cadd(cscale(q2, cs), cmul(pminus, q3));
-    base[2 * C] = cadd(cmul(make_double2(-pplus.x, -pplus.y), q2), cscale(q3, cs));
-    base[3 * C] = cadd(cmul(pminus, q1), cscale(q4, cs));
+    sm[i1] = csub(cscale(q1, cs), cmul(pplus, q4));
+    sm[i2] = cadd(cscale(q2, cs), cmul(pminus, q3));
+    sm[i3] = cadd(cmul(make_double2(-pplus.x, -pplus.y), q2), cscale(q3, cs));
+    sm[i4] = cadd(cmul(pminus, q1), cscale(q4, cs));
   }
   block_sum<NT, NACC>(acc, red);
   if (threadIdx.x < DNC) a.part_col[(size_t)blockIdx.x * DNC + threadIdx.x] = red[0][threadIdx.x];
@@ -258,7 +259,7 @@ __device__ __forceinline__ void dirac_col_body(const DiracArgs& a, double2* __re
   for (int e = threadIdx.x; e < 4 * C * NY; e += NT) {
     const int k = e / (4 * C), q = e - k * (4 * C);
     const int m = q / C, c = q - m * C;
-    psi[m * comp + (size_t)k * NX + col0 + c] = sm[e];
+    psi[m * comp + (size_t)k * NX + col0 + c] = sm[pad8(e)];
   }
 }
 

@@ -82,20 +82,23 @@ template <int R, bool INV, class C> __device__ __forceinline__ void dft(C* v) {
 }
 
 // ---------------------------------------------------------------- layouts
-// Contiguous rows: sequence b, element k at b*(N + pad) + k + pad(k);
-// PADSH > 0 inserts one slot every 2^PADSH elements (bank-conflict relief for
-// the stride-R writes of the first stage).
-template <int N, int PADSH> struct RowMap {
-  static constexpr int stride = N + (PADSH > 0 ? (N >> PADSH) : 0);
-  __device__ __forceinline__ static int padded(int k) { return PADSH > 0 ? k + (k >> PADSH) : k; }
-  __device__ __forceinline__ static int idx(int b, int k) { return b * stride + padded(k); }
-  // butterfly q -> (sequence, butterfly-in-sequence): consecutive q walk along a row
+// Shared-memory layouts.  Both are a linear order plus one padding slot every
+// 8 elements (phys = lin + lin/8), which spreads the stride-R accesses of the
+// first Stockham stage over distinct 16-byte bank groups.
+__device__ __forceinline__ int pad8(int lin) { return lin + (lin >> 3); }
+__host__ __device__ constexpr int padded_size(int n) { return n + (n >> 3); }
+
+// Contiguous rows: sequence b, element k at lin = b*N + k; consecutive
+// butterflies walk along a row.
+template <int N> struct RowMap {
+  __device__ __forceinline__ static int idx(int b, int k) { return pad8(b * N + k); }
   template <int NBF> __device__ __forceinline__ static void split(int q, int& b, int& j) { b = q / NBF; j = q % NBF; }
 };
 
-// Column tile stored row-major: sequence (column) b, element k at k*NB + b.
+// Column tile stored row-major: sequence (column) b, element k at lin = k*NB + b;
+// consecutive butterflies walk across the columns first.
 template <int NB> struct ColMap {
-  __device__ __forceinline__ static int idx(int b, int k) { return k * NB + b; }
+  __device__ __forceinline__ static int idx(int b, int k) { return pad8(k * NB + b); }
   template <int NBF> __device__ __forceinline__ static void split(int q, int& b, int& j) { b = q % NB; j = q / NB; }
 };
 
@@ -104,15 +107,19 @@ template <int N, int NS> struct Radix {
   static constexpr int value = rem >= 8 ? 8 : (rem >= 4 ? 4 : 2);
 };
 
-// One Stockham stage over all NB sequences.
+// One Stockham stage over all NB sequences.  Phase 1 reads each butterfly's R
+// inputs from shared memory and its R-1 twiddles from the (L1-resident) table,
+// so the twiddle latency overlaps the barrier; phase 2 computes and writes.
 template <class C, int N, int NS, int NB, int NT, bool INV, class Map>
 __device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
   constexpr int R = Radix<N, NS>::value;
   constexpr int NBF = N / R;                 // butterflies per sequence
   constexpr int TOT = NB * NBF;              // butterflies per stage
   constexpr int PER = (TOT + NT - 1) / NT;   // per thread
+  constexpr int TWS = N / (NS * R);          // twiddle-table stride of this stage
   const int tid = threadIdx.x;
   C v[PER][R];
+  C w[PER][R > 1 ? R - 1 : 1];
 #pragma unroll
   for (int m = 0; m < PER; ++m) {
     const int q = tid + m * NT;
@@ -121,6 +128,11 @@ __device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
       Map::template split<NBF>(q, b, j);
 #pragma unroll
       for (int r = 0; r < R; ++r) v[m][r] = s[Map::idx(b, j + r * NBF)];
+      if (NS > 1) {
+        const int k = j & (NS - 1);
+#pragma unroll
+        for (int r = 1; r < R; ++r) w[m][r - 1] = __ldg(&tw[(k * r) * TWS]);
+      }
     }
   }
   __syncthreads();
@@ -133,11 +145,7 @@ __device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
       const int k = j & (NS - 1);
       if (NS > 1) {
 #pragma unroll
-        for (int r = 1; r < R; ++r) {
-          C w = tw[(k * r) * (N / (NS * R))];
-          if (INV) w = cconj(w);
-          v[m][r] = cmul(v[m][r], w);
-        }
+        for (int r = 1; r < R; ++r) v[m][r] = cmul(v[m][r], INV ? cconj(w[m][r - 1]) : w[m][r - 1]);
       }
       dft<R, INV>(v[m]);
       const int d = (j - k) * R + k;

@@ -3,14 +3,14 @@
 // calls, GPU_Dirac2D.py:369-388).  The host prepends a prelude defining the
 // reference's '%f' constants (mass, c, dt, dX, dY, dPx, dPy; :358-367),
 // struct UserPhys { A0..A3(t, x, y) } from Potential_{0..3}_String, and the
-// macros DIR_NX, DIR_NY, DIR_ROWS, DIR_RNT, DIR_PAD, DIR_C, DIR_CNT, DIR_SNT.
+// macros DIR_NX, DIR_NY, DIR_ROWS, DIR_RNT, DIR_C, DIR_CNT, DIR_SNT.
 #pragma once
 #include "wig_dirac.cuh"
 
 extern "C" __global__ void __launch_bounds__(DIR_RNT)
 dirac_rowpass(wig::DiracArgs a, double2* psi, int mode, int parity, double t_step, double t_obs,
               double* obs_row) {
-  wig::dirac_row_body<UserPhys, DIR_NX, DIR_NY, DIR_ROWS, DIR_RNT, DIR_PAD>(
+  wig::dirac_row_body<UserPhys, DIR_NX, DIR_NY, DIR_ROWS, DIR_RNT>(
       a, UserPhys(), psi, mode, parity, t_step, t_obs, obs_row);
 }
 

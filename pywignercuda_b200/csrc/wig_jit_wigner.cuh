@@ -6,18 +6,24 @@
 //     (SetCUDA_Constants :833-842), visible to the user's expressions;
 //   * struct UserPhys { Potential(t, x), KineticEnergy(p), f(p) } built from the
 //     potential, kinetic and damping expression strings;
-//   * the size / tiling macros WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT, WIG_XPAD,
+//   * the size / tiling macros WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT,
 //     WIG_KIN_STRING, WIG_PC, WIG_PNT, WIG_DAMP, WIG_RNT.
 #pragma once
+#ifndef WIG_PMINB
+#define WIG_PMINB 3
+#endif
+#ifndef WIG_XMINB
+#define WIG_XMINB 4
+#endif
 #include "wig_wigner.cuh"
 
-extern "C" __global__ void __launch_bounds__(WIG_XNT)
+extern "C" __global__ void __launch_bounds__(WIG_XNT, WIG_XMINB)
 wig_xpass(wig::WigArgs a, double2* W, int scale_mode, double* obs_row) {
-  wig::xpass_body<UserPhys, WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT, WIG_XPAD, WIG_KIN_STRING != 0>(
+  wig::xpass_body<UserPhys, WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT, WIG_KIN_STRING != 0>(
       a, UserPhys(), W, scale_mode, obs_row);
 }
 
-extern "C" __global__ void __launch_bounds__(WIG_PNT)
+extern "C" __global__ void __launch_bounds__(WIG_PNT, WIG_PMINB)
 wig_ppass(wig::WigArgs a, double2* W, double t) {
   wig::ppass_body<UserPhys, WIG_NX, WIG_NP, WIG_PC, WIG_PNT, WIG_DAMP>(a, UserPhys(), W, t, a.partials);
 }
@@ -35,6 +41,16 @@ wig_finalize(wig::WigArgs a, int mode, double* obs_row, double2* scale_out) {
 extern "C" __global__ void __launch_bounds__(WIG_RNT)
 wig_scale(double2* W, long n, const double2* s) {
   wig::scale_body<WIG_RNT>(W, n, s);
+}
+
+extern "C" __global__ void __launch_bounds__(WIG_XNT)
+wig_odm_xpass(wig::WigArgs a, const double2* W, double2* T) {
+  wig::odm_xpass_body<UserPhys, WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT>(a, UserPhys(), W, T);
+}
+
+extern "C" __global__ void __launch_bounds__(WIG_PNT)
+wig_odm_ppass(wig::WigArgs a, double2* W, const double2* T, double coef, double sign) {
+  wig::odm_ppass_body<WIG_NX, WIG_NP, WIG_PC, WIG_PNT>(a, W, T, coef, sign);
 }
 
 // Per-instance 1-D factor tables, computed on the device with the same

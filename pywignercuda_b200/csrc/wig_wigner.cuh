@@ -52,6 +52,9 @@ struct WigArgs {
   const double2* tw_p;     // [n_p]
   double* partials;        // [n_cta][NACC]
   int n_partials;          // CTAs that wrote `partials`
+  // ODM Lindblad damping (SetA_ODM :1206-1244, _Lindbladian_ODM :1516-1634), exact host values
+  const double* lambda_tab; // [n_x] exact shifted Lambda
+  double hbar_exact, L_material;
 };
 
 // ------------------------------------------------------------------ reductions
@@ -176,10 +179,10 @@ __device__ __forceinline__ void scale_body(double2* __restrict__ W, long n, cons
 }
 
 // x-pass: ROWS rows per CTA.
-template <class Phys, int NX, int NP, int ROWS, int NT, int PAD, bool KIN_STRING>
+template <class Phys, int NX, int NP, int ROWS, int NT, bool KIN_STRING>
 __device__ __forceinline__ void xpass_body(const WigArgs& a, const Phys& ph, double2* __restrict__ W,
                                            int scale_mode, double* obs_row) {
-  typedef RowMap<NX, PAD> M;
+  typedef RowMap<NX> M;
   extern __shared__ double2 sm[];
   __shared__ double red[NT / 32][NACC];
   double2 s = make_double2(1., 0.);
@@ -223,31 +226,40 @@ __device__ __forceinline__ void xpass_body(const WigArgs& a, const Phys& ph, dou
   }
 }
 
-// D(B) = IFFT_p[theta FFT_p(sign(p) f(p) B)] / n_p, in place on the tile.
+// D(B) = IFFT_p[theta FFT_p(sign(p) f(p) B)] / n_p, in place on the tile;
+// sfp / ths are the per-row factor tables staged in shared memory.
 template <int NP, int C, int NT>
-__device__ __forceinline__ void cl_apply_D(const WigArgs& a, double2* B) {
+__device__ __forceinline__ void cl_apply_D(const WigArgs& a, double2* B, const double* sfp, const double* ths) {
   typedef ColMap<C> M;
-  for (int e = threadIdx.x; e < C * NP; e += NT) B[e] = cscale(B[e], a.sfp[e / C]);
+  for (int e = threadIdx.x; e < C * NP; e += NT) B[pad8(e)] = cscale(B[pad8(e)], sfp[e / C]);
   __syncthreads();
   cta_fft<double2, NP, C, NT, false, M>(B, a.tw_p);
-  for (int e = threadIdx.x; e < C * NP; e += NT) B[e] = cscale(B[e], a.theta_s[e / C]);
+  for (int e = threadIdx.x; e < C * NP; e += NT) B[pad8(e)] = cscale(B[pad8(e)], ths[e / C]);
   __syncthreads();
   cta_fft<double2, NP, C, NT, true, M>(B, a.tw_p);
 }
 
 // p-pass: a tile of C columns x NP rows per CTA.  DAMP: 0 none, 1 Caldeira-Leggett.
+// Shared memory: A [padded C*NP], B [padded C*NP] and the two per-row CL
+// tables [2*NP doubles] when DAMP == 1.
 template <class Phys, int NX, int NP, int C, int NT, int DAMP>
 __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, double2* __restrict__ W,
                                            double t, double* __restrict__ partials) {
   typedef ColMap<C> M;
+  constexpr int TILE = padded_size(C * NP);
   extern __shared__ double2 sm[];
   __shared__ double red[NT / 32][NACC];
   double2* A = sm;
-  double2* B = sm + C * NP;
+  double2* B = sm + TILE;
+  double* sfp = reinterpret_cast<double*>(sm + 2 * TILE);
+  double* ths = sfp + NP;
   const int col0 = blockIdx.x * C;
+  if (DAMP == 1) {
+    for (int k = threadIdx.x; k < NP; k += NT) { sfp[k] = a.sfp[k]; ths[k] = a.theta_s[k]; }
+  }
   for (int e = threadIdx.x; e < C * NP; e += NT) {
     const int k = e / C, c = e - k * C;
-    A[e] = W[(size_t)k * NX + col0 + c];
+    A[pad8(e)] = W[(size_t)k * NX + col0 + c];
   }
   __syncthreads();
   cta_fft<double2, NP, C, NT, false, M>(A, a.tw_p);
@@ -263,21 +275,21 @@ __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, dou
     const double r = a.r_theta[k];
     double sn, cs;
     sincos(phase, &sn, &cs);
-    double2 v = cmul(A[e], make_double2(r * cs, -r * sn));
+    double2 v = cmul(A[pad8(e)], make_double2(r * cs, -r * sn));
     v = cscale(v, a.mask1[col]);
     v = cscale(v, a.mask2s[col]);
-    A[e] = v;
+    A[pad8(e)] = v;
   }
   __syncthreads();
   cta_fft<double2, NP, C, NT, true, M>(A, a.tw_p);
   if (DAMP == 1) {
-    for (int e = threadIdx.x; e < C * NP; e += NT) B[e] = A[e];
-    cl_apply_D<NP, C, NT>(a, B);
-    for (int e = threadIdx.x; e < C * NP; e += NT) B[e] = cadd(A[e], cmul(a.cl_k1, B[e]));
-    cl_apply_D<NP, C, NT>(a, B);
-    for (int e = threadIdx.x; e < C * NP; e += NT) B[e] = cadd(A[e], cmul(a.cl_k12, B[e]));
-    cl_apply_D<NP, C, NT>(a, B);
-    for (int e = threadIdx.x; e < C * NP; e += NT) A[e] = cadd(A[e], cmul(a.cl_c3, B[e]));
+    for (int e = threadIdx.x; e < C * NP; e += NT) B[pad8(e)] = A[pad8(e)];
+    cl_apply_D<NP, C, NT>(a, B, sfp, ths);
+    for (int e = threadIdx.x; e < C * NP; e += NT) B[pad8(e)] = cadd(A[pad8(e)], cmul(a.cl_k1, B[pad8(e)]));
+    cl_apply_D<NP, C, NT>(a, B, sfp, ths);
+    for (int e = threadIdx.x; e < C * NP; e += NT) B[pad8(e)] = cadd(A[pad8(e)], cmul(a.cl_k12, B[pad8(e)]));
+    cl_apply_D<NP, C, NT>(a, B, sfp, ths);
+    for (int e = threadIdx.x; e < C * NP; e += NT) A[pad8(e)] = cadd(A[pad8(e)], cmul(a.cl_c3, B[pad8(e)]));
     __syncthreads();
   }
   double acc[NACC];
@@ -286,7 +298,7 @@ __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, dou
   for (int e = threadIdx.x; e < C * NP; e += NT) {
     const int k = e / C, c = e - k * C;
     const int col = col0 + c;
-    const double2 v = A[e];
+    const double2 v = A[pad8(e)];
     W[(size_t)k * NX + col] = v;
     accumulate_obs(acc, v, a.x_tab[col], a.p_tab[k], a.dV_tab[col], a.V0_tab[col], a.mass_exact);
   }
@@ -294,4 +306,119 @@ __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, dou
   if (threadIdx.x < NACC) partials[(size_t)blockIdx.x * NACC + threadIdx.x] = red[0][threadIdx.x];
 }
 
+// ------------------------------------------------------------------ ODM Lindblad
+// g_ODM(p) = sqrt(L f(|p| + hbar/(2L)))  (g_ODM :1196-1197); the five
+// momentum-space factor combinations of _Lindbladian_ODM (:1524-1623), with
+// the two gg terms (:1602-1623) summed: T_k = IFFT_x[FFT_x(W) G_k] / n_x.
+template <class Phys>
+__device__ __forceinline__ double odm_g(const WigArgs& a, const Phys& ph, double p) {
+  return sqrt(a.L_material * ph.f(fabs(p) + a.hbar_exact / (2. * a.L_material)));
+}
+
+__device__ __forceinline__ double sgn(double v) { return v > 0. ? 1. : (v < 0. ? -1. : 0.); }
+
+template <class Phys, int NX, int NP, int ROWS, int NT>
+__device__ __forceinline__ void odm_xpass_body(const WigArgs& a, const Phys& ph, const double2* __restrict__ W,
+                                               double2* __restrict__ T) {
+  typedef RowMap<NX> M;
+  extern __shared__ double2 sm[];
+  double2* F = sm;                                 // FFT_x(W) of the CTA's rows
+  double2* B = sm + padded_size(ROWS * NX);        // one factor combination at a time
+  const int row0 = blockIdx.x * ROWS;
+  const double2* Wb = W + (size_t)row0 * NX;
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    F[M::idx(r, k)] = Wb[e];
+  }
+  __syncthreads();
+  cta_fft<double2, NX, ROWS, NT, false, M>(F, a.tw_x);
+  const double inv_n = 1.0 / (double)NX;
+  const size_t plane = (size_t)NX * NP;
+#pragma unroll 1
+  for (int term = 0; term < 5; ++term) {
+    for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+      const int r = e / NX, k = e - r * NX;
+      const double p = a.p_tab[row0 + r], lam = a.lambda_tab[k];
+      const double pp = p + 0.5 * a.hbar_exact * lam, pm = p - 0.5 * a.hbar_exact * lam;
+      const double gp = odm_g(a, ph, pp), gm = odm_g(a, ph, pm);
+      double m;
+      if (term == 0) m = gp * gm;
+      else if (term == 1) m = gp * (gm * sgn(pm));
+      else if (term == 2) m = (gp * sgn(pp)) * gm;
+      else if (term == 3) m = (gp * sgn(pp)) * (gm * sgn(pm));
+      else m = -0.5 * gp * gp + -0.5 * gm * gm;
+      const int id = M::idx(r, k);
+      B[id] = cscale(F[id], m * inv_n);
+    }
+    __syncthreads();
+    cta_fft<double2, NX, ROWS, NT, true, M>(B, a.tw_x);
+    double2* Tk = T + term * plane + (size_t)row0 * NX;
+    for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+      const int r = e / NX, k = e - r * NX;
+      Tk[e] = B[M::idx(r, k)];
+    }
+    __syncthreads();
+  }
+}
+
+// ODM p-pass: W <- W + coef * IFFT_p[ sum_k trig_k(x, theta) FFT_p(T_k) ]
+// (trig factors of SetA_ODM from the exact X, Theta tables; coef =
+// dt 2 gamma weight / n / n_p folded), then the observable partial sums.
+template <int NX, int NP, int C, int NT>
+__device__ __forceinline__ void odm_ppass_body(const WigArgs& a, double2* __restrict__ W,
+                                               const double2* __restrict__ T, double coef, double sign) {
+  typedef ColMap<C> M;
+  extern __shared__ double2 sm[];
+  __shared__ double red[NT / 32][NACC];
+  double2* Acc = sm;
+  double2* B = sm + padded_size(C * NP);
+  const int col0 = blockIdx.x * C;
+  const size_t plane = (size_t)NX * NP;
+  for (int e = threadIdx.x; e < C * NP; e += NT) Acc[pad8(e)] = make_double2(0., 0.);
+#pragma unroll 1
+  for (int term = 0; term < 5; ++term) {
+    const double2* Tk = T + term * plane;
+    for (int e = threadIdx.x; e < C * NP; e += NT) {
+      const int k = e / C, c = e - k * C;
+      B[pad8(e)] = Tk[(size_t)k * NX + col0 + c];
+    }
+    __syncthreads();
+    cta_fft<double2, NP, C, NT, false, M>(B, a.tw_p);
+    for (int e = threadIdx.x; e < C * NP; e += NT) {
+      const int k = e / C, c = e - k * C;
+      const double X = a.x_tab[col0 + c], Th = a.theta_s[k] * (double)NP;
+      const double xp = X + 0.5 * a.hbar_exact * Th, xm = X - 0.5 * a.hbar_exact * Th;
+      double2 v = B[pad8(e)];
+      if (term == 0) {
+        v = cscale(v, cos(xp) * cos(xm));
+      } else if (term == 1) {
+        v = cscale(cscale(v, cos(xm)), sin(xp));
+        v = cmul(v, make_double2(0., sign));
+      } else if (term == 2) {
+        v = cscale(cscale(v, sin(xm)), cos(xp));
+        v = cmul(v, make_double2(0., -sign));
+      } else if (term == 3) {
+        v = cscale(v, sin(xp) * sin(xm));
+      }
+      Acc[pad8(e)] = cadd(Acc[pad8(e)], v);
+    }
+    __syncthreads();
+  }
+  cta_fft<double2, NP, C, NT, true, M>(Acc, a.tw_p);
+  double acc[NACC];
+#pragma unroll
+  for (int v = 0; v < NACC; ++v) acc[v] = 0.;
+  for (int e = threadIdx.x; e < C * NP; e += NT) {
+    const int k = e / C, c = e - k * C;
+    const int col = col0 + c;
+    const size_t g = (size_t)k * NX + col;
+    const double2 v = cadd(W[g], cscale(Acc[pad8(e)], coef));
+    W[g] = v;
+    accumulate_obs(acc, v, a.x_tab[col], a.p_tab[k], a.dV_tab[col], a.V0_tab[col], a.mass_exact);
+  }
+  block_sum<NT, NACC>(acc, red);
+  if (threadIdx.x < NACC) a.partials[(size_t)blockIdx.x * NACC + threadIdx.x] = red[0][threadIdx.x];
+}
+
 }  // namespace wig
+

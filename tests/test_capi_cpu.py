@@ -87,9 +87,12 @@ def test_expression_injection_refused(expr):
     assert rc == 1
 
 
-def test_odm_reported_unsupported_when_missing():
-    rc, log = jit(wig_desc(damping=_lib.DAMP_ODM))
-    assert rc in (0, 6)
+def test_odm_kernels_compile():
+    d = wig_desc(1024, 1024, damping=_lib.DAMP_ODM, fp=b' p*p/sqrt( p*p + 0.5 ) ')
+    d.n_lindblad, d.l_material = 2, 3.
+    rc, log = jit(d)
+    assert rc == 0, log
+    assert 'wig_odm_xpass' in log and 'wig_odm_ppass' in log
 
 
 def test_python_classes_fail_loudly_without_gpu():
