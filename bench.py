@@ -1,20 +1,30 @@
-"""Benchmark: Wigner2D grid-point-steps per second on B200.
+"""Benchmark: Wigner2D grid-point-steps per second on B200, FP32 batched vs
+plain complex128.
 
-Workload: the 1024x1024 double-well Caldeira-Leggett instance (x, p in
-[-12, 12), V = 0.05x^4 - x^2, gamma = 0.1, kT = 0.5 -> D_theta = 0.1,
-f(p) = |p|, cat state at x = +-3, sigma 0.7, dt = 0.005), complex128, built
-through the public drop-in class.  R = 16 independent replicas are stepped in
-lock-step (wig_run_many): the per-step working set is 16 x 16 MB = 256 MB,
-larger than the 126 MB L2, so no replica's state stays cached between its
-steps.  One bench "step" = one propagation of every replica.
+Headline (value): the FP32 batched form on 64 independent instances --
+square grids drawn from {128, 256, 512, 1024} with numpy default_rng(0),
+V = a x^4 + b x^2 (a ~ U[0.01, 0.1], b ~ U[-1, 0.5]), Caldeira-Leggett
+gamma ~ U[0, 0.2] with D_theta = 2 gamma m kT (kT = 0.5), coherent states at
+x0 ~ U[-2, 2], p0 ~ U[-1, 1], amplitudes 10, dt = 0.005 -- 22.3 M grid points,
+180 MB of complex64 state (larger than the 126 MB L2), all instances in one
+x-pass and one p-pass launch per step, the run replayed as one CUDA graph,
+tile shape from the autotuner.  One bench "step" = one propagation of every
+instance.
+
+Alongside (plain_c128): the complex128 drop-in path on the 1024x1024 double
+well (V = 0.05x^4 - x^2, gamma = 0.1, D_theta = 0.1, f = |p|, cat state,
+dt = 0.005), 16 replicas stepped in lock-step (256 MB > L2); the ratio of the
+two is the metric's "FP32 batched vs plain complex128".  drift_vs_fp64 states
+the FP32 run's norm / energy error against a complex128 run of every instance.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload batch|c128|dirac]
 
-N > 1 (launched by torchrun): every rank runs its own R replicas (weak
-scaling, no data-path collective: the instances are independent); the
-elapsed time is the max over ranks.  --impl reference times the oracle's
-restatement of the reference's propagator (numpy + scipy.fft on all host
-cores) on the same workload; rank 0 only.
+N > 1 (torchrun): each rank runs its own copy of the workload (weak scaling;
+the instances are independent, no data-path collective); time = max over
+ranks.  --impl reference times the oracle's CPU restatement of the reference
+propagator (complex128, numpy + scipy.fft, all host cores) on a sample of the
+same batch; rank 0 only.
 """
 import argparse
 import json
@@ -42,6 +52,7 @@ PASS_BYTES = NX * NP * 16 * 2      # one fused pass reads and writes the c128 gr
 # dram__bytes_read.sum + dram__bytes_write.sum per p-pass launch, from the ncu capture
 # summarised in profiles/wig_ppass_c128_1024.md (None until a capture exists)
 NCU_TRAFFIC_PPASS = None
+NCU_TRAFFIC_BATCH = None
 
 
 def peaks():
@@ -159,6 +170,57 @@ def barrier(world):
         dist.barrier()
 
 
+def batch_config(seed=0, count=64):
+    """The 64-instance mixed-grid batch (see the module docstring)."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice([128, 256, 512, 1024], size=count)
+    a = rng.uniform(0.01, 0.1, count)
+    b = rng.uniform(-1., 0.5, count)
+    g = rng.uniform(0., 0.2, count)
+    x0 = rng.uniform(-2., 2., count)
+    p0 = rng.uniform(-1., 1., count)
+    kT, mass = 0.5, 1.
+    return [dict(n=int(sizes[i]), a=float(a[i]), b=float(b[i]), gamma=float(g[i]),
+                 d_theta=float(2 * g[i] * mass * kT), x0=float(x0[i]), p0=float(p0[i]))
+            for i in range(count)]
+
+
+def coherent_state(n, x0, p0, amp=10.):
+    """Wigner function of the coherent state at (x0, p0), omega = m = hbar = 1,
+    FFT-shifted, normalised (Wigner_HarmonicOscillator with n = 0)."""
+    d = 2. * amp / n
+    g = np.fft.fftshift(np.linspace(-amp, amp - d, n))
+    X, P = g[np.newaxis, :], g[:, np.newaxis]
+    W = np.exp(-((X - x0) ** 2 + (P - p0) ** 2))
+    return W / (W.sum() * d * d)
+
+
+def c128_reference_obs(cases, steps, dev):
+    """complex128 drop-in runs of the batch's instances (exact constants,
+    coefficient slots so one module per grid size): obs[count, steps+1, 11]."""
+    import torch
+    from pywignercuda_b200 import GPU_Wigner2D_FFT, _lib
+
+    class Poly(GPU_Wigner2D_FFT):
+        constants_mode = _lib.CONST_EXACT
+
+        def __init__(self, c):
+            self.dampingFunction, self.grossPitaevskiiCoefficient = 'CaldeiraLeggett', 0.
+            self.fp_Damping_String = 'fabs(p)'
+            self.coefficients = [c['a'], c['b']]
+            self.SetTimeTrack(DT, steps, 10 ** 9, fileName='')
+            GPU_Wigner2D_FFT.__init__(self, c['n'], c['n'], 10., 10., 1., 1., c['d_theta'], 0., c['gamma'],
+                                      'cf[0]*pow(x,4) + cf[1]*pow(x,2)', '4.*cf[0]*pow(x,3) + 2.*cf[1]*x',
+                                      '0.5*p*p')
+    out = []
+    for c in cases:
+        inst = Poly(c)
+        W = torch.from_numpy(coherent_state(c['n'], c['x0'], c['p0']).astype(np.complex128)).to(dev)
+        out.append(inst.propagate(W, steps))
+        del inst
+    return np.array(out)
+
+
 def cpu_baseline_run(max_seconds=20.0, min_steps=2, max_steps=None):
     """The oracle's restatement of the reference's step (numpy + scipy.fft, all
     host cores) on one 1024^2 instance; returns (grid-pt-steps/s, steps, seconds)."""
@@ -180,123 +242,215 @@ def cpu_baseline_run(max_seconds=20.0, min_steps=2, max_steps=None):
     return NX * NP * n / el, n, el, WORKERS
 
 
+def cpu_batch_sample(cases, max_seconds=15.0):
+    """The oracle (complex128, numpy + scipy.fft, all cores) on a sample of the
+    batch: one instance of each grid size, stepped in turn until max_seconds."""
+    from oracle.wigner2d import WignerParams, WignerOracle
+    from oracle.common import WORKERS
+    sample = []
+    for n in (128, 256, 512, 1024):
+        c = next((c for c in cases if c['n'] == n), None)
+        if c is None:
+            continue
+        prm = WignerParams(n, n, 10., 10., DT, potential='%r*pow(x,4) + %r*pow(x,2)' % (c['a'], c['b']),
+                           dpotential='0.', gamma=c['gamma'], d_theta=c['d_theta'], damping='CaldeiraLeggett',
+                           fp_damping='fabs(p)', constants='exact')
+        o = WignerOracle(prm)
+        W = o.initial_normalise(coherent_state(n, c['x0'], c['p0']))
+        W = o.step(W, 0.)                   # warm-up: tables, FFT plans
+        sample.append([o, W, n])
+    pts, steps, t0 = 0, 0, time.perf_counter()
+    while True:
+        for item in sample:
+            o, W, n = item
+            o.observables(W)
+            item[1] = o.step(W, DT)
+            pts += n * n
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= max_seconds and steps >= 2:
+            break
+    return pts / el, steps, el, WORKERS, '%d rounds of one step of a 128/256/512/1024 instance' % steps
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    budget = 150.0
-    # warm-up steps (untimed) then K timed steps, each one propagation of one instance
-    rate, n, el, cores = cpu_baseline_run(max_seconds=min(budget, 1e9), min_steps=args.steps,
-                                          max_steps=args.steps)
+    cases = batch_config()
+    budget = min(120.0, 2.0 * max(args.steps, 1))
+    rate, n, el, cores, what = cpu_batch_sample(cases, max_seconds=budget)
     line = {'metric': METRIC, 'value': rate, 'unit': UNIT, 'n_gpus': args.gpus, 'steps': n,
             'warmup': args.warmup, 'ms_per_step': 1e3 * el / n, 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c128', 'data': 'synthetic',
             'impl': 'reference',
-            'config': {'workload': 'Wigner2D 1024x1024 double well, Caldeira-Leggett, complex128',
-                       'form': 'CPU restatement of GPU_Wigner2D_FFT.Run (numpy + scipy.fft)'},
-            'cpu_baseline': {'value': rate, 'unit': UNIT, 'cores': cores, 'kind': 'port',
-                             'sample': '%d propagations of one 1024x1024 instance' % n},
+            'config': {'workload': 'sample of the 64-instance mixed-grid batch (default_rng(0))',
+                       'form': 'CPU restatement of GPU_Wigner2D_FFT.Run (complex128, numpy + scipy.fft)'},
+            'cpu_baseline': {'value': rate, 'unit': UNIT, 'cores': cores, 'kind': 'port', 'sample': what},
             'e2e': {'value': rate, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line))
 
 
-def run_ours(args, world, rank, local):
+def run_c128(args, world, rank, local, steps=None, emit=True):
+    """The plain complex128 drop-in path on the 1024x1024 double well, R replicas."""
     import ctypes
     import torch
     from pywignercuda_b200 import _lib
     lib = _lib.load()
+    steps = steps or args.steps
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
     R = args.replicas
-    insts = [make_instance(args.steps) for _ in range(R)]
+    insts = [make_instance(steps) for _ in range(R)]
     W0 = cat_state(insts[0])
     Ws = [torch.from_numpy(W0.astype(np.complex128)).to(dev) for _ in range(R)]
     stream = torch.cuda.current_stream(dev)
     hs = (ctypes.c_void_p * R)(*[i._handle.value for i in insts])
     ws = (ctypes.c_void_p * R)(*[w.data_ptr() for w in Ws])
-    obs = [np.empty((args.steps + 1, _lib.WIG_NOBS)) for _ in range(R)]
+    obs = [np.empty((steps + 1, _lib.WIG_NOBS)) for _ in range(R)]
     obs_p = (_lib._DP * R)(*[_lib.dptr(o) for o in obs])
-    warm = [np.empty((args.warmup + 1, _lib.WIG_NOBS)) for _ in range(R)]
-    warm_p = (_lib._DP * R)(*[_lib.dptr(o) for o in warm])
-    _lib.check(lib.wig_run_many(hs, ws, R, 0, args.warmup, 0, warm_p, stream.cuda_stream), 'warm-up')
+    _lib.check(lib.wig_run_many(hs, ws, R, 0, args.warmup, 0, None, stream.cuda_stream), 'warm-up')
     torch.cuda.synchronize()
     barrier(world)
-    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     flags = _lib.WIG_RUN_CONTINUE | _lib.WIG_RUN_PROFILE
     with ClockSampler(local) as clk:
         e0.record(stream)
-        _lib.check(lib.wig_run_many(hs, ws, R, args.warmup, args.steps, flags, obs_p, stream.cuda_stream),
-                   'timed run')
+        _lib.check(lib.wig_run_many(hs, ws, R, args.warmup, steps, flags, obs_p, stream.cuda_stream), 'timed')
         e1.record(stream)
         torch.cuda.synchronize()
-    barrier(world)
     ms = barrier_max(world, e0.elapsed_time(e1))
-    pts_steps = world * R * NX * NP * args.steps
-    value = pts_steps / (ms / 1e3)
-    # per-kernel device time (CUDA events around every launch, same stream)
+    value = world * R * NX * NP * steps / (ms / 1e3)
     x_ms = p_ms = 0.
     launches = 0
     for i in insts:
         out = (ctypes.c_double * 2)()
         cnt = ctypes.c_int64()
         _lib.check(lib.wig_profile(i._handle, out, ctypes.byref(cnt)), 'wig_profile')
-        x_ms += out[0]
-        p_ms += out[1]
-        launches += cnt.value
-    dom, dom_ms = ('wig_ppass', p_ms) if p_ms >= x_ms else ('wig_xpass', x_ms)
-    avg_s = dom_ms / launches / 1e3
+        x_ms, p_ms, launches = x_ms + out[0], p_ms + out[1], launches + cnt.value
     peak, peak_kind = peaks()
-    achieved = PASS_BYTES / avg_s / 1e9
-    # physics check of the timed run: the norm stays 1, no NaN
-    norm_err = max(float(np.max(np.abs(o[:, 0] - 1.))) for o in obs)
-    # ---------------- e2e: host buffers in, host buffers out, through the C ABI
-    hin = [torch.from_numpy(W0.astype(np.complex128)).pin_memory() for _ in range(R)]
-    hout = [torch.empty_like(h).pin_memory() for h in hin]
+    p_gbs = PASS_BYTES / (p_ms / launches / 1e3) / 1e9
+    res = {'value': value, 'unit': UNIT, 'ms_per_step': ms / steps, 'steps': steps, 'replicas': R,
+           'workload': 'Wigner2D 1024x1024 double well V=0.05x^4-x^2, Caldeira-Leggett gamma=0.1 D_theta=0.1 '
+                       'f=|p|, cat state, dt=0.005, complex128',
+           'x_pass_us': x_ms / launches * 1e3, 'p_pass_us': p_ms / launches * 1e3,
+           'p_pass_hbm_frac': p_gbs / peak,
+           'max_abs_norm_error': max(float(np.max(np.abs(o[:, 0] - 1.))) for o in obs),
+           'clocks': clk.summary()}
+    del insts
+    if emit and rank == 0:
+        line = {'metric': 'Wigner2D grid-pt-steps/s (plain complex128)', 'value': value, 'unit': UNIT,
+                'n_gpus': world, 'steps': steps, 'warmup': args.warmup, 'ms_per_step': ms / steps,
+                'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c128',
+                'data': 'synthetic', 'config': {'workload': res['workload'], 'replicas_per_gpu': R},
+                'roofline': {'bound': 'hbm', 'kernel': 'wig_ppass', 'achieved': p_gbs, 'peak': peak,
+                             'unit': 'GB/s', 'frac': p_gbs / peak, 'peak_kind': peak_kind,
+                             'traffic': NCU_TRAFFIC_PPASS},
+                'gpu_launches': R * (2 * steps + 3), 'clocks': res['clocks']}
+        print(json.dumps(line))
+    return res
+
+
+def run_batch(args, world, rank, local):
+    """Headline: the FP32 batched form on the 64-instance mixed-grid batch."""
+    import torch
+    from pywignercuda_b200.batch import WignerBatch, instance
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    cases = batch_config()
+    batch = WignerBatch([instance(c['n'], x_amplitude=10., dt=DT, gamma=c['gamma'], d_theta=c['d_theta'],
+                                  v4=c['a'], v2=c['b']) for c in cases])
+    states = [coherent_state(c['n'], c['x0'], c['p0']) for c in cases]
+    total = batch.total
+    stream = torch.cuda.current_stream(dev)
+    scratch = batch.pack(states)
+    warps, tune_ms = batch.autotune(scratch, probe_steps=3)
+    del scratch
+    K = args.steps
+    W = batch.pack(states)
+    batch.run(W, args.warmup)                                           # normalises
+    batch.run(W, K, continue_run=True, observables=False)               # captures the K-step graph
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        batch.run(W, K, continue_run=True)                              # graph replay; obs D2H included
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = barrier_max(world, e0.elapsed_time(e1))
+    value = world * total * K / (ms / 1e3)
+    if args.profile_only:
+        if rank == 0:
+            print(json.dumps({'metric': METRIC, 'value': value, 'unit': UNIT, 'steps': K, 'warps': warps,
+                              'note': 'profile-only run (timed section only)'}))
+        return
+    # per-pass device time (a short non-graph run with events around every launch)
+    nprof = min(K, 20)
+    batch.run(W, nprof, continue_run=True, graph=False, observables=False, profile=True)
+    x_ms, p_ms, nl = batch.profile()
+    peak, peak_kind = peaks()
+    pass_bytes = total * 8 * 2                                        # complex64 read + write per pass
+    dom, dom_ms = ('wigb_ppass', p_ms) if p_ms >= x_ms else ('wigb_xpass', x_ms)
+    achieved = pass_bytes / (dom_ms / nl / 1e3) / 1e9
+    # FP32 drift against complex128 on every instance (fresh run, same steps)
+    nval = min(K, 200)
+    Wv = batch.pack(states)
+    obs32 = batch.run(Wv, nval, graph=False)
+    obs64 = c128_reference_obs(cases, nval, dev)
+    norm_err = float(np.max(np.abs(obs32[:, :, 0] - obs64[:, :, 0])))
+    e_scale = np.maximum(np.abs(obs64[:, :, 9]), 1e-300)
+    energy_err = float(np.max(np.abs(obs32[:, :, 9] - obs64[:, :, 9]) / e_scale))
+    del Wv
+    # e2e: pinned host state in, run, host state and observables out, all timed
+    hin = torch.from_numpy(np.concatenate([s.astype(np.complex64).ravel() for s in states])).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    Wd = torch.empty(total, dtype=torch.complex64, device=dev)
+    Wd.copy_(hin)
+    batch.run(Wd, K, observables=False)                                 # captures this run's graph
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
-    for w, h in zip(Ws, hin):
-        w.copy_(h, non_blocking=True)
-    _lib.check(lib.wig_run_many(hs, ws, R, 0, args.steps, 0, obs_p, stream.cuda_stream), 'e2e run')
-    for w, h in zip(Ws, hout):
-        h.copy_(w, non_blocking=True)
+    Wd.copy_(hin, non_blocking=True)
+    batch.run(Wd, K)
+    hout.copy_(Wd, non_blocking=True)
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = barrier_max(world, max(f0.elapsed_time(f1), 1e3 * (time.perf_counter() - t0)))
-    grid_bytes = NX * NP * 16
+    c128 = run_c128(args, world, rank, local, steps=min(K, 100), emit=False)
     line = {
-        'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
-        'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
-        'vs_baseline': None, 'dtype': 'c128', 'data': 'synthetic',
-        'config': {'workload': 'Wigner2D 1024x1024 double well V=0.05x^4-x^2, Caldeira-Leggett gamma=0.1 '
-                               'D_theta=0.1 f=|p|, cat state, dt=0.005',
-                   'form': 'plain complex128 (the FP32 batched form is not built yet)',
-                   'replicas_per_gpu': R, 'parallelism': 'independent instances, one process per GPU',
-                   'l2': 'per-step working set %d MB > 126 MB L2' % (R * grid_bytes >> 20),
-                   'max_abs_norm_error': norm_err},
+        'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': K, 'warmup': args.warmup,
+        'ms_per_step': ms / K, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f32 (FP64 phase arguments and observables)', 'data': 'synthetic',
+        'config': {'workload': '64 Wigner2D instances, square grids from {128,256,512,1024} (default_rng(0)), '
+                               'V=a x^4+b x^2, Caldeira-Leggett, coherent states, dt=0.005',
+                   'form': 'FP32 batched, one x-pass + one p-pass launch per step, CUDA graph',
+                   'instances': len(cases), 'grid_points': total, 'warps_per_cta': warps,
+                   'autotune_ms': tune_ms, 'parallelism': 'independent instances, one process per GPU',
+                   'l2': 'state %d MB > 126 MB L2' % (total * 8 >> 20)},
+        'plain_c128': c128,
+        'ratio_fp32_batched_vs_c128': value / c128['value'],
+        'drift_vs_fp64': {'steps': nval, 'norm_max_abs': norm_err, 'energy_max_rel': energy_err,
+                          'reference': 'complex128 drop-in path, exact constants, same instances'},
         'roofline': {'bound': 'hbm', 'kernel': dom, 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                     'frac': achieved / peak, 'peak_kind': peak_kind,
-                     'algorithmic_bytes_per_launch': PASS_BYTES, 'avg_launch_us': avg_s * 1e6,
-                     'x_pass_us': x_ms / launches * 1e3, 'p_pass_us': p_ms / launches * 1e3,
-                     'traffic': NCU_TRAFFIC_PPASS},
-        'e2e': {'value': world * R * NX * NP * args.steps / (e2e_ms / 1e3), 'unit': UNIT,
-                'h2d_bytes_per_step': R * grid_bytes / args.steps,
-                'd2h_bytes_per_step': (R * grid_bytes + R * (args.steps + 1) * 11 * 8) / args.steps,
-                'note': 'one Run()-style call per bench: upload W_init, K propagations, download W_end '
-                        'and the observables; bytes are per propagation step'},
-        'gpu_launches': R * (2 * args.steps + 3),
+                     'frac': achieved / peak, 'peak_kind': peak_kind, 'algorithmic_bytes_per_launch': pass_bytes,
+                     'avg_launch_us': dom_ms / nl * 1e3, 'x_pass_us': x_ms / nl * 1e3, 'p_pass_us': p_ms / nl * 1e3,
+                     'traffic': NCU_TRAFFIC_BATCH},
+        'e2e': {'value': world * total * K / (e2e_ms / 1e3), 'unit': UNIT,
+                'h2d_bytes_per_step': total * 8 / K,
+                'd2h_bytes_per_step': (total * 8 + len(cases) * (K + 1) * 11 * 8) / K,
+                'note': 'one run call: upload the packed states, K propagations, download states and '
+                        'observables; bytes per propagation step'},
+        'gpu_launches': 2 * K + 2,
         'clocks': clk.summary(),
     }
     if rank == 0 and args.cpu_baseline:
-        rate, n, el, cores = cpu_baseline_run(max_seconds=15.0)
+        rate, n, el, cores, what = cpu_batch_sample(cases, max_seconds=15.0)
         line['cpu_baseline'] = {'value': rate, 'unit': UNIT, 'cores': cores, 'kind': 'port',
-                                'sample': '%d propagations of one 1024x1024 instance (%.1f s)' % (n, el)}
+                                'sample': what + ' (%.1f s)' % el}
     if rank == 0:
         print(json.dumps(line))
-    del insts
 
 
 def make_dirac_instance(time_steps):
@@ -364,7 +518,9 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--replicas', type=int, default=REPLICAS)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
-    ap.add_argument('--workload', default='wigner', choices=['wigner', 'dirac'])
+    ap.add_argument('--workload', default='batch', choices=['batch', 'c128', 'dirac'])
+    ap.add_argument('--profile-only', action='store_true',
+                    help='batch workload: only the timed section (for profiler launch lists)')
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -373,8 +529,10 @@ def main():
             run_reference(args, world, rank)
         elif args.workload == 'dirac':
             run_dirac(args, world, rank, local)
+        elif args.workload == 'c128':
+            run_c128(args, world, rank, local)
         else:
-            run_ours(args, world, rank, local)
+            run_batch(args, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -58,11 +58,12 @@ enum wig_constants {
   WIG_CONST_EXACT = 1   /* full double precision                                 */
 };
 
-enum wig_precision { WIG_PREC_C128 = 0 };
+enum wig_precision { WIG_PREC_C128 = 0, WIG_PREC_F32 = 1 };
 
 /* wig_run / dirac_run flags */
 #define WIG_RUN_CONTINUE 1u /* W continues an earlier call: skip the entry normalisation */
 #define WIG_RUN_PROFILE 2u  /* time every x-pass / p-pass launch with CUDA events (wig_profile) */
+#define WIG_RUN_GRAPH 4u    /* wigb_run: capture the launch sequence in a CUDA graph once, replay it */
 
 #define WIG_NOBS 11   /* norm, <x>, <x^2>, <p>, <p^2>, <xp>, <V'>, <pV'>, <xV'>, <H>, negative area */
 #define DIRAC_NOBS 10 /* <x>, <y>, <alpha1>, <alpha2>, <beta>, <K>, <A0>, <px>, <py>, norm_kept */
@@ -98,6 +99,9 @@ typedef struct wig_desc {
   const double* lambda_table;  /* [n_x] */
   const double* dv_table;      /* [n_x] dPotential(0, x) */
   const double* v0_table;      /* [n_x] Potential(0, x)  */
+  /* Values of cf[0] .. cf[7], which the expression strings may use: instances
+   * that differ only in these share one compiled module. */
+  double coef[8];
 } wig_desc;
 
 /* Replaces GPU_Wigner2D_FFT.__init__ (:1718-1751): SetPhaseSpaceBox2D,
@@ -160,6 +164,7 @@ typedef struct dirac_desc {
   const double* y_table;       /* [n_y] shifted Y  */
   const double* px_table;      /* [n_x] shifted Px */
   const double* py_table;      /* [n_y] shifted Py */
+  double coef[8];              /* values of cf[0] .. cf[7] in the expressions */
 } dirac_desc;
 
 /* Replaces GPU_Dirac2D.__init__ (GPU_Dirac2D.py:306-392). */
@@ -184,6 +189,58 @@ int dirac_run_host(dirac_handle* h, const void* psi_in_host, void* psi_out_host,
                    int64_t n_steps, double* obs_host, void* stream);
 
 int dirac_destroy(dirac_handle* h);
+
+/* ---------------------------------------------------------------- batched FP32
+ * Many independent Wigner2D instances with polynomial potentials
+ * V(x) = v4 x^4 + v2 x^2 + v1 x + v0, kinetic p^2/2m, Caldeira-Leggett damping
+ * (gamma != 0) with f(p) = |p| or p^2/sqrt(p^2 + f_eps), on uneven grids
+ * (powers of two in [64, 1024]), advanced together in FP32 complex (W,
+ * FFTs, pointwise factors) with FP64 phase arguments range-reduced before
+ * sincosf and FP64 Kahan-compensated observables.  Constants are exact (no
+ * '%f' rounding).  No counterpart in the reference, which runs one complex128
+ * instance per Run() (GPU_Wigner2D_FFT.py:1843); the step is the same Lie
+ * split (:1884-1913). */
+typedef struct wigb_instance {
+  int32_t n_x, n_p;
+  int32_t damping_f;  /* 0: f = |p|, 1: f = p^2/sqrt(p^2 + f_eps) */
+  int32_t reserved;
+  double x_amplitude, p_amplitude, hbar, mass, dt;
+  double d_theta, d_lambda, gamma, f_eps;
+  double v4, v2, v1, v0;
+} wigb_instance;
+
+typedef struct wigb_handle wigb_handle;
+
+/* warps: tile shape (warps per CTA, 2 / 4 / 8; 0 = 8 until wigb_autotune picks one). */
+int wigb_create(const wigb_instance* instances, int64_t count, int32_t warps, wigb_handle** out);
+
+/* offsets[count + 1]: element offset of each instance's (n_p, n_x) complex64
+ * block in the packed state buffer; offsets[count] = total elements. */
+int wigb_offsets(wigb_handle* h, int64_t* offsets);
+
+/* Normalise (unless flags & WIG_RUN_CONTINUE) and advance every instance of
+ * the packed complex64 state W by n_prop propagations (t = t_index * dt).
+ * obs_host (may be NULL): count x (n_prop + 1) x WIG_NOBS doubles, instance
+ * major.  flags & WIG_RUN_GRAPH: the launch sequence is captured into a CUDA
+ * graph on first use (per W, t_index0, n_prop, flags, tile shape) and replayed. */
+int wigb_run(wigb_handle* h, void* W_dev, int64_t t_index0, int64_t n_prop, uint32_t flags,
+             double* obs_host, void* stream);
+
+/* The project's autotuner: times each candidate tile shape (8, 4, 2 warps per
+ * CTA) on probe_steps steps of the batch using W_scratch (overwritten) and
+ * keeps the fastest; *chosen gets it, ms_out[3] the timings (0 if skipped). */
+int wigb_autotune(wigb_handle* h, void* W_scratch, int64_t probe_steps, int32_t* chosen,
+                  double* ms_out, void* stream);
+
+/* Per-pass device time of the last wigb_run made with WIG_RUN_PROFILE and
+ * without WIG_RUN_GRAPH: ms_out[0] x-pass, ms_out[1] p-pass (summed). */
+int wigb_profile(wigb_handle* h, double* ms_out, int64_t* launches);
+
+int wigb_destroy(wigb_handle* h);
+
+/* Compile-only check (no GPU) of the batched kernels for the given grid sizes
+ * and tile shape; log receives the NVRTC / ptxas report. */
+int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t warps, char* log, int64_t log_cap);
 
 /* Compile-only check of an instance's kernels: builds the JIT source the way
  * wig_create / dirac_create do and compiles it with NVRTC for sm_100a without

@@ -49,6 +49,7 @@ class DiracParams:
     A2: str = '0.'
     A3: str = '0.'
     constants: str = 'cuda_%f'
+    coef: tuple = ()       # values of cf[0..7] in the expression strings
 
     dX: float = field(init=False)
     dY: float = field(init=False)
@@ -66,8 +67,10 @@ class DiracParams:
 
     def kconst(self):
         c = cuda_f if self.constants == 'cuda_%f' else float
+        cv = np.zeros(8)
+        cv[:len(self.coef)] = self.coef
         return dict(mass=c(self.mass), c=c(self.c), dt=c(self.dt), dX=c(self.dX),
-                    dY=c(self.dY), dPx=c(self.dPx), dPy=c(self.dPy))
+                    dY=c(self.dY), dPx=c(self.dPx), dPy=c(self.dPy), cf=cv)
 
 
 class DiracOracle:

@@ -65,6 +65,7 @@ class WignerParams:
     weight1: float = 1.0
     weight2: float = 0.0
     constants: str = 'cuda_%f'             # 'cuda_%f' | 'exact'
+    coef: tuple = ()                       # values of cf[0..7] in the expression strings
 
     # derived (filled by __post_init__)
     dX: float = field(init=False)
@@ -85,7 +86,12 @@ class WignerParams:
         return dict(dt=c(self.dt), dx=c(self.dX), dp=c(self.dP),
                     dtheta=c(self.dTheta), dlambda=c(self.dLambda),
                     mass=c(self.mass), hBar=c(self.hbar),
-                    D_Theta=c(self.d_theta), D_Lambda=c(self.d_lambda))
+                    D_Theta=c(self.d_theta), D_Lambda=c(self.d_lambda), cf=self.cvec())
+
+    def cvec(self):
+        v = np.zeros(8)
+        v[:len(self.coef)] = self.coef
+        return v
 
 
 class Tables:
@@ -105,8 +111,8 @@ class Tables:
                                                   nx))[np.newaxis, :]
         shape = (npp, nx)
         # observable tables, GPU_Wigner2D_FFT.py:583-591,1747,1785-1792
-        dV = eval_expr_like(prm.dpotential, self.X.shape, t=0., x=self.X)
-        V0 = eval_expr_like(prm.potential, self.X.shape, t=0., x=self.X)
+        dV = eval_expr_like(prm.dpotential, self.X.shape, t=0., x=self.X, cf=prm.cvec())
+        V0 = eval_expr_like(prm.potential, self.X.shape, t=0., x=self.X, cf=prm.cvec())
         self.dV_x = dV[0].copy()
         self.V0_x = V0[0].copy()
         self.obs_tables = [
@@ -206,7 +212,7 @@ class WignerOracle:
 
         def g(p):                     # g_ODM :1196-1197
             return np.sqrt(L * eval_expr_like(prm.fp_damping, np.shape(p),
-                                              p=np.abs(p) + hb / (2. * L)))
+                                              p=np.abs(p) + hb / (2. * L), cf=prm.cvec()))
 
         def gs(p):                    # g_sign_ODM :1199-1200
             return g(p) * np.sign(p)

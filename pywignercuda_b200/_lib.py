@@ -17,10 +17,12 @@ WIG_NOBS = 11
 DIRAC_NOBS = 10
 WIG_RUN_CONTINUE = 1
 WIG_RUN_PROFILE = 2
+WIG_RUN_GRAPH = 4
 
 DAMP_NONE, DAMP_CALDEIRA_LEGGETT, DAMP_ODM = 0, 1, 2
 CONST_CUDA_F, CONST_EXACT = 0, 1
 PREC_C128 = 0
+PREC_F32 = 1
 
 
 class WignerError(RuntimeError):
@@ -71,7 +73,14 @@ class WigDesc(ctypes.Structure):
                 ('weight1', c_double), ('weight2', c_double),
                 ('potential', c_char_p), ('kinetic', c_char_p), ('fp_damping', c_char_p),
                 ('x_table', _DP), ('p_table', _DP), ('theta_table', _DP), ('lambda_table', _DP),
-                ('dv_table', _DP), ('v0_table', _DP)]
+                ('dv_table', _DP), ('v0_table', _DP), ('coef', c_double * 8)]
+
+
+class WigbInstance(ctypes.Structure):
+    _fields_ = [('n_x', c_int32), ('n_p', c_int32), ('damping_f', c_int32), ('reserved', c_int32),
+                ('x_amplitude', c_double), ('p_amplitude', c_double), ('hbar', c_double), ('mass', c_double),
+                ('dt', c_double), ('d_theta', c_double), ('d_lambda', c_double), ('gamma', c_double),
+                ('f_eps', c_double), ('v4', c_double), ('v2', c_double), ('v1', c_double), ('v0', c_double)]
 
 
 class DiracDesc(ctypes.Structure):
@@ -80,7 +89,8 @@ class DiracDesc(ctypes.Structure):
                 ('x_amplitude', c_double), ('y_amplitude', c_double), ('mass', c_double),
                 ('c', c_double), ('hbar', c_double), ('dt', c_double),
                 ('a0', c_char_p), ('a1', c_char_p), ('a2', c_char_p), ('a3', c_char_p),
-                ('x_table', _DP), ('y_table', _DP), ('px_table', _DP), ('py_table', _DP)]
+                ('x_table', _DP), ('y_table', _DP), ('px_table', _DP), ('py_table', _DP),
+                ('coef', c_double * 8)]
 
 
 # (name, restype, argtypes) of every symbol include/wigner_b200.h declares
@@ -100,6 +110,13 @@ SIGNATURES = [
     ('dirac_destroy', c_int, [c_void_p]),
     ('wig_jit_check', c_int, [POINTER(WigDesc), c_char_p, c_int64]),
     ('dirac_jit_check', c_int, [POINTER(DiracDesc), c_char_p, c_int64]),
+    ('wigb_create', c_int, [c_void_p, c_int64, c_int32, POINTER(c_void_p)]),
+    ('wigb_offsets', c_int, [c_void_p, POINTER(c_int64)]),
+    ('wigb_run', c_int, [c_void_p, c_void_p, c_int64, c_int64, c_uint32, _DP, c_void_p]),
+    ('wigb_autotune', c_int, [c_void_p, c_void_p, c_int64, POINTER(c_int32), _DP, c_void_p]),
+    ('wigb_profile', c_int, [c_void_p, _DP, POINTER(c_int64)]),
+    ('wigb_destroy', c_int, [c_void_p]),
+    ('wigb_jit_check', c_int, [POINTER(c_int32), c_int64, c_int32, c_char_p, c_int64]),
     ('wig_last_error', c_char_p, []),
     ('wig_abi_version', c_int, []),
 ]

@@ -21,7 +21,8 @@ CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libwigner_b200.so')
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 
-JIT_SOURCES = {'kJitWignerSource': 'wig_jit_wigner.cuh', 'kJitDiracSource': 'wig_jit_dirac.cuh'}
+JIT_SOURCES = {'kJitWignerSource': 'wig_jit_wigner.cuh', 'kJitDiracSource': 'wig_jit_dirac.cuh',
+               'kJitBatchSource': 'wig_jit_batch.cuh'}
 
 
 def inline(fn, seen=None):

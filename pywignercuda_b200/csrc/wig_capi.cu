@@ -30,6 +30,7 @@
 
 #include "../../include/wigner_b200.h"
 #include "wig_dirac.cuh"
+#include "wig_batch.cuh"
 #include "wig_device_src.inc"   // kJitWignerSource, kJitDiracSource (generated by build.py)
 
 namespace {
@@ -394,7 +395,7 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
       {"mass", d->mass}, {"hBar", d->hbar}, {"D_Theta", d->d_theta}, {"D_Lambda", d->d_lambda}};
   std::string src = kMathPrelude;
   for (auto& c : consts) src += "__constant__ double " + std::string(c.name) + "=" + fmt_const(c.v, cm) + ";";
-  src += "\nstruct UserPhys {\n";
+  src += "\nstruct UserPhys {\n  double cf[8];\n";
   src += "  __device__ __forceinline__ double Potential(double t, double x) const { return (" + V + "); }\n";
   src += "  __device__ __forceinline__ double KineticEnergy(double p) const { return (" + K + "); }\n";
   src += "  __device__ __forceinline__ double f(double p) const { return (" + F + "); }\n};\n";
@@ -507,6 +508,7 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   a.lambda_tab = lam_d;
   a.hbar_exact = d->hbar;
   a.L_material = d->l_material;
+  for (int i = 0; i < 8; ++i) a.coef[i] = d->coef[i];
   // _Lindbladian_ODM scale dt*2*gamma*weight/n (n = 1, Order1), with 1/n_p folded in
   h->odm_coef[0] = d->dt * 2 * d->gamma * d->weight1 / 1. * (1.0 / (double)NP);
   h->odm_coef[1] = d->dt * 2 * d->gamma * d->weight2 / 1. * (1.0 / (double)NP);
@@ -514,7 +516,7 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   a.r_lambda = rl_d; a.r_theta = rt_d; a.mask1 = m1_d; a.mask2s = m2_d; a.sfp = sfp_d;
   a.tw_x = twx_d; a.tw_p = twp_d; a.partials = part_d; a.n_partials = 0;
   {
-    void* args[] = {&rl_d, &rt_d, &m1_d, &m2_d, &sfp_d};
+    void* args[] = {&a, &rl_d, &rt_d, &m1_d, &m2_d, &sfp_d};
     rc = launch(f_setup, 8, 256, 0, 0, args);
     if (!rc) {
       cudaError_t e = cudaDeviceSynchronize();
@@ -792,7 +794,7 @@ static int dirac_plan(const dirac_desc* d, DiracPlan* P) {
                                                       {"dPy", P->dPy}};
   std::string src = kMathPrelude;
   for (auto& c : consts) src += "__constant__ double " + std::string(c.name) + "=" + fmt_const(c.v, cm) + ";";
-  src += "\nstruct UserPhys {\n";
+  src += "\nstruct UserPhys {\n  double cf[8];\n";
   const std::string* As[4] = {&A0, &A1, &A2, &A3};
   for (int i = 0; i < 4; ++i)
     src += "  __device__ __forceinline__ double A" + std::to_string(i) +
@@ -874,6 +876,7 @@ extern "C" int dirac_create(const dirac_desc* d, dirac_handle** out) {
   a.x_tab = x_d; a.y_tab = y_d; a.px_tab = px_d; a.py_tab = py_d; a.bx = bx_d; a.by = by_d;
   a.tw_x = twx_d; a.tw_y = twy_d; a.part_row[0] = pr0; a.part_row[1] = pr1; a.part_col = pc;
   a.n_row_cta = h->n_row; a.n_col_cta = h->n_col;
+  for (int i = 0; i < 8; ++i) a.coef[i] = d->coef[i];
   {
     void* args[] = {&bx_d, &by_d};
     rc = launch(f_setup, 8, 256, 0, 0, args);
@@ -1017,3 +1020,400 @@ extern "C" int dirac_destroy(dirac_handle* h) {
 
 extern "C" const char* wig_last_error(void) { return g_last_error.c_str(); }
 extern "C" int wig_abi_version(void) { return WIG_ABI_VERSION; }
+
+// ======================================================================== batched FP32
+// Many independent Wigner2D instances (polynomial potentials, uneven grids) in
+// one x-pass and one p-pass launch per step; see wig_batch.cuh.  A run can be
+// captured once into a CUDA graph (WIG_RUN_GRAPH) and replayed; the tile shape
+// (warps per CTA) is chosen by wigb_autotune from timed candidates.
+namespace {
+PFN_cuOccupancyMaxActiveBlocksPerMultiprocessor g_occ = nullptr;
+
+struct BVariant {
+  int warps = 0;
+  CUfunction fx = nullptr, fp = nullptr, fr = nullptr, fs = nullptr;
+  int smem_x = 0, smem_p = 0, occ_x = 1, occ_p = 1;
+};
+
+int batch_smem_x(int n, int warps) {
+  const int spw = wig::spw_of(n);
+  return (n + (n + 1) / 2 + warps * spw * wig::seq_stride32(n)) * (int)sizeof(float2);
+}
+int batch_smem_p(int n, int warps, bool damped) {
+  const int spw = wig::spw_of(n);
+  const int cs = wig::seq_stride32(n) + 1;
+  return (n + (3 * n + 1) / 2 + (damped ? 2 : 1) * warps * spw * cs) * (int)sizeof(float2);
+}
+}  // namespace
+
+struct wigb_handle {
+  int device = 0, count = 0, n_sm = 148;
+  std::vector<wigb_instance> inst;
+  std::vector<wig::BInst> binst;
+  std::vector<int> classes;
+  int64_t total = 0;
+  std::vector<int64_t> offsets;
+  wig::BArgs a{};
+  int n_xitems = 0, n_pitems = 0, grid_x = 1, grid_p = 1;
+  DevBuf bufs;                      // tables that do not depend on the tile shape
+  void* items_d = nullptr;          // x-items then p-items (int2), per tile shape
+  double* partials_d = nullptr;
+  std::map<int, BVariant> variants; // by warps per CTA
+  int warps = 0;
+  double* obs = nullptr;
+  size_t obs_cap = 0;
+  cudaGraphExec_t gexec = nullptr;  // cached graph of the last WIG_RUN_GRAPH run
+  void* g_W = nullptr;
+  int64_t g_t0 = -1, g_n = -1;
+  uint32_t g_flags = 0;
+  int g_warps = -1;
+  void* g_stream = nullptr;
+  std::vector<cudaEvent_t> ev;      // WIG_RUN_PROFILE (non-graph runs): 3 events per step
+  size_t ev_used = 0;
+};
+
+static std::string wigb_source(const std::vector<int>& classes, int warps) {
+  char head[128];
+  snprintf(head, sizeof(head), "#define WIGB_WARPS %d\n#define WIGB_CASES(F)", warps);
+  std::string src = head;
+  for (int n : classes) src += " F(" + std::to_string(n) + ")";
+  src += "\n";
+  src += kJitBatchSource;
+  return src;
+}
+
+extern "C" int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t warps, char* log, int64_t log_cap) {
+  if (!sizes || n_sizes < 1 || (warps != 2 && warps != 4 && warps != 8)) {
+    fail(WIG_ERR_ARG, "wigb_jit_check: bad arguments");
+    copy_log(g_last_error, log, log_cap);
+    return WIG_ERR_ARG;
+  }
+  std::vector<int> cls(sizes, sizes + n_sizes);
+  std::sort(cls.begin(), cls.end());
+  cls.erase(std::unique(cls.begin(), cls.end()), cls.end());
+  std::lock_guard<std::mutex> lk(g_mu);
+  std::vector<char> cubin;
+  std::string lg;
+  int rc = nvrtc_compile(wigb_source(cls, warps), &cubin, &lg, true);
+  copy_log(rc ? g_last_error : lg, log, log_cap);
+  return rc;
+}
+
+static int wigb_compile(wigb_handle* h, int warps, BVariant* v) {
+  const std::string src = wigb_source(h->classes, warps);
+  bool any_damped = false;
+  for (auto& b : h->binst) any_damped |= b.damp != 0;
+  int smx = 0, smp = 0;
+  for (int n : h->classes) {
+    smx = std::max(smx, batch_smem_x(n, warps));
+    smp = std::max(smp, batch_smem_p(n, warps, any_damped));
+  }
+  if (smx > 227 * 1024 || smp > 227 * 1024)
+    return fail(WIG_ERR_ARG, "batched tile of %d warps needs %d / %d bytes of shared memory", warps, smx, smp);
+  CUmodule mod;
+  int rc = get_module(src, h->device, &mod);
+  if (!rc) rc = get_fn(mod, "wigb_xpass", &v->fx, smx);
+  if (!rc) rc = get_fn(mod, "wigb_ppass", &v->fp, smp);
+  if (!rc) rc = get_fn(mod, "wigb_reduce", &v->fr, 0);
+  if (!rc) rc = get_fn(mod, "wigb_scale", &v->fs, 0);
+  if (rc) return rc;
+  v->warps = warps;
+  v->smem_x = smx;
+  v->smem_p = smp;
+  if (!g_occ) entry("cuOccupancyMaxActiveBlocksPerMultiprocessor", g_occ);
+  if (g_occ) {
+    g_occ(&v->occ_x, v->fx, warps * 32, smx);
+    g_occ(&v->occ_p, v->fp, warps * 32, smp);
+  }
+  v->occ_x = std::max(v->occ_x, 1);
+  v->occ_p = std::max(v->occ_p, 1);
+  return WIG_OK;
+}
+
+// Work lists for a tile of `warps` warps: x-items of warps*spw(n_x) rows,
+// p-items of warps*spw(n_p) columns; p-items of each instance contiguous
+// (the last-CTA reduction reads them as a range), instances ordered by
+// decreasing per-item cost so the persistent loop ends balanced.
+static int wigb_set_warps(wigb_handle* h, int warps) {
+  auto it = h->variants.find(warps);
+  if (it == h->variants.end()) {
+    BVariant v;
+    if (int rc = wigb_compile(h, warps, &v)) return rc;
+    it = h->variants.emplace(warps, v).first;
+  }
+  const BVariant& v = it->second;
+  std::vector<int> order(h->count);
+  for (int i = 0; i < h->count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (int64_t)h->binst[a].n_p * (h->binst[a].damp ? 4 : 1) > (int64_t)h->binst[b].n_p * (h->binst[b].damp ? 4 : 1);
+  });
+  std::vector<int2> xi, pi;
+  for (int i : order) {
+    wig::BInst& b = h->binst[i];
+    const int rpb = warps * wig::spw_of(b.n_x), cpb = warps * wig::spw_of(b.n_p);
+    if (b.n_p % rpb || b.n_x % cpb)
+      return fail(WIG_ERR_ARG, "instance %d: grid %d x %d does not tile with %d warps", i, b.n_x, b.n_p, warps);
+    b.xitem0 = (int)xi.size();
+    b.n_xitems = b.n_p / rpb;
+    for (int r = 0; r < b.n_p; r += rpb) xi.push_back(make_int2(i, r));
+    b.pitem0 = (int)pi.size();
+    b.n_pitems = b.n_x / cpb;
+    for (int c = 0; c < b.n_x; c += cpb) pi.push_back(make_int2(i, c));
+  }
+  if (h->items_d) cudaFree(h->items_d);
+  if (h->partials_d) cudaFree(h->partials_d);
+  h->items_d = nullptr;
+  h->partials_d = nullptr;
+  WIG_CUDA(cudaMalloc(&h->items_d, (xi.size() + pi.size()) * sizeof(int2)));
+  WIG_CUDA(cudaMemcpy(h->items_d, xi.data(), xi.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  WIG_CUDA(cudaMemcpy((int2*)h->items_d + xi.size(), pi.data(), pi.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  WIG_CUDA(cudaMalloc((void**)&h->partials_d, pi.size() * wig::NACC * sizeof(double)));
+  WIG_CUDA(cudaMemcpy((void*)h->a.inst, h->binst.data(), h->binst.size() * sizeof(wig::BInst), cudaMemcpyHostToDevice));
+  h->a.xitems = (const int2*)h->items_d;
+  h->a.pitems = (const int2*)h->items_d + xi.size();
+  h->a.partials = h->partials_d;
+  h->n_xitems = (int)xi.size();
+  h->n_pitems = (int)pi.size();
+  h->grid_x = std::max(1, std::min(h->n_xitems, h->n_sm * v.occ_x));
+  h->grid_p = std::max(1, std::min(h->n_pitems, h->n_sm * v.occ_p));
+  h->warps = warps;
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  return WIG_OK;
+}
+
+extern "C" int wigb_destroy(wigb_handle* h) {
+  if (!h) return WIG_OK;
+  cudaDeviceSynchronize();
+  for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  h->bufs.free_all();
+  if (h->items_d) cudaFree(h->items_d);
+  if (h->partials_d) cudaFree(h->partials_d);
+  if (h->obs) cudaFree(h->obs);
+  delete h;
+  return WIG_OK;
+}
+
+extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t warps, wigb_handle** out) {
+  if (!inst || !out || count < 1) return fail(WIG_ERR_ARG, "wigb_create: empty batch");
+  *out = nullptr;
+  for (int64_t i = 0; i < count; ++i) {
+    const wigb_instance& d = inst[i];
+    if (d.n_x < 64 || d.n_x > 1024 || d.n_p < 64 || d.n_p > 1024 || (d.n_x & (d.n_x - 1)) || (d.n_p & (d.n_p - 1)))
+      return fail(WIG_ERR_ARG, "instance %lld: grid %d x %d, batched grids must be powers of two in [64, 1024]",
+                  (long long)i, d.n_x, d.n_p);
+    if (!(d.x_amplitude > 0) || !(d.p_amplitude > 0) || !(d.hbar != 0) || !(d.mass != 0) || !std::isfinite(d.dt))
+      return fail(WIG_ERR_ARG, "instance %lld: amplitudes > 0, hbar and mass nonzero, dt finite", (long long)i);
+    if (d.damping_f != 0 && d.damping_f != 1)
+      return fail(WIG_ERR_ARG, "instance %lld: damping_f must be 0 (|p|) or 1 (p^2/sqrt(p^2+eps))", (long long)i);
+  }
+  if (warps != 0 && warps != 2 && warps != 4 && warps != 8)
+    return fail(WIG_ERR_ARG, "wigb_create: warps must be 0 (default 8), 2, 4 or 8");
+  int device = 0;
+  WIG_CUDA(cudaGetDevice(&device));
+  WIG_CUDA(cudaFree(0));
+  wigb_handle* h = new wigb_handle();
+  h->device = device;
+  h->count = (int)count;
+  h->inst.assign(inst, inst + count);
+  cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, device);
+  std::vector<int> cls;
+  for (auto& d : h->inst) { cls.push_back(d.n_x); cls.push_back(d.n_p); }
+  std::sort(cls.begin(), cls.end());
+  cls.erase(std::unique(cls.begin(), cls.end()), cls.end());
+  h->classes = cls;
+  std::vector<float2> tw;
+  std::map<int, int> tw_off;
+  for (int n : cls) {
+    tw_off[n] = (int)tw.size();
+    for (auto& z : twiddles(n)) tw.push_back(make_float2((float)z.x, (float)z.y));
+  }
+  h->binst.resize(count);
+  h->offsets.resize(count + 1);
+  int64_t off = 0;
+  for (int64_t i = 0; i < count; ++i) {
+    const wigb_instance& d = h->inst[i];
+    wig::BInst& b = h->binst[i];
+    memset(&b, 0, sizeof(b));
+    b.n_x = d.n_x; b.n_p = d.n_p;
+    b.damp = d.gamma != 0. ? 1 : 0;
+    b.ff = d.damping_f;
+    b.off = off;
+    h->offsets[i] = off;
+    off += (int64_t)d.n_x * d.n_p;
+    b.tw_x = tw_off[d.n_x]; b.tw_p = tw_off[d.n_p];
+    b.dt = d.dt; b.hbar = d.hbar; b.mass = d.mass;
+    b.dx = 2. * d.x_amplitude / d.n_x; b.dp = 2. * d.p_amplitude / d.n_p;
+    b.dtheta = 2. * M_PI / (2. * d.p_amplitude); b.dlambda = 2. * M_PI / (2. * d.x_amplitude);
+    b.D_theta = d.d_theta; b.D_lambda = d.d_lambda; b.f_eps = d.f_eps;
+    b.v4 = d.v4; b.v2 = d.v2; b.v1 = d.v1; b.v0 = d.v0;
+    // CaldeiraDissipatorOrder3 (GPU_Wigner2D_FFT.py:1145-1157) in Horner form, imaginary parts
+    const double g = d.dt * d.gamma, c1 = 2. / 3. * g, c2 = g, c3 = 2. * g;
+    b.cl_k1 = (c1 + c2) != 0. ? c1 * c2 / (c1 + c2) : 0.;
+    b.cl_k12 = c1 + c2;
+    b.cl_c3 = c3;
+  }
+  h->total = off;
+  h->offsets[count] = off;
+  DevBuf& B = h->bufs;
+  float2* tw_d = nullptr;
+  wig::BInst* inst_d = nullptr;
+  unsigned* cnt_d = nullptr;
+  double2* scale_d = nullptr;
+  int rc = B.alloc(&tw_d, tw.size(), tw.data());
+  if (!rc) rc = B.alloc(&inst_d, (size_t)count);
+  if (!rc) rc = B.alloc(&cnt_d, (size_t)count);
+  if (!rc) rc = B.alloc(&scale_d, (size_t)count);
+  if (!rc) {
+    cudaError_t e = cudaMemset(cnt_d, 0, count * sizeof(unsigned));
+    if (e != cudaSuccess) rc = fail(WIG_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
+  }
+  if (rc) { B.free_all(); delete h; return rc; }
+  h->a.tw = tw_d;
+  h->a.inst = inst_d;
+  h->a.counters = cnt_d;
+  h->a.scale = scale_d;
+  if ((rc = wigb_set_warps(h, warps ? warps : 8))) { wigb_destroy(h); return rc; }
+  *out = h;
+  return WIG_OK;
+}
+
+extern "C" int wigb_offsets(wigb_handle* h, int64_t* offsets) {
+  if (!h || !offsets) return fail(WIG_ERR_ARG, "wigb_offsets: null argument");
+  for (int i = 0; i <= h->count; ++i) offsets[i] = h->offsets[i];
+  return WIG_OK;
+}
+
+static int wigb_launch_run(wigb_handle* h, float2* W, int64_t t_index0, int64_t n_prop, uint32_t flags,
+                           cudaStream_t st) {
+  const BVariant& v = h->variants[h->warps];
+  wig::BArgs a = h->a;
+  a.W = W;
+  a.obs = h->obs;
+  a.obs_stride = (int)(n_prop + 1);
+  const int nt = v.warps * 32;
+  int nxi = h->n_xitems, npi = h->n_pitems;
+  {
+    int mode = (flags & WIG_RUN_CONTINUE) ? 0 : 1, sample = 0;
+    void* args[] = {&a, &npi, &mode, &sample};
+    if (int rc = launch(v.fr, h->grid_p, nt, 0, st, args)) return rc;
+  }
+  const bool prof = (flags & WIG_RUN_PROFILE) && !(flags & WIG_RUN_GRAPH);
+  if (prof) {
+    while (h->ev.size() < 3 * (size_t)n_prop) {
+      cudaEvent_t e;
+      WIG_CUDA(cudaEventCreate(&e));
+      h->ev.push_back(e);
+    }
+    h->ev_used = 3 * (size_t)n_prop;
+  }
+  for (int64_t n = 0; n < n_prop; ++n) {
+    if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n], st));
+    void* xargs[] = {&a, &nxi};
+    if (int rc = launch(v.fx, h->grid_x, nt, v.smem_x, st, xargs)) return rc;
+    if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 1], st));
+    double t = (double)(t_index0 + n);   // time index (the polynomial potential is time independent)
+    int sample = (int)(n + 1);
+    void* pargs[] = {&a, &npi, &t, &sample};
+    if (int rc = launch(v.fp, h->grid_p, nt, v.smem_p, st, pargs)) return rc;
+    if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 2], st));
+  }
+  void* sargs[] = {&a, &npi};
+  return launch(v.fs, h->grid_p, nt, 0, st, sargs);
+}
+
+extern "C" int wigb_run(wigb_handle* h, void* W_dev, int64_t t_index0, int64_t n_prop, uint32_t flags,
+                        double* obs_host, void* stream) {
+  if (!h || !W_dev) return fail(WIG_ERR_ARG, "wigb_run: null handle or W");
+  if (((uintptr_t)W_dev & 15) != 0) return fail(WIG_ERR_ARG, "wigb_run: W must be 16-byte aligned");
+  if (n_prop < 0) return fail(WIG_ERR_ARG, "wigb_run: n_prop < 0");
+  int cur;
+  WIG_CUDA(cudaGetDevice(&cur));
+  if (cur != h->device) return fail(WIG_ERR_ARG, "wigb_run: current device %d != handle device %d", cur, h->device);
+  const size_t nobs = (size_t)h->count * (n_prop + 1) * WIG_NOBS;
+  if (nobs > h->obs_cap) {
+    if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+    if (int rc = ensure_obs(&h->obs, &h->obs_cap, nobs)) return rc;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  float2* W = (float2*)W_dev;
+  if (flags & WIG_RUN_GRAPH) {
+    const uint32_t key_flags = flags & ~(uint32_t)WIG_RUN_GRAPH;
+    if (!(h->gexec && h->g_W == W_dev && h->g_t0 == t_index0 && h->g_n == n_prop && h->g_flags == key_flags &&
+          h->g_warps == h->warps)) {
+      if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+      cudaStream_t cap;
+      WIG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+      cudaGraph_t g;
+      cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+      int rc = e == cudaSuccess ? wigb_launch_run(h, W, t_index0, n_prop, key_flags, cap)
+                                : fail(WIG_ERR_CUDA, "cudaStreamBeginCapture: %s", cudaGetErrorString(e));
+      cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+      cudaStreamDestroy(cap);
+      if (rc) return rc;
+      if (e2 != cudaSuccess) return fail(WIG_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e2));
+      e = cudaGraphInstantiate(&h->gexec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) { h->gexec = nullptr; return fail(WIG_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e)); }
+      h->g_W = W_dev; h->g_t0 = t_index0; h->g_n = n_prop; h->g_flags = key_flags; h->g_warps = h->warps;
+    }
+    WIG_CUDA(cudaGraphLaunch(h->gexec, st));
+  } else {
+    if (int rc = wigb_launch_run(h, W, t_index0, n_prop, flags, st)) return rc;
+  }
+  if (obs_host) {
+    WIG_CUDA(cudaMemcpyAsync(obs_host, h->obs, nobs * sizeof(double), cudaMemcpyDeviceToHost, st));
+    WIG_CUDA(cudaStreamSynchronize(st));
+    return check_finite(obs_host, nobs, "wigb_run observables");
+  }
+  return WIG_OK;
+}
+
+// Time each candidate tile shape on `probe_steps` steps of the batch (state in
+// W_scratch, modified) and keep the fastest.
+extern "C" int wigb_autotune(wigb_handle* h, void* W_scratch, int64_t probe_steps, int32_t* chosen, double* ms_out,
+                             void* stream) {
+  if (!h || !W_scratch || probe_steps < 1) return fail(WIG_ERR_ARG, "wigb_autotune: bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int cands[] = {8, 4, 2};
+  int best = 0;
+  double best_ms = 1e300;
+  cudaEvent_t e0, e1;
+  WIG_CUDA(cudaEventCreate(&e0));
+  WIG_CUDA(cudaEventCreate(&e1));
+  for (int ci = 0; ci < 3; ++ci) {
+    const int w = cands[ci];
+    if (wigb_set_warps(h, w) != WIG_OK) continue;   // e.g. a tile that does not fit: skip it
+    if (int rc = wigb_run(h, W_scratch, 0, 1, 0, nullptr, stream)) return rc;   // warm-up
+    WIG_CUDA(cudaEventRecord(e0, st));
+    if (int rc = wigb_run(h, W_scratch, 0, probe_steps, WIG_RUN_CONTINUE, nullptr, stream)) return rc;
+    WIG_CUDA(cudaEventRecord(e1, st));
+    WIG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    WIG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms_out) ms_out[ci] = ms;
+    if (ms < best_ms) { best_ms = ms; best = w; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!best) return fail(WIG_ERR_ARG, "wigb_autotune: no tile shape fits this batch");
+  if (int rc = wigb_set_warps(h, best)) return rc;
+  if (chosen) *chosen = best;
+  return WIG_OK;
+}
+
+extern "C" int wigb_profile(wigb_handle* h, double* ms_out, int64_t* launches) {
+  if (!h || !ms_out) return fail(WIG_ERR_ARG, "wigb_profile: null argument");
+  ms_out[0] = ms_out[1] = 0.;
+  const size_t steps = h->ev_used / 3;
+  for (size_t n = 0; n < steps; ++n) {
+    float a = 0.f, b = 0.f;
+    WIG_CUDA(cudaEventSynchronize(h->ev[3 * n + 2]));
+    WIG_CUDA(cudaEventElapsedTime(&a, h->ev[3 * n], h->ev[3 * n + 1]));
+    WIG_CUDA(cudaEventElapsedTime(&b, h->ev[3 * n + 1], h->ev[3 * n + 2]));
+    ms_out[0] += a;
+    ms_out[1] += b;
+  }
+  if (launches) *launches = (int64_t)steps;
+  return WIG_OK;
+}

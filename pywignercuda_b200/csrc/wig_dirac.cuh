@@ -43,6 +43,7 @@ struct DiracArgs {
   double* part_row[2];   // [n_cta_row][DNR], ping-pong by row-pass parity
   double* part_col;      // [n_cta_col][DNC]
   int n_row_cta, n_col_cta;
+  double coef[8];        // cf[0..7] of the expression strings
 };
 
 // ---------------------------------------------------------------- A mix

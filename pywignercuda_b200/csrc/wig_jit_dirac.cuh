@@ -7,11 +7,18 @@
 #pragma once
 #include "wig_dirac.cuh"
 
+__device__ __forceinline__ UserPhys user_phys(const wig::DiracArgs& a) {
+  UserPhys ph;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) ph.cf[i] = a.coef[i];
+  return ph;
+}
+
 extern "C" __global__ void __launch_bounds__(DIR_RNT)
 dirac_rowpass(wig::DiracArgs a, double2* psi, int mode, int parity, double t_step, double t_obs,
               double* obs_row) {
   wig::dirac_row_body<UserPhys, DIR_NX, DIR_NY, DIR_ROWS, DIR_RNT>(
-      a, UserPhys(), psi, mode, parity, t_step, t_obs, obs_row);
+      a, user_phys(a), psi, mode, parity, t_step, t_obs, obs_row);
 }
 
 extern "C" __global__ void __launch_bounds__(DIR_CNT)

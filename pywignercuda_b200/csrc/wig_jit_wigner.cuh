@@ -17,15 +17,22 @@
 #endif
 #include "wig_wigner.cuh"
 
+__device__ __forceinline__ UserPhys user_phys(const wig::WigArgs& a) {
+  UserPhys ph;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) ph.cf[i] = a.coef[i];
+  return ph;
+}
+
 extern "C" __global__ void __launch_bounds__(WIG_XNT, WIG_XMINB)
 wig_xpass(wig::WigArgs a, double2* W, int scale_mode, double* obs_row) {
   wig::xpass_body<UserPhys, WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT, WIG_KIN_STRING != 0>(
-      a, UserPhys(), W, scale_mode, obs_row);
+      a, user_phys(a), W, scale_mode, obs_row);
 }
 
 extern "C" __global__ void __launch_bounds__(WIG_PNT, WIG_PMINB)
 wig_ppass(wig::WigArgs a, double2* W, double t) {
-  wig::ppass_body<UserPhys, WIG_NX, WIG_NP, WIG_PC, WIG_PNT, WIG_DAMP>(a, UserPhys(), W, t, a.partials);
+  wig::ppass_body<UserPhys, WIG_NX, WIG_NP, WIG_PC, WIG_PNT, WIG_DAMP>(a, user_phys(a), W, t, a.partials);
 }
 
 extern "C" __global__ void __launch_bounds__(WIG_RNT)
@@ -45,7 +52,7 @@ wig_scale(double2* W, long n, const double2* s) {
 
 extern "C" __global__ void __launch_bounds__(WIG_XNT)
 wig_odm_xpass(wig::WigArgs a, const double2* W, double2* T) {
-  wig::odm_xpass_body<UserPhys, WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT>(a, UserPhys(), W, T);
+  wig::odm_xpass_body<UserPhys, WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT>(a, user_phys(a), W, T);
 }
 
 extern "C" __global__ void __launch_bounds__(WIG_PNT)
@@ -59,9 +66,9 @@ wig_odm_ppass(wig::WigArgs a, double2* W, const double2* T, double coef, double 
 //   r_theta   exp(-D_Theta theta^2 dt)           expPotential_source :117
 //   mask1/2   1 - exp(-(x -+ x_max)^2/(10 dx)^2)  expPotential_source :121-123
 //   sfp       sign(p) f(p)                       theta_fp_source :422-428
-extern "C" __global__ void wig_setup(double* r_lambda, double* r_theta, double* mask1,
+extern "C" __global__ void wig_setup(wig::WigArgs a, double* r_lambda, double* r_theta, double* mask1,
                                      double* mask2s, double* sfp) {
-  const UserPhys ph;
+  const UserPhys ph = user_phys(a);
   const int NX = WIG_NX, NP = WIG_NP;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < NX; k += gridDim.x * blockDim.x) {
     const int jj = (k + NX / 2) % NX;

@@ -55,6 +55,7 @@ struct WigArgs {
   // ODM Lindblad damping (SetA_ODM :1206-1244, _Lindbladian_ODM :1516-1634), exact host values
   const double* lambda_tab; // [n_x] exact shifted Lambda
   double hbar_exact, L_material;
+  double coef[8];           // cf[0..7] of the expression strings
 };
 
 // ------------------------------------------------------------------ reductions

@@ -77,6 +77,10 @@ class GPU_Dirac2D:
         self._strings = [str(getattr(self, 'Potential_%d_String' % k)).encode() for k in range(4)]
         d.a0, d.a1, d.a2, d.a3 = self._strings
         d.x_table, d.y_table, d.px_table, d.py_table = [dptr(t) for t in self._tabs]
+        coefs = getattr(self, 'coefficients', None)
+        if coefs is not None:
+            for i, v in enumerate(coefs):
+                d.coef[i] = float(v)
         self._desc = d
         torch = _torch()
         self._device = torch.cuda.current_device()

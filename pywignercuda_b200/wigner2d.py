@@ -86,15 +86,23 @@ class Propagator_Base:
         self.Lambda = np.fft.fftshift(self.Lambda_range)[np.newaxis, :]
         self.P = np.fft.fftshift(self.P_range)[:, np.newaxis]
 
-    # ---- expression strings evaluated on the host (:674-692, :1674-1681)
+    # ---- expression strings evaluated on the host (:674-692, :1674-1681); the
+    # strings may use cf[0..7], the instance's optional ``coefficients``
+    def _coef(self):
+        c = np.zeros(8)
+        coefs = getattr(self, 'coefficients', None)
+        if coefs is not None:
+            c[:len(coefs)] = coefs
+        return c
+
     def Potential(self, t, x):
-        return _eval(self.potentialString, t=t, x=x)
+        return _eval(self.potentialString, t=t, x=x, cf=self._coef())
 
     def dPotential(self, t, x):
-        return _eval(self.dPotentialString, t=t, x=x)
+        return _eval(self.dPotentialString, t=t, x=x, cf=self._coef())
 
     def fp_Damping(self, p):
-        return _eval(self.fp_Damping_String, p=p)
+        return _eval(self.fp_Damping_String, p=p, cf=self._coef())
 
     # ---- helpers
     def fft_shift2D(self, X):
@@ -243,6 +251,8 @@ class GPU_Wigner2D_FFT(Propagator_Base):
         d.x_table, d.p_table = dptr(self._x_tab), dptr(self._p_tab)
         d.theta_table, d.lambda_table = dptr(self._theta_tab), dptr(self._lambda_tab)
         d.dv_table, d.v0_table = dptr(self._dv_tab), dptr(self._v0_tab)
+        for i, v in enumerate(self._coef()):
+            d.coef[i] = float(v)
         self._desc = d
         torch = _torch()
         self._device = torch.cuda.current_device()

@@ -111,3 +111,12 @@ def test_python_classes_fail_loudly_without_gpu():
                                       '0.5*p*p')
     with pytest.raises(WignerCudaError):
         Inst()
+
+
+def test_batch_jit_compiles_without_spills():
+    sizes = (ctypes.c_int32 * 4)(128, 256, 512, 1024)
+    buf = ctypes.create_string_buffer(1 << 17)
+    rc = _lib.load().wigb_jit_check(sizes, 4, 8, buf, len(buf))
+    log = buf.value.decode()
+    assert rc == 0, log
+    assert 'wigb_xpass' in log and 'wigb_ppass' in log
