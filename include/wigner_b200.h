@@ -251,6 +251,26 @@ int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t warps, char* l
 int wig_jit_check(const wig_desc* desc, char* log, int64_t log_cap);
 int dirac_jit_check(const dirac_desc* desc, char* log, int64_t log_cap);
 
+/* The observables of a Wigner function W ((n_p, n_x) complex128, device) --
+ * the 11 values wig_run records for a sample it does not renormalise (norm,
+ * <x>, <x^2>, <p>, <p^2>, <xp>, <V'>, <pV'>, <xV'>, <H>, negative area) --
+ * written to obs_dev[WIG_NOBS] (device), for callers that cannot allocate
+ * device memory (host callbacks and allocator hooks where cudaMalloc would
+ * re-enter or deadlock, deployments that forbid allocation after start-up).
+ * No counterpart in the reference.  It allocates nothing: its per-row partial
+ * sums live in a fixed device array of 4096 rows x 12 doubles (384 KB per
+ * device, held until the process exits), so n_p <= 4096 and n_x <= 4096,
+ * larger grids are rejected with WIG_ERR_ARG.  The tables (x, p, dV/dx,
+ * V(0, x); the library's shifted grids) are device arrays the caller owns;
+ * dx, dp are the grid steps and mass enters <H> = <p^2/2m + V>.  All calls on
+ * a device share the array and each overwrites the rows it reads, so calls
+ * whose kernels overlap on the GPU race.  The first call on a device looks up
+ * the array's address with that device current: make it before any stream
+ * capture.  Asynchronous on `stream`. */
+int wig_observables_noalloc(const void* W_dev, int32_t n_x, int32_t n_p, double dx, double dp, double mass,
+                            const double* x_tab_dev, const double* p_tab_dev, const double* dv_tab_dev,
+                            const double* v0_tab_dev, double* obs_dev, void* stream);
+
 /* Message of the calling thread's last failed call ("" if none). */
 const char* wig_last_error(void);
 

@@ -117,6 +117,8 @@ SIGNATURES = [
     ('wigb_profile', c_int, [c_void_p, _DP, POINTER(c_int64)]),
     ('wigb_destroy', c_int, [c_void_p]),
     ('wigb_jit_check', c_int, [POINTER(c_int32), c_int64, c_int32, c_char_p, c_int64]),
+    ('wig_observables_noalloc', c_int, [c_void_p, c_int32, c_int32, c_double, c_double, c_double, c_void_p,
+                                        c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('wig_last_error', c_char_p, []),
     ('wig_abi_version', c_int, []),
 ]

@@ -1019,6 +1019,9 @@ extern "C" int dirac_destroy(dirac_handle* h) {
 }
 
 extern "C" const char* wig_last_error(void) { return g_last_error.c_str(); }
+
+// Records a failure for wig_last_error from other translation units of the library.
+int wig_record_error(int code, const char* msg) { return fail(code, "%s", msg); }
 extern "C" int wig_abi_version(void) { return WIG_ABI_VERSION; }
 
 // ======================================================================== batched FP32
