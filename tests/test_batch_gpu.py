@@ -1,6 +1,7 @@
 """Batched FP32 form against the FP64 oracle.
 
-The norm is renormalised in FP64 every damped step, so it matches to 1e-6.
+The norm is renormalised in FP64 every damped step, so it matches to 1e-6
+(undamped instances drift by the FP32 FFT rounding, ~1e-8 per step).
 The energy carries the FP32 FFT rounding: FFT noise is spread uniformly over
 the grid (relative to the state's norm) and the energy observable weights the
 grid edges heavily (V ~ a x^4 up to ~1e3 at |x| = 10), so <H> drifts by
@@ -31,7 +32,10 @@ def test_mixed_sizes_against_fp64_oracle():
     b, obs, Ws = run_batch(cases, steps)
     for i, c in enumerate(cases):
         ref_obs, ref_W = WignerOracle(to_params(c)).run(initial_state(c), steps)
-        assert np.max(np.abs(obs[i, :, 0] - ref_obs[:, 0])) < 1e-6, i           # norm
+        # norm: renormalised in FP64 every damped step; an undamped instance keeps
+        # the FP32 FFT rounding (~1e-8 per step)
+        nb = 1e-6 if c['gamma'] else 2e-8 * steps
+        assert np.max(np.abs(obs[i, :, 0] - ref_obs[:, 0])) < nb, i
         escale = max(1., np.abs(ref_obs[:, 9]).max())
         assert np.max(np.abs(obs[i, :, 9] - ref_obs[:, 9])) < 2e-6 * steps * escale, i   # energy
         assert np.max(np.abs(obs[i, :, 1] - ref_obs[:, 1])) < 1e-4, i           # <x>
