@@ -54,6 +54,16 @@ struct BArgs {
 // butterflies (one or more per lane, no idle-lane branches)
 __host__ __device__ constexpr int spw_of(int n) { return n >= 512 ? 1 : 512 / n; }
 
+// Column stride of the p-pass tile (float2 units).  The transposing loads and
+// stores put CPB consecutive columns of one row on consecutive lanes, a
+// half-warp covering 16/CPB rows (8-byte accesses are served per half-warp):
+// stride = 16/CPB (mod 16) spreads them over 16 distinct bank pairs; CPB >= 16
+// needs an odd stride.
+__host__ __device__ constexpr int col_stride(int n, int cpb) {
+  return cpb >= 16 ? seq_stride32(n) + 1
+                   : seq_stride32(n) + ((16 / cpb - seq_stride32(n) % 16) + 16) % 16;
+}
+
 // dt*lambda*p/m etc. reduced to [-pi, pi] in FP64 (two-term 2 pi, Cody-Waite)
 __device__ __forceinline__ float reduce_phase(double phi) {
   const double q = rint(phi * 0.15915494309189533577);
@@ -140,7 +150,7 @@ __device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BIn
   float2* S = smb + N + (N + 1) / 2 + (threadIdx.x >> 5) * SPW * SEQ;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int m = threadIdx.x; m < N; m += blockDim.x) {
-    twsm[m] = A.tw[I.tw_x + m];
+    if (m < stage_tw_size(N)) twsm[m] = A.tw[I.tw_x + m];
     const int jj = (m + N / 2) % N;
     const double lam = I.dlambda * (jj - 0.5 * N);
     rtab[m] = (float)(exp(-I.D_lambda * lam * lam) / (double)N);
@@ -186,7 +196,7 @@ template <int N>
 __device__ __forceinline__ void batch_cl_D(const BInst& I, float2* B, const float2* twsm, const float* sfp,
                                            const float* ths, int lane) {
   constexpr int SPW = spw_of(N);
-  constexpr int CS = seq_stride32(N) + 1;
+  constexpr int CS = col_stride(N, WIGB_WARPS * SPW);
   for (int sq = 0; sq < SPW; ++sq)
     for (int k = lane; k < N; k += 32) B[sq * CS + pad16(k)] = cscale(B[sq * CS + pad16(k)], sfp[k]);
   __syncwarp();
@@ -201,11 +211,11 @@ template <int N>
 __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BInst& I, int col0, int item,
                                              double t, int sample) {
   constexpr int SPW = spw_of(N);
-  constexpr int CS = seq_stride32(N) + 1;
   constexpr int CPB = WIGB_WARPS * SPW;
+  constexpr int CS = col_stride(N, CPB);
   constexpr int NT = WIGB_WARPS * 32;
   extern __shared__ float2 smb[];
-  float2* twsm = smb;                                     // [N]
+  float2* twsm = smb;                                     // [N] (per-stage twiddle tables)
   float* rth = reinterpret_cast<float*>(smb + N);          // [N] exp(-D theta^2 dt)
   float* sfp = rth + N;                                    // [N] sign(p) f(p)
   float* ths = sfp + N;                                    // [N] theta / N
@@ -214,7 +224,7 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nx = I.n_x;
   for (int m = threadIdx.x; m < N; m += NT) {
-    twsm[m] = A.tw[I.tw_p + m];
+    if (m < stage_tw_size(N)) twsm[m] = A.tw[I.tw_p + m];
     const int ii = (m + N / 2) % N;
     const double th = I.dtheta * (ii - 0.5 * N);
     rth[m] = (float)exp(-I.D_theta * th * th * I.dt);

@@ -1044,7 +1044,7 @@ int batch_smem_x(int n, int warps) {
 }
 int batch_smem_p(int n, int warps, bool damped) {
   const int spw = wig::spw_of(n);
-  const int cs = wig::seq_stride32(n) + 1;
+  const int cs = wig::col_stride(n, warps * spw);
   return (n + (3 * n + 1) / 2 + (damped ? 2 : 1) * warps * spw * cs) * (int)sizeof(float2);
 }
 }  // namespace
@@ -1228,8 +1228,22 @@ extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t war
   std::vector<float2> tw;
   std::map<int, int> tw_off;
   for (int n : cls) {
+    // per-stage tables of the warp FFT (wig_fft32.cuh): T[(r-1)*NS + k] = W_{NS R}^{k r}
     tw_off[n] = (int)tw.size();
-    for (auto& z : twiddles(n)) tw.push_back(make_float2((float)z.x, (float)z.y));
+    const std::vector<double2> full = twiddles(n);
+    for (int ns = 1; ns < n; ns *= wig::radix32_of(n, ns)) {
+      const int R = wig::radix32_of(n, ns);
+      if (ns == 1) continue;
+      for (int r = 1; r < R; ++r)
+        for (int k = 0; k < ns; ++k) {
+          const double2 z = full[(size_t)k * r * (n / (ns * R))];
+          tw.push_back(make_float2((float)z.x, (float)z.y));
+        }
+    }
+    if ((int)tw.size() - tw_off[n] != wig::stage_tw_size(n)) {
+      delete h;
+      return fail(WIG_ERR_ARG, "internal: twiddle table size mismatch for n=%d", n);
+    }
   }
   h->binst.resize(count);
   h->offsets.resize(count + 1);

@@ -8,9 +8,13 @@
 // 16 elements keeps the stride-16 writes of the first stage on distinct banks
 // (8-byte accesses are served per half-warp).
 //
-// Twiddles come from a shared-memory table tw[m] = exp(-2 pi i m / N) (float,
-// rounded from extended precision on the host).  Forward = exp(-i ...),
-// inverse unnormalised.
+// Twiddles come from per-stage tables in shared memory: for a stage that
+// combines sub-transforms of length NS with radix R, T[(r-1)*NS + k] =
+// exp(-2 pi i k r / (NS R)) for r = 1..R-1, k < NS (float, rounded from
+// extended precision on the host), so the lanes of a warp (consecutive k) read
+// consecutive entries.  stage_tw_offset() gives each stage's offset; a size's
+// tables take stage_tw_size(N) entries.  Forward = exp(-i ...), inverse
+// unnormalised.
 #pragma once
 #include "wig_fft.cuh"
 
@@ -56,6 +60,15 @@ template <int N, int NS> struct Radix32 {
   static constexpr int value = rem >= 16 ? 16 : rem;   // 16 or the remaining 8 / 4 / 2
 };
 
+__host__ __device__ constexpr int radix32_of(int n, int ns) { return n / ns >= 16 ? 16 : n / ns; }
+// entries of the stages before the one that starts at sub-length NS
+__host__ __device__ constexpr int stage_tw_offset(int n, int ns) {
+  int off = 0;
+  for (int s = 1; s < ns; s *= radix32_of(n, s)) off += (s > 1 ? (radix32_of(n, s) - 1) * s : 0);
+  return off;
+}
+__host__ __device__ constexpr int stage_tw_size(int n) { return stage_tw_offset(n, n); }
+
 // One stage over the warp's SPW sequences (s: the warp's first sequence,
 // sequences SEQ elements apart).
 template <int N, int NS, int SPW, int SEQ, bool INV>
@@ -64,7 +77,7 @@ __device__ __forceinline__ void warp_fft_stage(float2* s, const float2* tw, int 
   constexpr int NBF = N / R;
   constexpr int TOT = SPW * NBF;
   constexpr int PER = (TOT + 31) / 32;
-  constexpr int TWS = N / (NS * R);
+  constexpr int TWO = stage_tw_offset(N, NS);
   float2 v[PER][R];
 #pragma unroll
   for (int m = 0; m < PER; ++m) {
@@ -85,7 +98,7 @@ __device__ __forceinline__ void warp_fft_stage(float2* s, const float2* tw, int 
       if (NS > 1) {
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          float2 w = tw[(k * r) * TWS];
+          float2 w = tw[TWO + (r - 1) * NS + k];
           if (INV) w.y = -w.y;
           v[m][r] = cmul(v[m][r], w);
         }
@@ -110,15 +123,18 @@ template <int N, int SPW, int SEQ, bool INV> struct WarpFft<N, N, SPW, SEQ, INV>
 };
 
 // FFT of the warp's SPW sequences, SEQ elements apart (caller has
-// __syncwarp'ed; returns synced).
+// __syncwarp'ed; returns synced).  Out of line: each (N, SPW, SEQ, direction)
+// is compiled once however many times a kernel calls it, which keeps the
+// batched kernels (several size classes, up to ten FFTs each) small enough for
+// the instruction cache.
 template <int N, int SPW, int SEQ, bool INV>
-__device__ __forceinline__ void warp_fft_cs(float2* s, const float2* tw, int lane) {
+__device__ __noinline__ void warp_fft_cs(float2* s, const float2* tw, int lane) {
   WarpFft<N, 1, SPW, SEQ, INV>::run(s, tw, lane);
 }
 
 template <int N, int SPW, bool INV>
 __device__ __forceinline__ void warp_fft(float2* s, const float2* tw, int lane) {
-  WarpFft<N, 1, SPW, seq_stride32(N), INV>::run(s, tw, lane);
+  warp_fft_cs<N, SPW, seq_stride32(N), INV>(s, tw, lane);
 }
 
 }  // namespace wig

@@ -3,10 +3,10 @@
 The norm is renormalised in FP64 every damped step, so it matches to 1e-6
 (undamped instances drift by the FP32 FFT rounding, ~1e-8 per step).
 The energy carries the FP32 FFT rounding: FFT noise is spread uniformly over
-the grid (relative to the state's norm) and the energy observable weights the
-grid edges heavily (V ~ a x^4 up to ~1e3 at |x| = 10), so <H> drifts by
-~1e-6 per step; the bound is 2e-6 x steps of the energy scale.  The state is
-checked to 1e-3 relative L2."""
+the grid (relative to the state's norm) and the energy observable weights it
+with H(x, p), largest at the grid edges (V ~ a x^4 up to ~1e3 at |x| = 10), so
+<H> drifts by ~1e-8 of max|H| over the grid per step; the bound is
+1e-8 x steps x max|H|.  The state is checked to 1e-3 relative L2."""
 import numpy as np
 import pytest
 
@@ -36,8 +36,9 @@ def test_mixed_sizes_against_fp64_oracle():
         # the FP32 FFT rounding (~1e-8 per step)
         nb = 1e-6 if c['gamma'] else 2e-8 * steps
         assert np.max(np.abs(obs[i, :, 0] - ref_obs[:, 0])) < nb, i
-        escale = max(1., np.abs(ref_obs[:, 9]).max())
-        assert np.max(np.abs(obs[i, :, 9] - ref_obs[:, 9])) < 2e-6 * steps * escale, i   # energy
+        prm = to_params(c)
+        hmax = np.abs(WignerOracle(prm).tab.obs_tables[8]).max()
+        assert np.max(np.abs(obs[i, :, 9] - ref_obs[:, 9])) < 1e-8 * steps * hmax, i   # energy
         assert np.max(np.abs(obs[i, :, 1] - ref_obs[:, 1])) < 1e-4, i           # <x>
         assert rel_l2(Ws[i], ref_W) < 1e-3, (i, rel_l2(Ws[i], ref_W))
 
