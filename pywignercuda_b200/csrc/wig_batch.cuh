@@ -1,27 +1,32 @@
 // Batched FP32 Wigner2D propagation: many independent instances of uneven
 // grid sizes advanced together, one x-pass launch and one p-pass launch per
 // step over a work list that spans every instance (x-items: blocks of rows,
-// p-items: blocks of columns).  Each CTA's warps own whole sequences (rows or
-// columns) and run the warp-level FP32 FFT of wig_fft32.cuh.
+// p-items: blocks of columns).  Every sequence (a row in the x-pass, a column
+// in the p-pass) is transformed by the register-resident FFT of wig_rfft.cuh:
+// rf_g(N) lanes of a warp hold its N elements in registers, so the whole
+// p-pass -- forward FFT, Moyal factor, inverse FFT, the three Caldeira-Leggett
+// dissipator applications (six more FFTs), observables -- runs on registers,
+// with shared memory only for the coalescing tile and one exchange per FFT.
 //
 // Precision policy: W, FFTs and the pointwise factors are FP32 complex; FP64
 // is used only to form the large phase arguments (dt*lambda*p/m and
 // dt*[V(x - hbar theta/2) - V(x + hbar theta/2)]/hbar, the latter from the
-// exact polynomial expansion) and to range-reduce them to [-pi, pi] before
-// sincosf, and for the observables (FP64 Kahan-compensated sums per thread,
-// FP64 tree / per-instance reductions).
+// exact polynomial expansion, both in units of 2 pi) and to reduce them to
+// one turn before sincospif, and for the observables (FP64 per-column
+// moments, FP64 tree / per-instance reductions).
 //
 // Normalisation (GPU_Wigner2D_FFT.Run :1912-1913): every p-item writes FP64
 // partial sums; the last CTA of an instance to finish (arrival counter, no
 // waiting) reduces them in item order, writes that step's observables and the
 // instance's pending scale, which the next x-pass applies on load.
 #pragma once
-#include "wig_fft32.cuh"
+#include "wig_rfft.cuh"
 #include "wig_wigner.cuh"
 
 #ifndef WIGB_WARPS
 #define WIGB_WARPS 8
 #endif
+#define WIGB_NT (WIGB_WARPS * 32)
 
 namespace wig {
 
@@ -31,7 +36,8 @@ struct BInst {
   int ff;            // f(p): 0 |p|, 1 p^2/sqrt(p^2 + f_eps)
   long long off;     // element offset in the packed state buffer
   int xitem0, n_xitems, pitem0, n_pitems;
-  int tw_x, tw_p;    // offsets of the instance's twiddle tables in the table buffer
+  int tw_x, tw_p;    // offsets of the instance's twiddle tables (2N entries each) in the table buffer
+  int ft_x, ft_p;    // offsets of its float tables: [rtab n_x][mm n_x] and [rth n_p][sfp n_p][ths n_p]
   double dt, hbar, mass, dx, dp, dtheta, dlambda, D_theta, D_lambda, f_eps;
   double v4, v2, v1, v0;   // V(x) = v4 x^4 + v2 x^2 + v1 x + v0
   double cl_k1, cl_k12, cl_c3;   // imaginary parts of the Caldeira-Leggett Horner coefficients
@@ -43,33 +49,46 @@ struct BArgs {
   const int2* pitems;    // (instance, first column)
   float2* W;
   const float2* tw;
+  const float* ft;
   double* partials;      // [n_pitems][NACC]
   unsigned* counters;    // [n_inst]
+  unsigned* tickets;     // [2] work-list tickets of the x- and p-pass (zero between launches)
   double2* scale;        // [n_inst]
   double* obs;           // [n_inst][obs_stride][NOBS]
   int obs_stride;
 };
 
-// sequences per warp: enough that every stage of the warp FFT has >= 32
-// butterflies (one or more per lane, no idle-lane branches)
-__host__ __device__ constexpr int spw_of(int n) { return n >= 512 ? 1 : 512 / n; }
+// Shared memory of one item (float2 units): the x-pass exchange regions; the
+// p-pass tile and its Caldeira-Leggett copy A.  The twiddle and factor tables
+// are read through the read-only data path (a few KB per size, L1-resident).
+__host__ __device__ constexpr int bx_smem(int n, int warps) { return warps * rf_spw(n) * (n + (rf_g(n) == 8 ? 8 : 0)); }
+__host__ __device__ constexpr int bp_smem(int n, int warps) { return 2 * warps * rf_spw(n) * n; }
 
-// Column stride of the p-pass tile (float2 units).  The transposing loads and
-// stores put CPB consecutive columns of one row on consecutive lanes, a
-// half-warp covering 16/CPB rows (8-byte accesses are served per half-warp):
-// stride = 16/CPB (mod 16) spreads them over 16 distinct bank pairs; CPB >= 16
-// needs an odd stride.
-__host__ __device__ constexpr int col_stride(int n, int cpb) {
-  return cpb >= 16 ? seq_stride32(n) + 1
-                   : seq_stride32(n) + ((16 / cpb - seq_stride32(n) % 16) + 16) % 16;
+// p-pass: column of the CT-wide tile owned by group `grp` of warp `warp`.
+// With 8-lane groups two sequences share a half-warp; pairing columns c and
+// c ^ PM keeps their tile accesses on distinct bank pairs.
+template <int N>
+__device__ __forceinline__ int rf_col(int warp, int grp) {
+  constexpr int G = rf_g(N), SPW = rf_spw(N), CT = WIGB_WARPS * SPW;
+  if constexpr (G == 8) {
+    constexpr int PM = CT / 2 < 8 ? CT / 2 : 8;
+    const int hw = 2 * warp + (grp >> 1);
+    const int base = (hw & (PM - 1)) | ((hw / PM) * 2 * PM);
+    return base ^ ((grp & 1) * PM);
+  } else {
+    return warp * SPW + grp;
+  }
 }
 
-// dt*lambda*p/m etc. reduced to [-pi, pi] in FP64 (two-term 2 pi, Cody-Waite)
-__device__ __forceinline__ float reduce_phase(double phi) {
-  const double q = rint(phi * 0.15915494309189533577);
-  double r = fma(-q, 6.2831853071795862320, phi);
-  r = fma(-q, 2.4492935982947063e-16, r);
-  return (float)r;
+// signed FFT-shifted index of array position k (coordinate = step * index)
+__device__ __forceinline__ int shifted(int k, int n) { return k < n / 2 ? k : k - n; }
+
+// e^{-2 pi i t} * r, t reduced to one turn in FP64
+__device__ __forceinline__ float2 turn_factor(double t, float r) {
+  const float f = (float)(t - rint(t));
+  float sn, cs;
+  sincospif(2.f * f, &sn, &cs);
+  return make_float2(r * cs, -r * sn);
 }
 
 struct Kahan {
@@ -100,17 +119,14 @@ __device__ __forceinline__ void accumulate_obs_k(Kahan (&acc)[NACC], float2 v, d
   if (w < 0.) acc[11].add(w);
 }
 
-// Write this CTA's partials; the last CTA of the instance reduces them (item
-// order, Kahan), writes the sample's observables and the instance's scale.
+// Write this CTA's partials; the last CTA of the instance reduces them (a fixed
+// order of Kahan sums), writes the sample's observables and the instance's scale.
 // mode: 0 none (scale 1), 1 normalise.
 template <int NT>
 __device__ __forceinline__ void batch_item_done(const BArgs& A, int inst, const BInst& I, int item,
-                                                Kahan (&acc)[NACC], int mode, int sample) {
+                                                double (&v)[NACC], int mode, int sample) {
   __shared__ double red[NT / 32][NACC];
   __shared__ int s_last;
-  double v[NACC];
-#pragma unroll
-  for (int k = 0; k < NACC; ++k) v[k] = acc[k].s + (-acc[k].c);
   block_sum<NT, NACC>(v, red);
   if (threadIdx.x < NACC) A.partials[(size_t)item * NACC + threadIdx.x] = red[0][threadIdx.x];
   __threadfence();
@@ -119,10 +135,19 @@ __device__ __forceinline__ void batch_item_done(const BArgs& A, int inst, const 
   __syncthreads();
   if (!s_last) return;
   __threadfence();
+  // 16 strided Kahan sums per accumulator, combined in a fixed order
+  __shared__ double part[NACC][17];
   __shared__ double tot[NACC];
+  for (int q = threadIdx.x; q < NACC * 16; q += NT) {
+    const int v = q >> 4, j = q & 15;
+    Kahan k;
+    for (int it = j; it < I.n_pitems; it += 16) k.add(__ldcg(&A.partials[(size_t)(I.pitem0 + it) * NACC + v]));
+    part[v][j] = k.s - k.c;
+  }
+  __syncthreads();
   if (threadIdx.x < NACC) {
     Kahan k;
-    for (int it = 0; it < I.n_pitems; ++it) k.add(__ldcg(&A.partials[(size_t)(I.pitem0 + it) * NACC + threadIdx.x]));
+    for (int j = 0; j < 16; ++j) k.add(part[threadIdx.x][j]);
     tot[threadIdx.x] = k.s - k.c;
   }
   __syncthreads();
@@ -139,199 +164,220 @@ __device__ __forceinline__ void batch_item_done(const BArgs& A, int inst, const 
   }
 }
 
-// ------------------------------------------------------------------ x-pass
-template <int N>
-__device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BInst& I, int row0) {
-  constexpr int SPW = spw_of(N);
-  constexpr int SEQ = seq_stride32(N);
-  extern __shared__ float2 smb[];
-  float2* twsm = smb;                                   // [N]
-  float* rtab = reinterpret_cast<float*>(smb + N);       // [N]
-  float2* S = smb + N + (N + 1) / 2 + (threadIdx.x >> 5) * SPW * SEQ;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int m = threadIdx.x; m < N; m += blockDim.x) {
-    if (m < stage_tw_size(N)) twsm[m] = A.tw[I.tw_x + m];
-    const int jj = (m + N / 2) % N;
-    const double lam = I.dlambda * (jj - 0.5 * N);
-    rtab[m] = (float)(exp(-I.D_lambda * lam * lam) / (double)N);
-  }
-  const double2 sd = A.scale[inst];
-  const float2 sc = make_float2((float)sd.x, (float)sd.y);
-  float2* Wi = A.W + I.off;
-  for (int sq = 0; sq < SPW; ++sq) {
-    const int row = row0 + warp * SPW + sq;
-    const float2* src = Wi + (size_t)row * N;
-    for (int k = lane; k < N; k += 32) S[sq * SEQ + pad16(k)] = cmul(src[k], sc);
+// Next work item of a persistent CTA (dynamic: a CTA that falls behind takes
+// fewer items).  The CTA drawing the last of the gridDim.x overflowing tickets
+// resets the counter for the next launch.  Every thread returns the item.
+__device__ __forceinline__ int next_item(unsigned* ticket, int n_items) {
+  __shared__ int s_item;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned t = atomicAdd(ticket, 1u);
+    if (t == (unsigned)n_items + gridDim.x - 1u) *ticket = 0u;
+    s_item = (int)t;
   }
   __syncthreads();
-  warp_fft<N, SPW, false>(S, twsm, lane);
-  for (int sq = 0; sq < SPW; ++sq) {
-    const int row = row0 + warp * SPW + sq;
-    const int ii = (row + I.n_p / 2) % I.n_p;
-    const double p = I.dp * (ii - 0.5 * I.n_p);
-    const double cp = I.dt * p / I.mass;
-    for (int k = lane; k < N; k += 32) {
-      const int jj = (k + N / 2) % N;
-      const double lam = I.dlambda * (jj - 0.5 * N);
-      float sn, cs;
-      sincosf(reduce_phase(cp * lam), &sn, &cs);
-      const float r = rtab[k];
-      const int id = sq * SEQ + pad16(k);
-      S[id] = cmul(S[id], make_float2(r * cs, -r * sn));
+  return s_item;
+}
+
+// ------------------------------------------------------------------ x-pass
+// Item: WIGB_WARPS * rf_spw(N) consecutive rows; lane g of group `grp` holds
+// elements g + G m of its row.
+template <int N>
+__device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BInst& I, int row0) {
+  typedef RegFft<float2, N> F;
+  constexpr int E = F::E, G = F::G, Q = F::Q, SPW = rf_spw(N);
+  constexpr int XS = N + (G == 8 ? 8 : 0);
+  extern __shared__ float2 smb[];
+  const float2* tf = A.tw + I.tw_x;
+  const float2* ti = tf + N;
+  const float* rtab = A.ft + I.ft_x;   // exp(-D_lambda lambda^2) / N
+  float2* X = smb;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
+  const int row = row0 + warp * SPW + grp;
+  const double2 sd = A.scale[inst];
+  const float2 sc = make_float2((float)sd.x, (float)sd.y);
+  float2* Wr = A.W + I.off + (size_t)row * N;
+  float2 v[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m) v[m] = cmul(Wr[g + G * m], sc);
+  const PlainSlot sl{(warp * SPW + grp) * XS};
+  F::fwd(v, X, sl, tf, g);
+  // kinetic factor exp(-i dt lambda p / m) r_lambda(lambda) / N, in turns
+  const double cq = I.dt * I.dp * I.dlambda * (double)shifted(row, I.n_p) / (I.mass * 6.283185307179586477);
+#pragma unroll
+  for (int i = 0; i < Q; ++i)
+#pragma unroll
+    for (int b = 0; b < G; ++b) {
+      const int k = g * Q + i + E * b;
+      const int lj = b < G / 2 ? k : k - N;
+      v[i * G + b] = cmul(v[i * G + b], turn_factor(cq * (double)lj, __ldg(rtab + k)));
     }
-  }
-  __syncwarp();
-  warp_fft<N, SPW, true>(S, twsm, lane);
-  for (int sq = 0; sq < SPW; ++sq) {
-    const int row = row0 + warp * SPW + sq;
-    float2* dst = Wi + (size_t)row * N;
-    for (int k = lane; k < N; k += 32) dst[k] = S[sq * SEQ + pad16(k)];
-  }
+  F::inv(v, X, sl, ti, g);
+#pragma unroll
+  for (int m = 0; m < E; ++m) Wr[g + G * m] = v[m];
 }
 
 // ------------------------------------------------------------------ p-pass
-// Column tile of WIGB_WARPS*SPW columns, stored column-major in shared memory
-// (column stride SEQ+1, odd, so the transposing loads/stores are conflict-free).
-template <int N>
-__device__ __forceinline__ void batch_cl_D(const BInst& I, float2* B, const float2* twsm, const float* sfp,
-                                           const float* ths, int lane) {
-  constexpr int SPW = spw_of(N);
-  constexpr int CS = col_stride(N, WIGB_WARPS * SPW);
-  for (int sq = 0; sq < SPW; ++sq)
-    for (int k = lane; k < N; k += 32) B[sq * CS + pad16(k)] = cscale(B[sq * CS + pad16(k)], sfp[k]);
-  __syncwarp();
-  warp_fft_cs<N, SPW, CS, false>(B, twsm, lane);
-  for (int sq = 0; sq < SPW; ++sq)
-    for (int k = lane; k < N; k += 32) B[sq * CS + pad16(k)] = cscale(B[sq * CS + pad16(k)], ths[k]);
-  __syncwarp();
-  warp_fft_cs<N, SPW, CS, true>(B, twsm, lane);
-}
-
+// Item: a tile of CT = WIGB_WARPS * rf_spw(N) columns x N rows, staged in
+// shared memory (element (k, c) at k CT + (c ^ sw(k))) so that the global
+// loads and stores are row segments; each group then owns one column.
 template <int N>
 __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BInst& I, int col0, int item,
-                                             double t, int sample) {
-  constexpr int SPW = spw_of(N);
-  constexpr int CPB = WIGB_WARPS * SPW;
-  constexpr int CS = col_stride(N, CPB);
-  constexpr int NT = WIGB_WARPS * 32;
+                                             int sample) {
+  typedef RegFft<float2, N> F;
+  constexpr int E = F::E, G = F::G, Q = F::Q, SPW = rf_spw(N), CT = WIGB_WARPS * SPW, NT = WIGB_NT;
   extern __shared__ float2 smb[];
-  float2* twsm = smb;                                     // [N] (per-stage twiddle tables)
-  float* rth = reinterpret_cast<float*>(smb + N);          // [N] exp(-D theta^2 dt)
-  float* sfp = rth + N;                                    // [N] sign(p) f(p)
-  float* ths = sfp + N;                                    // [N] theta / N
-  float2* tile = smb + N + (3 * N + 1) / 2;                // [CPB * CS]
-  float2* btile = tile + CPB * CS;                         // [CPB * CS] (Caldeira-Leggett)
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float2* tf = A.tw + I.tw_p;
+  const float2* ti = tf + N;
+  const float* rth = A.ft + I.ft_p;   // exp(-D_theta theta^2 dt)
+  const float* sfp = rth + N;         // sign(p) f(p)
+  const float* ths = sfp + N;         // theta / N
+  float2* tile = smb;
+  float2* atile = tile + CT * N;      // A (post-Moyal column), same slot map
   const int nx = I.n_x;
-  for (int m = threadIdx.x; m < N; m += NT) {
-    if (m < stage_tw_size(N)) twsm[m] = A.tw[I.tw_p + m];
-    const int ii = (m + N / 2) % N;
-    const double th = I.dtheta * (ii - 0.5 * N);
-    rth[m] = (float)exp(-I.D_theta * th * th * I.dt);
-    const double p = I.dp * (ii - 0.5 * N);
-    double f = (I.ff == 0) ? fabs(p) : p * p / sqrt(p * p + I.f_eps);
-    sfp[m] = (float)(p >= 0. ? f : -f);
-    ths[m] = (float)(th / (double)N);
-  }
   float2* Wi = A.W + I.off;
-  for (int e = threadIdx.x; e < CPB * N; e += NT) {
-    const int k = e / CPB, c = e - k * CPB;
-    tile[c * CS + pad16(k)] = Wi[(size_t)k * nx + col0 + c];
+  for (int e = threadIdx.x; e < CT * N; e += NT) {
+    const int k = e / CT, c = e & (CT - 1);
+    tile[k * CT + (c ^ tile_sw<CT>(k))] = Wi[(size_t)k * nx + col0 + c];
   }
   __syncthreads();
-  float2* S = tile + warp * SPW * CS;
-  warp_fft_cs<N, SPW, CS, false>(S, twsm, lane);
-  const double xmax = I.dx * (nx - 1.) / 2.;
-  for (int sq = 0; sq < SPW; ++sq) {
-    const int col = col0 + warp * SPW + sq;
-    const int jj = (col + nx / 2) % nx;
-    const double x = I.dx * (jj - 0.5 * nx);
-    const float m1 = (float)(1. - exp(-(x - xmax) * (x - xmax) / ((10. * I.dx) * (10. * I.dx))));
-    const float m2 = (float)((1. - exp(-(x + xmax) * (x + xmax) / ((10. * I.dx) * (10. * I.dx)))) / (double)N);
-    const float mm = m1 * m2;
-    // V(x - u) - V(x + u) = -2u (4 v4 x^3 + 4 v4 x u^2 + 2 v2 x + v1), u = hbar theta / 2
-    const double a3 = 4. * I.v4 * x * x * x + 2. * I.v2 * x + I.v1, a1 = 4. * I.v4 * x;
-    const double ph0 = -I.dt / I.hbar;
-    for (int k = lane; k < N; k += 32) {
-      const int ii = (k + N / 2) % N;
-      const double th = I.dtheta * (ii - 0.5 * N);
-      const double u = 0.5 * I.hbar * th;
-      const double dV = -2. * u * (a3 + a1 * u * u);
-      float sn, cs;
-      sincosf(reduce_phase(-ph0 * dV), &sn, &cs);
-      const float r = rth[k] * mm;
-      const int id = sq * CS + pad16(k);
-      S[id] = cmul(S[id], make_float2(r * cs, -r * sn));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
+  const int c = rf_col<N>(warp, grp);
+  const TileSlot<CT> sl{c};
+  float2 w[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m) w[m] = tile[sl(g + G * m)];
+  // Moyal factor exp(-i dt [V(x - u) - V(x + u)] / hbar) r_theta mask1 mask2 / N,
+  // u = hbar theta / 2 = h j:  V(x - u) - V(x + u) = -2u (a3 + a1 u^2); phase in turns
+  const int col = col0 + c;
+  const double x = I.dx * (double)shifted(col, nx);
+  const double h = 0.5 * I.hbar * I.dtheta;
+  const double kk = -I.dt * h / (3.141592653589793238 * I.hbar);
+  const double al = kk * ((4. * I.v4 * x * x + 2. * I.v2) * x + I.v1);
+  const double be = kk * h * h * (4. * I.v4 * x);
+  const float mm = __ldg(A.ft + I.ft_x + nx + col);
+  // One transform pair per pass through this loop (kept rolled so the kernel
+  // holds a single copy of each FFT):
+  //   it = 0:  w = IFFT[Moyal FFT(w)]                       -> A = w (kept in atile)
+  //   it = 1..3 (Caldeira-Leggett, Horner form):
+  //            w = A + coef_it D(w),  D(w) = IFFT[theta/N FFT(sign(p) f(p) w)]
+  const int n_it = I.damp == 1 ? 4 : 1;
+#pragma unroll 1
+  for (int it = 0; it < n_it; ++it) {
+    if (it > 0) {
+#pragma unroll
+      for (int m = 0; m < E; ++m) w[m] = cscale(w[m], __ldg(sfp + g + G * m));
+    }
+    F::fwd(w, tile, sl, tf, g);
+    if (it == 0) {
+#pragma unroll
+      for (int i = 0; i < Q; ++i)
+#pragma unroll
+        for (int b = 0; b < G; ++b) {
+          const int k = g * Q + i + E * b;
+          const double j = (double)(b < G / 2 ? k : k - N);
+          w[i * G + b] = cmul(w[i * G + b], turn_factor(j * fma(be, j * j, al), __ldg(rth + k) * mm));
+        }
+    } else {
+#pragma unroll
+      for (int i = 0; i < Q; ++i)
+#pragma unroll
+        for (int b = 0; b < G; ++b) w[i * G + b] = cscale(w[i * G + b], __ldg(ths + g * Q + i + E * b));
+    }
+    F::inv(w, tile, sl, ti, g);
+    if (it == 0) {
+      if (n_it > 1) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) atile[sl(g + G * m)] = w[m];
+      }
+    } else {
+      const float cf = (float)(it == 1 ? I.cl_k1 : (it == 2 ? I.cl_k12 : I.cl_c3));
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const float2 a = atile[sl(g + G * m)];
+        w[m] = make_float2(a.x - cf * w[m].y, a.y + cf * w[m].x);
+      }
     }
   }
-  __syncwarp();
-  warp_fft_cs<N, SPW, CS, true>(S, twsm, lane);
-  if (I.damp == 1) {
-    float2* Bw = btile + warp * SPW * CS;
-    const float2 k1 = make_float2(0.f, (float)I.cl_k1), k12 = make_float2(0.f, (float)I.cl_k12);
-    const float2 c3 = make_float2(0.f, (float)I.cl_c3);
-    for (int sq = 0; sq < SPW; ++sq)
-      for (int k = lane; k < N; k += 32) Bw[sq * CS + pad16(k)] = S[sq * CS + pad16(k)];
-    __syncwarp();
-    batch_cl_D<N>(I, Bw, twsm, sfp, ths, lane);
-    for (int sq = 0; sq < SPW; ++sq)
-      for (int k = lane; k < N; k += 32) {
-        const int id = sq * CS + pad16(k);
-        Bw[id] = cadd(S[id], cmul(k1, Bw[id]));
-      }
-    __syncwarp();
-    batch_cl_D<N>(I, Bw, twsm, sfp, ths, lane);
-    for (int sq = 0; sq < SPW; ++sq)
-      for (int k = lane; k < N; k += 32) {
-        const int id = sq * CS + pad16(k);
-        Bw[id] = cadd(S[id], cmul(k12, Bw[id]));
-      }
-    __syncwarp();
-    batch_cl_D<N>(I, Bw, twsm, sfp, ths, lane);
-    for (int sq = 0; sq < SPW; ++sq)
-      for (int k = lane; k < N; k += 32) {
-        const int id = sq * CS + pad16(k);
-        S[id] = cadd(S[id], cmul(c3, Bw[id]));
-      }
+  // observables: column moments sum W, sum W p_j, sum W p_j^2 (FP64), Im and
+  // the negative part (FP32 per lane), reduced over the group's lanes
+  double s0 = 0., s1 = 0., s2 = 0.;
+  float si = 0.f, sn = 0.f;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const double wr = (double)w[m].x;
+    const double pj = (double)(g + G * m - (m >= E / 2 ? N : 0));
+    s0 += wr;
+    const double wp = wr * pj;
+    s1 += wp;
+    s2 = fma(wp, pj, s2);
+    si += w[m].y;
+    sn += fminf(w[m].x, 0.f);
   }
+  double sid = (double)si, snd = (double)sn;
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    sid += __shfl_xor_sync(0xffffffffu, sid, o);
+    snd += __shfl_xor_sync(0xffffffffu, snd, o);
+  }
+  double acc[NACC];
+#pragma unroll
+  for (int v = 0; v < NACC; ++v) acc[v] = 0.;
+  if (g == 0) {
+    const double dV = (4. * I.v4 * x * x + 2. * I.v2) * x + I.v1;
+    const double V = ((I.v4 * x * x + I.v2) * x + I.v1) * x + I.v0;
+    const double M1 = s1 * I.dp, M2 = s2 * (I.dp * I.dp);
+    acc[0] = s0;
+    acc[1] = sid;
+    acc[2] = s0 * x;
+    acc[3] = s0 * x * x;
+    acc[4] = M1;
+    acc[5] = M2;
+    acc[6] = M1 * x;
+    acc[7] = s0 * dV;
+    acc[8] = M1 * dV;
+    acc[9] = s0 * x * dV;
+    acc[10] = M2 / (2. * I.mass) + s0 * V;
+    acc[11] = snd;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < E; ++m) tile[sl(g + G * m)] = w[m];
   __syncthreads();
-  Kahan acc[NACC];
-  for (int e = threadIdx.x; e < CPB * N; e += NT) {
-    const int k = e / CPB, c = e - k * CPB;
-    const int col = col0 + c;
-    const float2 v = tile[c * CS + pad16(k)];
-    Wi[(size_t)k * nx + col] = v;
-    const int jj = (col + nx / 2) % nx, ii = (k + N / 2) % N;
-    accumulate_obs_k(acc, v, I.dx * (jj - 0.5 * nx), I.dp * (ii - 0.5 * N), I);
+  for (int e = threadIdx.x; e < CT * N; e += NT) {
+    const int k = e / CT, cc = e & (CT - 1);
+    Wi[(size_t)k * nx + col0 + cc] = tile[k * CT + (cc ^ tile_sw<CT>(k))];
   }
   batch_item_done<NT>(A, inst, I, item, acc, I.damp ? 1 : 0, sample);
-  (void)t;
 }
 
 // Initial normalisation and sample 0 (Run :1778-1780), over the p-items.
 template <int N>
 __device__ __forceinline__ void batch_reduce_item(const BArgs& A, int inst, const BInst& I, int col0, int item,
                                                   int mode, int sample) {
-  constexpr int SPW = spw_of(N);
-  constexpr int CPB = WIGB_WARPS * SPW;
-  constexpr int NT = WIGB_WARPS * 32;
+  constexpr int CPB = WIGB_WARPS * rf_spw(N);
+  constexpr int NT = WIGB_NT;
   const int nx = I.n_x;
   const float2* Wi = A.W + I.off;
   Kahan acc[NACC];
   for (int e = threadIdx.x; e < CPB * N; e += NT) {
     const int k = e / CPB, c = e - k * CPB;
     const int col = col0 + c;
-    const int jj = (col + nx / 2) % nx, ii = (k + N / 2) % N;
-    accumulate_obs_k(acc, Wi[(size_t)k * nx + col], I.dx * (jj - 0.5 * nx), I.dp * (ii - 0.5 * N), I);
+    accumulate_obs_k(acc, Wi[(size_t)k * nx + col], I.dx * shifted(col, nx), I.dp * shifted(k, N), I);
   }
-  batch_item_done<NT>(A, inst, I, item, acc, mode, sample);
+  double v[NACC];
+#pragma unroll
+  for (int k = 0; k < NACC; ++k) v[k] = acc[k].s + (-acc[k].c);
+  batch_item_done<NT>(A, inst, I, item, v, mode, sample);
 }
 
 template <int N>
 __device__ __forceinline__ void batch_scale_item(const BArgs& A, int inst, const BInst& I, int col0) {
-  constexpr int SPW = spw_of(N);
-  constexpr int CPB = WIGB_WARPS * SPW;
-  constexpr int NT = WIGB_WARPS * 32;
+  constexpr int CPB = WIGB_WARPS * rf_spw(N);
+  constexpr int NT = WIGB_NT;
   const double2 sd = A.scale[inst];
   const float2 sc = make_float2((float)sd.x, (float)sd.y);
   float2* Wi = A.W + I.off;

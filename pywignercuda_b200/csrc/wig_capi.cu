@@ -1038,14 +1038,30 @@ struct BVariant {
   int smem_x = 0, smem_p = 0, occ_x = 1, occ_p = 1;
 };
 
-int batch_smem_x(int n, int warps) {
-  const int spw = wig::spw_of(n);
-  return (n + (n + 1) / 2 + warps * spw * wig::seq_stride32(n)) * (int)sizeof(float2);
-}
-int batch_smem_p(int n, int warps, bool damped) {
-  const int spw = wig::spw_of(n);
-  const int cs = wig::col_stride(n, warps * spw);
-  return (n + (3 * n + 1) / 2 + (damped ? 2 : 1) * warps * spw * cs) * (int)sizeof(float2);
+int batch_smem_x(int n, int warps) { return wig::bx_smem(n, warps) * (int)sizeof(float2); }
+int batch_smem_p(int n, int warps) { return wig::bp_smem(n, warps) * (int)sizeof(float2); }
+
+// exp(-2 pi i m / n) as a float pair: among the pairs within 2 ulp of the
+// extended-precision value, the one with |w|^2 closest to 1 (ties: the closest
+// in angle).  A forward twiddle and its conjugate in the inverse transform then
+// leave the spectral component's magnitude unbiased.
+float2 twiddle_f(int n, long long m) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  const long double a = 2.0L * pi * (long double)(m % n) / (long double)n;
+  const long double c = cosl(a), s = -sinl(a);
+  const float c0 = (float)c, s0 = (float)s;
+  float bc = c0, bs = s0;
+  long double best = 1e30L;
+  for (int i = -2; i <= 2; ++i)
+    for (int j = -2; j <= 2; ++j) {
+      float cc = c0, ss = s0;
+      for (int k = 0; k < (i < 0 ? -i : i); ++k) cc = nextafterf(cc, i > 0 ? 2.f : -2.f);
+      for (int k = 0; k < (j < 0 ? -j : j); ++k) ss = nextafterf(ss, j > 0 ? 2.f : -2.f);
+      const long double d = fabsl((long double)cc * cc + (long double)ss * ss - 1.0L);
+      const long double key = d + 1e-3L * (fabsl((long double)cc - c) + fabsl((long double)ss - s));
+      if (key < best) { best = key; bc = cc; bs = ss; }
+    }
+  return make_float2(bc, bs);
 }
 }  // namespace
 
@@ -1076,8 +1092,12 @@ struct wigb_handle {
 };
 
 static std::string wigb_source(const std::vector<int>& classes, int warps) {
-  char head[128];
-  snprintf(head, sizeof(head), "#define WIGB_WARPS %d\n#define WIGB_CASES(F)", warps);
+  // register cap: 8-warp tiles run one CTA per SM (255 registers), smaller
+  // tiles three 4-warp / six 2-warp CTAs (168 registers)
+  char head[192];
+  const int minb = warps == 8 ? 1 : 12 / warps;
+  snprintf(head, sizeof(head), "#define WIGB_WARPS %d\n#define WIGB_XMINB %d\n#define WIGB_PMINB %d\n#define WIGB_CASES(F)",
+           warps, minb, minb);
   std::string src = head;
   for (int n : classes) src += " F(" + std::to_string(n) + ")";
   src += "\n";
@@ -1104,12 +1124,10 @@ extern "C" int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t war
 
 static int wigb_compile(wigb_handle* h, int warps, BVariant* v) {
   const std::string src = wigb_source(h->classes, warps);
-  bool any_damped = false;
-  for (auto& b : h->binst) any_damped |= b.damp != 0;
   int smx = 0, smp = 0;
   for (int n : h->classes) {
     smx = std::max(smx, batch_smem_x(n, warps));
-    smp = std::max(smp, batch_smem_p(n, warps, any_damped));
+    smp = std::max(smp, batch_smem_p(n, warps));
   }
   if (smx > 227 * 1024 || smp > 227 * 1024)
     return fail(WIG_ERR_ARG, "batched tile of %d warps needs %d / %d bytes of shared memory", warps, smx, smp);
@@ -1133,8 +1151,8 @@ static int wigb_compile(wigb_handle* h, int warps, BVariant* v) {
   return WIG_OK;
 }
 
-// Work lists for a tile of `warps` warps: x-items of warps*spw(n_x) rows,
-// p-items of warps*spw(n_p) columns; p-items of each instance contiguous
+// Work lists for a tile of `warps` warps: x-items of warps*rf_spw(n_x) rows,
+// p-items of warps*rf_spw(n_p) columns; p-items of each instance contiguous
 // (the last-CTA reduction reads them as a range), instances ordered by
 // decreasing per-item cost so the persistent loop ends balanced.
 static int wigb_set_warps(wigb_handle* h, int warps) {
@@ -1153,7 +1171,7 @@ static int wigb_set_warps(wigb_handle* h, int warps) {
   std::vector<int2> xi, pi;
   for (int i : order) {
     wig::BInst& b = h->binst[i];
-    const int rpb = warps * wig::spw_of(b.n_x), cpb = warps * wig::spw_of(b.n_p);
+    const int rpb = warps * wig::rf_spw(b.n_x), cpb = warps * wig::rf_spw(b.n_p);
     if (b.n_p % rpb || b.n_x % cpb)
       return fail(WIG_ERR_ARG, "instance %d: grid %d x %d does not tile with %d warps", i, b.n_x, b.n_p, warps);
     b.xitem0 = (int)xi.size();
@@ -1225,28 +1243,22 @@ extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t war
   std::sort(cls.begin(), cls.end());
   cls.erase(std::unique(cls.begin(), cls.end()), cls.end());
   h->classes = cls;
+  // register-FFT twiddles per size (wig_rfft.cuh): forward tf[a G + g] = W_n^{g a},
+  // inverse ti[(i G + b) G + t] = W_n^{b (t Q + i)}
   std::vector<float2> tw;
   std::map<int, int> tw_off;
   for (int n : cls) {
-    // per-stage tables of the warp FFT (wig_fft32.cuh): T[(r-1)*NS + k] = W_{NS R}^{k r}
+    const int E = wig::rf_e(n), G = wig::rf_g(n), Q = E / G;
     tw_off[n] = (int)tw.size();
-    const std::vector<double2> full = twiddles(n);
-    for (int ns = 1; ns < n; ns *= wig::radix32_of(n, ns)) {
-      const int R = wig::radix32_of(n, ns);
-      if (ns == 1) continue;
-      for (int r = 1; r < R; ++r)
-        for (int k = 0; k < ns; ++k) {
-          const double2 z = full[(size_t)k * r * (n / (ns * R))];
-          tw.push_back(make_float2((float)z.x, (float)z.y));
-        }
-    }
-    if ((int)tw.size() - tw_off[n] != wig::stage_tw_size(n)) {
-      delete h;
-      return fail(WIG_ERR_ARG, "internal: twiddle table size mismatch for n=%d", n);
-    }
+    for (int a = 0; a < E; ++a)
+      for (int g = 0; g < G; ++g) tw.push_back(twiddle_f(n, (long long)g * a));
+    for (int i = 0; i < Q; ++i)
+      for (int b = 0; b < G; ++b)
+        for (int t = 0; t < G; ++t) tw.push_back(twiddle_f(n, (long long)b * (t * Q + i)));
   }
   h->binst.resize(count);
   h->offsets.resize(count + 1);
+  std::vector<float> ft;
   int64_t off = 0;
   for (int64_t i = 0; i < count; ++i) {
     const wigb_instance& d = h->inst[i];
@@ -1269,26 +1281,61 @@ extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t war
     b.cl_k1 = (c1 + c2) != 0. ? c1 * c2 / (c1 + c2) : 0.;
     b.cl_k12 = c1 + c2;
     b.cl_c3 = c3;
+    // per-frequency / per-column factors (expPLambda_source :153, expPotential_source :117-123,
+    // theta_fp_source :422-428), FP64 then rounded once
+    b.ft_x = (int)ft.size();
+    for (int k = 0; k < d.n_x; ++k) {   // r_lambda / n_x
+      const double lam = b.dlambda * (((k + d.n_x / 2) % d.n_x) - 0.5 * d.n_x);
+      ft.push_back((float)(exp(-b.D_lambda * lam * lam) / (double)d.n_x));
+    }
+    const double x_max = b.dx * (d.n_x - 1.) / 2.;
+    for (int k = 0; k < d.n_x; ++k) {   // mask1 mask2 / n_p
+      const double x = b.dx * (((k + d.n_x / 2) % d.n_x) - 0.5 * d.n_x);
+      const double w2 = (10. * b.dx) * (10. * b.dx);
+      const double m1 = 1. - exp(-(x - x_max) * (x - x_max) / w2), m2 = 1. - exp(-(x + x_max) * (x + x_max) / w2);
+      ft.push_back((float)(m1 * m2 / (double)d.n_p));
+    }
+    b.ft_p = (int)ft.size();
+    for (int k = 0; k < d.n_p; ++k) {   // r_theta
+      const double th = b.dtheta * (((k + d.n_p / 2) % d.n_p) - 0.5 * d.n_p);
+      ft.push_back((float)exp(-b.D_theta * th * th * b.dt));
+    }
+    for (int k = 0; k < d.n_p; ++k) {   // sign(p) f(p)
+      const double p = b.dp * (((k + d.n_p / 2) % d.n_p) - 0.5 * d.n_p);
+      const double f = b.ff == 0 ? fabs(p) : p * p / sqrt(p * p + b.f_eps);
+      ft.push_back((float)(p >= 0. ? f : -f));
+    }
+    for (int k = 0; k < d.n_p; ++k) {   // theta / n_p
+      const double th = b.dtheta * (((k + d.n_p / 2) % d.n_p) - 0.5 * d.n_p);
+      ft.push_back((float)(th / (double)d.n_p));
+    }
   }
   h->total = off;
   h->offsets[count] = off;
   DevBuf& B = h->bufs;
   float2* tw_d = nullptr;
+  float* ft_d = nullptr;
   wig::BInst* inst_d = nullptr;
   unsigned* cnt_d = nullptr;
+  unsigned* tick_d = nullptr;
   double2* scale_d = nullptr;
   int rc = B.alloc(&tw_d, tw.size(), tw.data());
+  if (!rc) rc = B.alloc(&ft_d, ft.size(), ft.data());
   if (!rc) rc = B.alloc(&inst_d, (size_t)count);
   if (!rc) rc = B.alloc(&cnt_d, (size_t)count);
+  if (!rc) rc = B.alloc(&tick_d, (size_t)2);
   if (!rc) rc = B.alloc(&scale_d, (size_t)count);
   if (!rc) {
     cudaError_t e = cudaMemset(cnt_d, 0, count * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(tick_d, 0, 2 * sizeof(unsigned));
     if (e != cudaSuccess) rc = fail(WIG_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
   }
   if (rc) { B.free_all(); delete h; return rc; }
   h->a.tw = tw_d;
+  h->a.ft = ft_d;
   h->a.inst = inst_d;
   h->a.counters = cnt_d;
+  h->a.tickets = tick_d;
   h->a.scale = scale_d;
   if ((rc = wigb_set_warps(h, warps ? warps : 8))) { wigb_destroy(h); return rc; }
   *out = h;
@@ -1329,9 +1376,8 @@ static int wigb_launch_run(wigb_handle* h, float2* W, int64_t t_index0, int64_t 
     void* xargs[] = {&a, &nxi};
     if (int rc = launch(v.fx, h->grid_x, nt, v.smem_x, st, xargs)) return rc;
     if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 1], st));
-    double t = (double)(t_index0 + n);   // time index (the polynomial potential is time independent)
-    int sample = (int)(n + 1);
-    void* pargs[] = {&a, &npi, &t, &sample};
+    int sample = (int)(n + 1);   // the polynomial potentials are time independent
+    void* pargs[] = {&a, &npi, &sample};
     if (int rc = launch(v.fp, h->grid_p, nt, v.smem_p, st, pargs)) return rc;
     if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 2], st));
   }
