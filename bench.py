@@ -49,10 +49,12 @@ DPOT = '0.2*pow(x,3) - 2*x'
 GAMMA, D_THETA = 0.1, 0.1
 REPLICAS = 16
 PASS_BYTES = NX * NP * 16 * 2      # one fused pass reads and writes the c128 grid once
-# dram__bytes_read.sum + dram__bytes_write.sum per p-pass launch, from the ncu capture
-# summarised in profiles/wig_ppass_c128_1024.md (None until a capture exists)
-NCU_TRAFFIC_PPASS = None
-NCU_TRAFFIC_BATCH = None
+# dram__bytes_read.sum + dram__bytes_write.sum per p-pass launch, from the ncu captures
+# summarised in profiles/wig_passes_c128_1024.md (one 1024^2 replica, whose state fits in
+# L2: the capture shows one read of it) and profiles/wigb_passes_batch64.md (the 64-instance
+# batch, 187 MB of state)
+NCU_TRAFFIC_PPASS = 16.94e6 + 0.04e6
+NCU_TRAFFIC_BATCH = 188.0e6 + 150.5e6
 
 
 def peaks():
