@@ -195,8 +195,9 @@ int dirac_destroy(dirac_handle* h);
  * V(x) = v4 x^4 + v2 x^2 + v1 x + v0, kinetic p^2/2m, Caldeira-Leggett damping
  * (gamma != 0) with f(p) = |p| or p^2/sqrt(p^2 + f_eps), on uneven grids
  * (powers of two in [64, 1024]), advanced together in FP32 complex (W,
- * FFTs, pointwise factors) with FP64 phase arguments range-reduced before
- * sincosf and FP64 Kahan-compensated observables.  Constants are exact (no
+ * FFTs, pointwise factors) with FP64 phase arguments reduced to one turn
+ * before sincospif and FP64 observables (per-column moments, compensated
+ * per-instance sums).  Constants are exact (no
  * '%f' rounding).  No counterpart in the reference, which runs one complex128
  * instance per Run() (GPU_Wigner2D_FFT.py:1843); the step is the same Lie
  * split (:1884-1913). */
@@ -241,6 +242,46 @@ int wigb_destroy(wigb_handle* h);
 /* Compile-only check (no GPU) of the batched kernels for the given grid sizes
  * and tile shape; log receives the NVRTC / ptxas report. */
 int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t warps, char* log, int64_t log_cap);
+
+/* ---- Adjoint (differentiable) FP32 form.  No counterpart in the reference,
+ * which has no gradients.  One Wigner2D grid (powers of two in [64, 1024] per
+ * axis) advanced by the Lie step of GPU_Wigner2D_FFT.Run (:1884-1899)
+ *   W_{n+1} = P(eps_n) K W_n,
+ * K the kinetic x-pass (p^2/2m, r_lambda), P the Moyal p-pass with
+ * V(x) = v4 x^4 + v2 x^2 + v0 + eps_n x, r_theta and the absorbing masks; eps_n
+ * is a control per step read from device memory; no damping, no
+ * normalisation.  State: (n_p, n_x) complex64, FFT-shifted, device. */
+typedef struct wiga_desc {
+  int32_t abi_version;   /* WIG_ABI_VERSION */
+  int32_t n_x, n_p;
+  int32_t reserved;
+  double x_amplitude, p_amplitude, hbar, mass, dt, d_theta, d_lambda;
+  double v4, v2, v0;
+} wiga_desc;
+
+typedef struct wiga_handle wiga_handle;
+
+int wiga_create(const wiga_desc* desc, wiga_handle** out);
+
+/* n_steps forward steps from step index step0, W in place.  eps_dev: device
+ * double array indexed by step (>= step0 + n_steps entries).  Y_dev (may be
+ * NULL): device complex64 [n_steps][n_p][n_x], receives Y_n = K W_n of each
+ * step, the input wig_step_adjoint needs.  Asynchronous on `stream`. */
+int wiga_forward(wiga_handle* h, void* W_dev, const double* eps_dev, int64_t step0, int64_t n_steps,
+                 void* Y_dev, void* stream);
+
+/* One adjoint step n.  On entry lam_dev (complex64, device) holds dL/dW_{n+1},
+ * on exit dL/dW_n = K^H P(eps_n)^H dL/dW_{n+1} (gradients in the convention
+ * dL = Re sum conj(grad) dW, the one torch uses for complex tensors).  Y_dev:
+ * Y_n from wiga_forward.  grad_dev[step] (device double) receives dL/d eps_n.
+ * Asynchronous on `stream`. */
+int wig_step_adjoint(wiga_handle* h, void* lam_dev, const void* Y_dev, const double* eps_dev, int64_t step,
+                     double* grad_dev, void* stream);
+
+int wiga_destroy(wiga_handle* h);
+
+/* Compile-only check (no GPU) of the adjoint kernels for the descriptor's grid. */
+int wiga_jit_check(const wiga_desc* desc, char* log, int64_t log_cap);
 
 /* Compile-only check of an instance's kernels: builds the JIT source the way
  * wig_create / dirac_create do and compiles it with NVRTC for sm_100a without

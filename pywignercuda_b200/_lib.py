@@ -83,6 +83,13 @@ class WigbInstance(ctypes.Structure):
                 ('f_eps', c_double), ('v4', c_double), ('v2', c_double), ('v1', c_double), ('v0', c_double)]
 
 
+class WigaDesc(ctypes.Structure):
+    _fields_ = [('abi_version', c_int32), ('n_x', c_int32), ('n_p', c_int32), ('reserved', c_int32),
+                ('x_amplitude', c_double), ('p_amplitude', c_double), ('hbar', c_double), ('mass', c_double),
+                ('dt', c_double), ('d_theta', c_double), ('d_lambda', c_double),
+                ('v4', c_double), ('v2', c_double), ('v0', c_double)]
+
+
 class DiracDesc(ctypes.Structure):
     _fields_ = [('abi_version', c_int32), ('n_x', c_int32), ('n_y', c_int32), ('constants', c_int32),
                 ('precision', c_int32), ('reserved', c_int32),
@@ -117,6 +124,11 @@ SIGNATURES = [
     ('wigb_profile', c_int, [c_void_p, _DP, POINTER(c_int64)]),
     ('wigb_destroy', c_int, [c_void_p]),
     ('wigb_jit_check', c_int, [POINTER(c_int32), c_int64, c_int32, c_char_p, c_int64]),
+    ('wiga_create', c_int, [POINTER(WigaDesc), POINTER(c_void_p)]),
+    ('wiga_forward', c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p]),
+    ('wig_step_adjoint', c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    ('wiga_destroy', c_int, [c_void_p]),
+    ('wiga_jit_check', c_int, [POINTER(WigaDesc), c_char_p, c_int64]),
     ('wig_observables_noalloc', c_int, [c_void_p, c_int32, c_int32, c_double, c_double, c_double, c_void_p,
                                         c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('wig_last_error', c_char_p, []),

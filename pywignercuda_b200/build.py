@@ -21,8 +21,10 @@ CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libwigner_b200.so')
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 
-JIT_SOURCES = {'kJitWignerSource': 'wig_jit_wigner.cuh', 'kJitDiracSource': 'wig_jit_dirac.cuh',
-               'kJitBatchSource': 'wig_jit_batch.cuh'}
+# generated include -> {string name: JIT entry file}
+JIT_SOURCES = {'wig_device_src.inc': {'kJitWignerSource': 'wig_jit_wigner.cuh', 'kJitDiracSource': 'wig_jit_dirac.cuh',
+                                      'kJitBatchSource': 'wig_jit_batch.cuh'},
+               'wig_adjoint_src.inc': {'kJitAdjointSource': 'wig_jit_adjoint.cuh'}}
 
 
 def inline(fn, seen=None):
@@ -43,25 +45,26 @@ def inline(fn, seen=None):
 
 
 def write_inc():
-    parts = ['// generated by pywignercuda_b200/build.py -- do not edit\n']
-    for name, fn in JIT_SOURCES.items():
-        src = inline(fn)
-        assert ')WIGSRC"' not in src
-        # split into chunks below the 64 KiB string-literal limit of some compilers
-        chunks = [src[i:i + 30000] for i in range(0, len(src), 30000)]
-        body = '\n'.join('R"WIGSRC(%s)WIGSRC"' % c for c in chunks)
-        parts.append('static const char %s[] =\n%s;\n' % (name, body))
-    path = os.path.join(CSRC, 'wig_device_src.inc')
-    text = ''.join(parts)
-    if not os.path.exists(path) or open(path).read() != text:
-        with open(path, 'w') as f:
-            f.write(text)
+    for inc, srcs in JIT_SOURCES.items():
+        parts = ['// generated by pywignercuda_b200/build.py -- do not edit\n']
+        for name, fn in srcs.items():
+            src = inline(fn)
+            assert ')WIGSRC"' not in src
+            # split into chunks below the 64 KiB string-literal limit of some compilers
+            chunks = [src[i:i + 30000] for i in range(0, len(src), 30000)]
+            body = '\n'.join('R"WIGSRC(%s)WIGSRC"' % c for c in chunks)
+            parts.append('static const char %s[] =\n%s;\n' % (name, body))
+        path = os.path.join(CSRC, inc)
+        text = ''.join(parts)
+        if not os.path.exists(path) or open(path).read() != text:
+            with open(path, 'w') as f:
+                f.write(text)
 
 
 def build(verbose=False):
     write_inc()
     sources = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith('.cu')]
-    deps = sources + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.cuh', '.inc'))]
+    deps = sources + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.cuh', '.inc', '.h'))]
     deps.append(os.path.join(os.path.dirname(HERE), 'include', 'wigner_b200.h'))
     if os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(d) for d in deps):
         return LIB

@@ -32,8 +32,9 @@
 #include "wig_dirac.cuh"
 #include "wig_batch.cuh"
 #include "wig_device_src.inc"   // kJitWignerSource, kJitDiracSource (generated by build.py)
+#include "wig_host.h"
 
-namespace {
+namespace wighost {
 
 // ------------------------------------------------------------------ errors
 thread_local std::string g_last_error;
@@ -48,13 +49,6 @@ int fail(int code, const char* fmt, ...) {
   return code;
 }
 
-#define WIG_CUDA(call)                                                                  \
-  do {                                                                                  \
-    cudaError_t e_ = (call);                                                            \
-    if (e_ != cudaSuccess)                                                              \
-      return fail(e_ == cudaErrorMemoryAllocation ? WIG_ERR_NOMEM : WIG_ERR_CUDA,       \
-                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
-  } while (0)
 
 // ------------------------------------------------------------------ driver API
 struct Driver {
@@ -276,27 +270,22 @@ const char* kMathPrelude =
     "#ifndef M_PI\n#define M_PI 3.14159265358979323846\n#endif\n"
     "#ifndef M_E\n#define M_E 2.7182818284590452354\n#endif\n";
 
-template <class T>
-int dev_upload(T** dst, const T* src, size_t n) {
-  WIG_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));
-  if (src) WIG_CUDA(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
-  return WIG_OK;
+int nvrtc_compile_locked(const std::string& src, std::vector<char>* cubin, std::string* log, bool verbose) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return nvrtc_compile(src, cubin, log, verbose);
 }
 
-struct DevBuf {
-  std::vector<void*> ptrs;
-  template <class T> int alloc(T** p, size_t n, const T* src = nullptr) {
-    int rc = dev_upload(p, src, n);
-    if (rc == WIG_OK) ptrs.push_back((void*)*p);
-    return rc;
-  }
-  void free_all() {
-    for (void* p : ptrs) cudaFree(p);
-    ptrs.clear();
-  }
-};
+int occupancy(CUfunction f, int threads, int dyn_smem) {
+  static PFN_cuOccupancyMaxActiveBlocksPerMultiprocessor occ = nullptr;
+  if (!occ) entry("cuOccupancyMaxActiveBlocksPerMultiprocessor", occ);
+  int n = 1;
+  if (!occ || occ(&n, f, threads, dyn_smem) != CUDA_SUCCESS) n = 1;
+  return n < 1 ? 1 : n;
+}
 
-}  // namespace
+}  // namespace wighost
+
+using namespace wighost;
 
 // ======================================================================== Wigner
 struct wig_handle {
@@ -1030,7 +1019,6 @@ extern "C" int wig_abi_version(void) { return WIG_ABI_VERSION; }
 // captured once into a CUDA graph (WIG_RUN_GRAPH) and replayed; the tile shape
 // (warps per CTA) is chosen by wigb_autotune from timed candidates.
 namespace {
-PFN_cuOccupancyMaxActiveBlocksPerMultiprocessor g_occ = nullptr;
 
 struct BVariant {
   int warps = 0;
@@ -1041,6 +1029,9 @@ struct BVariant {
 int batch_smem_x(int n, int warps) { return wig::bx_smem(n, warps) * (int)sizeof(float2); }
 int batch_smem_p(int n, int warps) { return wig::bp_smem(n, warps) * (int)sizeof(float2); }
 
+}  // namespace
+
+namespace wighost {
 // exp(-2 pi i m / n) as a float pair: among the pairs within 2 ulp of the
 // extended-precision value, the one with |w|^2 closest to 1 (ties: the closest
 // in angle).  A forward twiddle and its conjugate in the inverse transform then
@@ -1063,7 +1054,16 @@ float2 twiddle_f(int n, long long m) {
     }
   return make_float2(bc, bs);
 }
-}  // namespace
+
+void rf_twiddles(int n, std::vector<float2>* tw) {
+  const int E = wig::rf_e(n), G = wig::rf_g(n), Q = E / G;
+  for (int a = 0; a < E; ++a)
+    for (int g = 0; g < G; ++g) tw->push_back(twiddle_f(n, (long long)g * a));
+  for (int i = 0; i < Q; ++i)
+    for (int b = 0; b < G; ++b)
+      for (int t = 0; t < G; ++t) tw->push_back(twiddle_f(n, (long long)b * (t * Q + i)));
+}
+}  // namespace wighost
 
 struct wigb_handle {
   int device = 0, count = 0, n_sm = 148;
@@ -1141,11 +1141,8 @@ static int wigb_compile(wigb_handle* h, int warps, BVariant* v) {
   v->warps = warps;
   v->smem_x = smx;
   v->smem_p = smp;
-  if (!g_occ) entry("cuOccupancyMaxActiveBlocksPerMultiprocessor", g_occ);
-  if (g_occ) {
-    g_occ(&v->occ_x, v->fx, warps * 32, smx);
-    g_occ(&v->occ_p, v->fp, warps * 32, smp);
-  }
+  v->occ_x = occupancy(v->fx, warps * 32, smx);
+  v->occ_p = occupancy(v->fp, warps * 32, smp);
   v->occ_x = std::max(v->occ_x, 1);
   v->occ_p = std::max(v->occ_p, 1);
   return WIG_OK;
@@ -1243,18 +1240,11 @@ extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t war
   std::sort(cls.begin(), cls.end());
   cls.erase(std::unique(cls.begin(), cls.end()), cls.end());
   h->classes = cls;
-  // register-FFT twiddles per size (wig_rfft.cuh): forward tf[a G + g] = W_n^{g a},
-  // inverse ti[(i G + b) G + t] = W_n^{b (t Q + i)}
   std::vector<float2> tw;
   std::map<int, int> tw_off;
   for (int n : cls) {
-    const int E = wig::rf_e(n), G = wig::rf_g(n), Q = E / G;
     tw_off[n] = (int)tw.size();
-    for (int a = 0; a < E; ++a)
-      for (int g = 0; g < G; ++g) tw.push_back(twiddle_f(n, (long long)g * a));
-    for (int i = 0; i < Q; ++i)
-      for (int b = 0; b < G; ++b)
-        for (int t = 0; t < G; ++t) tw.push_back(twiddle_f(n, (long long)b * (t * Q + i)));
+    rf_twiddles(n, &tw);
   }
   h->binst.resize(count);
   h->offsets.resize(count + 1);

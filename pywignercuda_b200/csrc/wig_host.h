@@ -1,0 +1,67 @@
+// Host-side helpers shared by the library's translation units (internal; not
+// part of the C ABI): error recording, the NVRTC -> module -> function -> launch
+// path of the JIT-compiled kernels, device allocation lists and the FP32
+// twiddle rounding.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/wigner_b200.h"
+
+namespace wighost {
+
+extern thread_local std::string g_last_error;
+
+// Record a printf-style message as the thread's last error; returns code.
+int fail(int code, const char* fmt, ...);
+
+#define WIG_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return wighost::fail(e_ == cudaErrorMemoryAllocation ? WIG_ERR_NOMEM : WIG_ERR_CUDA, \
+                           "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+// NVRTC source -> sm_100a CUBIN (compile only; no GPU needed).  Takes the JIT lock itself
+// when `lock` is set.
+int nvrtc_compile_locked(const std::string& src, std::vector<char>* cubin, std::string* log, bool verbose);
+// Module of `src` on `device` (compiled once per process and cached).
+int get_module(const std::string& src, int device, CUmodule* mod);
+int get_fn(CUmodule mod, const char* name, CUfunction* f, int dyn_smem);
+int launch(CUfunction f, unsigned grid, unsigned block, unsigned smem, cudaStream_t st, void** args);
+int copy_log(const std::string& log, char* out, int64_t cap);
+// Blocks that can be resident per SM for a launch shape (1 when the query is unavailable).
+int occupancy(CUfunction f, int threads, int dyn_smem);
+// exp(-2 pi i m / n) as the float pair within 2 ulp whose |w|^2 is closest to 1.
+float2 twiddle_f(int n, long long m);
+// Register-FFT twiddle tables of size n (wig_rfft.cuh), appended to *tw (2n entries):
+// forward tf[a G + g] = W_n^{g a}, inverse ti[(i G + b) G + t] = W_n^{b (t Q + i)}.
+void rf_twiddles(int n, std::vector<float2>* tw);
+
+template <class T>
+int dev_upload(T** dst, const T* src, size_t n) {
+  WIG_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));
+  if (src) WIG_CUDA(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return WIG_OK;
+}
+
+// Device allocations owned by a handle, freed together.
+struct DevBuf {
+  std::vector<void*> ptrs;
+  template <class T> int alloc(T** p, size_t n, const T* src = nullptr) {
+    int rc = dev_upload(p, src, n);
+    if (rc == WIG_OK) ptrs.push_back((void*)*p);
+    return rc;
+  }
+  void free_all() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+};
+
+}  // namespace wighost
