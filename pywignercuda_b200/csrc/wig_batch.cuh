@@ -202,16 +202,20 @@ __device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BIn
   for (int m = 0; m < E; ++m) v[m] = cmul(Wr[g + G * m], sc);
   const PlainSlot sl{(warp * SPW + grp) * XS};
   F::fwd(v, X, sl, tf, g);
-  // kinetic factor exp(-i dt lambda p / m) r_lambda(lambda) / N, in turns
+  // kinetic factor exp(-i dt lambda p / m) r_lambda(lambda) / N, in turns.  The
+  // factors are evaluated in a rolled loop into the lane's exchange slots (free
+  // between the two transforms) and then applied: one copy of the FP64
+  // reduction + sincospif per kernel instead of E (instruction-cache footprint).
   const double cq = I.dt * I.dp * I.dlambda * (double)shifted(row, I.n_p) / (I.mass * 6.283185307179586477);
+#pragma unroll 2
+  for (int e = 0; e < E; ++e) {
+    const int i = e / G, b = e % G;
+    const int k = g * Q + i + E * b;
+    const int lj = b < G / 2 ? k : k - N;
+    X[sl(e * G + g)] = turn_factor(cq * (double)lj, __ldg(rtab + k));
+  }
 #pragma unroll
-  for (int i = 0; i < Q; ++i)
-#pragma unroll
-    for (int b = 0; b < G; ++b) {
-      const int k = g * Q + i + E * b;
-      const int lj = b < G / 2 ? k : k - N;
-      v[i * G + b] = cmul(v[i * G + b], turn_factor(cq * (double)lj, __ldg(rtab + k)));
-    }
+  for (int e = 0; e < E; ++e) v[e] = cmul(v[e], X[sl(e * G + g)]);
   F::inv(v, X, sl, ti, g);
 #pragma unroll
   for (int m = 0; m < E; ++m) Wr[g + G * m] = v[m];
@@ -270,14 +274,16 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
     }
     F::fwd(w, tile, sl, tf, g);
     if (it == 0) {
+      // Moyal factors through the column's (free) tile slots, as in the x-pass
+#pragma unroll 2
+      for (int e = 0; e < E; ++e) {
+        const int i = e / G, b = e % G;
+        const int k = g * Q + i + E * b;
+        const double j = (double)(b < G / 2 ? k : k - N);
+        tile[sl(e * G + g)] = turn_factor(j * fma(be, j * j, al), __ldg(rth + k) * mm);
+      }
 #pragma unroll
-      for (int i = 0; i < Q; ++i)
-#pragma unroll
-        for (int b = 0; b < G; ++b) {
-          const int k = g * Q + i + E * b;
-          const double j = (double)(b < G / 2 ? k : k - N);
-          w[i * G + b] = cmul(w[i * G + b], turn_factor(j * fma(be, j * j, al), __ldg(rth + k) * mm));
-        }
+      for (int e = 0; e < E; ++e) w[e] = cmul(w[e], tile[sl(e * G + g)]);
     } else {
 #pragma unroll
       for (int i = 0; i < Q; ++i)

@@ -90,6 +90,14 @@ __device__ __forceinline__ C twc32(C v, int j) {
   if (j == 24) return mul_mi<!INV>(v);
   const double c = cospi16(j), s = cospi16(8 - j);   // cos, sin of 2 pi j / 32
   C r;
+  if ((j & 7) == 4) {   // |c| = |s| = sqrt(1/2): one product per component
+    const double h = 0.70710678118654752440084436210485;
+    const auto cx = c > 0. ? v.x : -v.x, cy = c > 0. ? v.y : -v.y;   // v c / h
+    const auto sx = s > 0. ? v.x : -v.x, sy = s > 0. ? v.y : -v.y;   // v s / h
+    if (INV) { r.x = mulk(cx - sy, h); r.y = mulk(sx + cy, h); }
+    else     { r.x = mulk(cx + sy, h); r.y = mulk(cy - sx, h); }
+    return r;
+  }
   if (INV) { r.x = mulk2(v.x, c, v.y, -s); r.y = mulk2(v.x, s, v.y, c); }
   else     { r.x = mulk2(v.x, c, v.y, s);  r.y = mulk2(v.y, c, v.x, -s); }
   return r;
