@@ -212,10 +212,11 @@ __device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BIn
     const int i = e / G, b = e % G;
     const int k = g * Q + i + E * b;
     const int lj = b < G / 2 ? k : k - N;
-    X[sl(e * G + g)] = turn_factor(cq * (double)lj, __ldg(rtab + k));
+    X[sl(e * G + g)] = turn_factor(cq * (double)lj, 1.f);
   }
 #pragma unroll
-  for (int e = 0; e < E; ++e) v[e] = cmul(v[e], X[sl(e * G + g)]);
+  for (int e = 0; e < E; ++e)
+    v[e] = cscale(cmul(v[e], X[sl(e * G + g)]), __ldg(rtab + g * Q + e / G + E * (e % G)));
   F::inv(v, X, sl, ti, g);
 #pragma unroll
   for (int m = 0; m < E; ++m) Wr[g + G * m] = v[m];
@@ -240,9 +241,23 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
   float2* atile = tile + CT * N;      // A (post-Moyal column), same slot map
   const int nx = I.n_x;
   float2* Wi = A.W + I.off;
-  for (int e = threadIdx.x; e < CT * N; e += NT) {
-    const int k = e / CT, c = e & (CT - 1);
-    tile[k * CT + (c ^ tile_sw<CT>(k))] = Wi[(size_t)k * nx + col0 + c];
+  // coalesced tile load: all of the thread's loads issued before their
+  // shared-memory stores (one latency per item instead of one per element)
+  constexpr int PER = CT * N / NT, LB = PER;   // every load of the thread in flight
+  static_assert(PER * NT == CT * N && PER % LB == 0, "tile load shape");
+#pragma unroll 1
+  for (int r0 = 0; r0 < PER; r0 += LB) {
+    float2 buf[LB];
+#pragma unroll
+    for (int r = 0; r < LB; ++r) {
+      const int e = threadIdx.x + (r0 + r) * NT;
+      buf[r] = Wi[(size_t)(e / CT) * nx + col0 + (e & (CT - 1))];
+    }
+#pragma unroll
+    for (int r = 0; r < LB; ++r) {
+      const int e = threadIdx.x + (r0 + r) * NT, k = e / CT;
+      tile[k * CT + ((e & (CT - 1)) ^ tile_sw<CT>(k))] = buf[r];
+    }
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
@@ -353,8 +368,9 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
 #pragma unroll
   for (int m = 0; m < E; ++m) tile[sl(g + G * m)] = w[m];
   __syncthreads();
-  for (int e = threadIdx.x; e < CT * N; e += NT) {
-    const int k = e / CT, cc = e & (CT - 1);
+#pragma unroll 8
+  for (int r = 0; r < PER; ++r) {
+    const int e = threadIdx.x + r * NT, k = e / CT, cc = e & (CT - 1);
     Wi[(size_t)k * nx + col0 + cc] = tile[k * CT + (cc ^ tile_sw<CT>(k))];
   }
   batch_item_done<NT>(A, inst, I, item, acc, I.damp ? 1 : 0, sample);

@@ -1,0 +1,78 @@
+"""Multi-GPU sharding of the batched form (pywignercuda_b200/shard.py), on the
+CPU: the cost-balanced partition of the instances, and -- as two gloo ranks --
+the gather of the per-instance observables to rank 0 and the bench's
+max-over-ranks timing reduction."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from pywignercuda_b200.shard import gather_observables, imbalance, instance_cost, partition
+
+
+def _batch():
+    import bench
+    return [dict(n_x=c['n'], n_p=c['n'], gamma=c['gamma']) for c in bench.batch_config()]
+
+
+@pytest.mark.parametrize('world', [1, 2, 4, 8])
+def test_partition_covers_every_instance_once(world):
+    inst = _batch()
+    parts = partition(inst, world)
+    assert len(parts) == world
+    flat = sorted(i for p in parts for i in p)
+    assert flat == list(range(len(inst)))
+    assert all(p == sorted(p) for p in parts)
+    # LPT: the heaviest rank exceeds the mean by at most one instance's cost
+    loads = [sum(instance_cost(inst[i]) for i in p) for p in parts]
+    assert max(loads) - np.mean(loads) <= max(instance_cost(d) for d in inst) + 1e-6
+    if world <= 4:
+        assert imbalance(inst, parts) < 1.10
+
+
+def test_partition_is_deterministic():
+    inst = _batch()
+    assert partition(inst, 4) == partition(inst, 4)
+
+
+def _obs_of(i, n=6):
+    return np.full((n, 11), float(i)) + np.arange(11)[None, :] * 1e-3
+
+
+def _rank_main(rank, world, port, out_dir):
+    import torch.distributed as dist
+    import bench
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        inst = _batch()
+        parts = partition(inst, world)
+        local = np.stack([_obs_of(i) for i in parts[rank]])
+        full = gather_observables(local, parts, rank)
+        if rank == 0:
+            assert full.shape == (len(inst), 6, 11)
+            for i in range(len(inst)):
+                assert np.array_equal(full[i], _obs_of(i)), i
+        else:
+            assert full is None
+        ms = bench.barrier_max(world, 10. + rank)
+        assert ms == 10. + (world - 1)
+        bench.barrier(world)
+        open(os.path.join(out_dir, 'ok%d' % rank), 'w').write('ok')
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(('127.0.0.1', 0))
+        return s.getsockname()[1]
+
+
+def test_gloo_two_ranks_gather_and_max(tmp_path):
+    world = 2
+    mp.spawn(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    assert sorted(os.listdir(tmp_path)) == ['ok0', 'ok1']
