@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define WIG_ABI_VERSION 1
+#define WIG_ABI_VERSION 2
 
 enum wig_status {
   WIG_OK = 0,
@@ -60,6 +60,14 @@ enum wig_constants {
 
 enum wig_precision { WIG_PREC_C128 = 0, WIG_PREC_F32 = 1 };
 
+enum wig_potential_phase {
+  WIG_PHASE_MOYAL = 0, /* exp(-i dt [V(x - hbar theta/2) - V(x + hbar theta/2)] / hbar)
+                          (expPotential_source, GPU_Wigner2D_FFT.py:80-126)            */
+  WIG_PHASE_KVN = 1    /* classical Liouville (KvN) factor exp(+i dt V'(t, x) theta) from the
+                          dpotential string (exp_PotentialKvN_source :27-75,
+                          GPU_FokkerPlank2D_FFT :2242-2459)                          */
+};
+
 /* wig_run / dirac_run flags */
 #define WIG_RUN_CONTINUE 1u /* W continues an earlier call: skip the entry normalisation */
 #define WIG_RUN_PROFILE 2u  /* time every x-pass / p-pass launch with CUDA events (wig_profile) */
@@ -83,6 +91,9 @@ typedef struct wig_desc {
   int32_t constants;           /* wig_constants                                     */
   int32_t precision;           /* wig_precision                                     */
   int32_t n_lindblad;          /* ODM: 1 (GPU_Wigner2D_FFT) or 2 (GPU_Wigner2D_ODM2)  */
+  int32_t potential_phase;     /* wig_potential_phase (KvN: damping none or Caldeira-Leggett) */
+  int32_t skip_normalise;      /* 1: damped steps are not renormalised (GPU_FokkerPlank2D_FFT
+                                  with normalization != 'Wigner', :2404-2406)           */
   double x_amplitude, p_amplitude;
   double hbar, mass, dt;
   double d_theta, d_lambda, gamma;
@@ -91,6 +102,8 @@ typedef struct wig_desc {
   const char* potential;       /* potentialString, C expression in (t, x)           */
   const char* kinetic;         /* kinematicString, C expression in p                */
   const char* fp_damping;      /* fp_Damping_String, C expression in p              */
+  const char* dpotential;      /* dPotentialString, C expression in (t, x); used by
+                                  WIG_PHASE_KVN (NULL -> "0.")                          */
   /* Exact host tables of the observables (Run :1785-1792, :1747); NULL -> built
    * by the library (shifted linspace grids; zeros for dV / V0). */
   const double* x_table;       /* [n_x] */

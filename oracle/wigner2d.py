@@ -66,6 +66,12 @@ class WignerParams:
     weight2: float = 0.0
     constants: str = 'cuda_%f'             # 'cuda_%f' | 'exact'
     coef: tuple = ()                       # values of cf[0..7] in the expression strings
+    # GPU_FokkerPlank2D_FFT (GPU_Wigner2D_FFT.py:2242-2459): the classical (KvN /
+    # Liouville) potential factor exp(+i dt V'(t, x) theta) instead of the Moyal one
+    # (exp_PotentialKvN_source :27-75), and its `normalization` argument: damped
+    # steps renormalise only when it is 'Wigner' (:2404-2406)
+    kvn: bool = False
+    normalization: str = 'Wigner'
 
     # derived (filled by __post_init__)
     dX: float = field(init=False)
@@ -162,7 +168,7 @@ class WignerOracle:
         self.mask1 = 1. - np.exp(-np.power(self.xk - x_max, 2) / np.power(10. * k['dx'], 2))
         self.mask2 = 1. - np.exp(-np.power(self.xk + x_max, 2) / np.power(10. * k['dx'], 2))
         self._pot_cache = None
-        self._pot_time_dependent = _has_t(prm.potential)
+        self._pot_time_dependent = _has_t(prm.dpotential if prm.kvn else prm.potential)
         # ---- Caldeira-Leggett sign(p) f(p) (theta_fp_source :399-431)
         fp = eval_expr_like(prm.fp_damping, p.shape, p=p, **k)
         self.sfp = np.where(p >= 0., fp, -fp)
@@ -177,9 +183,14 @@ class WignerOracle:
         k, prm = self.kc, self.prm
         hb = k['hBar']
         shape = (prm.n_p, prm.n_x)
-        Vm = eval_expr_like(prm.potential, shape, t=t, x=self.xk - hb * self.thk / 2., **k)
-        Vp = eval_expr_like(prm.potential, shape, t=t, x=self.xk + hb * self.thk / 2., **k)
-        phase = k['dt'] * ((Vm - Vp) / hb)
+        if prm.kvn:
+            # Potential_XTheta = -dPotential(t, x) theta; phase = dt Potential_XTheta (:41-63)
+            dV = eval_expr_like(prm.dpotential, shape, t=t, x=self.xk + 0. * self.thk, **k)
+            phase = k['dt'] * (-dV * self.thk)
+        else:
+            Vm = eval_expr_like(prm.potential, shape, t=t, x=self.xk - hb * self.thk / 2., **k)
+            Vp = eval_expr_like(prm.potential, shape, t=t, x=self.xk + hb * self.thk / 2., **k)
+            phase = k['dt'] * ((Vm - Vp) / hb)
         r = self.r_theta
         f = (r * np.cos(phase)) + 1j * (-r * np.sin(phase))
         self._pot_cache = f
@@ -292,8 +303,9 @@ class WignerOracle:
                     W = W + self.lindblad_odm(W, prm.weight2, -1.)
                 else:
                     W = W + self.lindblad_odm(W, 1., 1.)
-            norm = W.sum() * (prm.dX * prm.dP)
-            W = W * (1 / norm)
+            if not prm.kvn or prm.normalization == 'Wigner':
+                norm = W.sum() * (prm.dX * prm.dP)
+                W = W * (1 / norm)
         return W
 
     def initial_normalise(self, W_init):

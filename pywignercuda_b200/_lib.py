@@ -12,7 +12,7 @@ from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_uint3
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libwigner_b200.so')
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 WIG_NOBS = 11
 DIRAC_NOBS = 10
 WIG_RUN_CONTINUE = 1
@@ -23,6 +23,7 @@ DAMP_NONE, DAMP_CALDEIRA_LEGGETT, DAMP_ODM = 0, 1, 2
 CONST_CUDA_F, CONST_EXACT = 0, 1
 PREC_C128 = 0
 PREC_F32 = 1
+PHASE_MOYAL, PHASE_KVN = 0, 1
 
 
 class WignerError(RuntimeError):
@@ -66,12 +67,12 @@ _DP = POINTER(c_double)
 class WigDesc(ctypes.Structure):
     _fields_ = [('abi_version', c_int32), ('n_x', c_int32), ('n_p', c_int32), ('damping', c_int32),
                 ('kinetic_from_string', c_int32), ('constants', c_int32), ('precision', c_int32),
-                ('n_lindblad', c_int32),
+                ('n_lindblad', c_int32), ('potential_phase', c_int32), ('skip_normalise', c_int32),
                 ('x_amplitude', c_double), ('p_amplitude', c_double), ('hbar', c_double),
                 ('mass', c_double), ('dt', c_double), ('d_theta', c_double), ('d_lambda', c_double),
                 ('gamma', c_double), ('epsilon', c_double), ('l_material', c_double),
                 ('weight1', c_double), ('weight2', c_double),
-                ('potential', c_char_p), ('kinetic', c_char_p), ('fp_damping', c_char_p),
+                ('potential', c_char_p), ('kinetic', c_char_p), ('fp_damping', c_char_p), ('dpotential', c_char_p),
                 ('x_table', _DP), ('p_table', _DP), ('theta_table', _DP), ('lambda_table', _DP),
                 ('dv_table', _DP), ('v0_table', _DP), ('coef', c_double * 8)]
 

@@ -336,9 +336,13 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
     return fail(WIG_ERR_ARG, "n_lindblad must be 1 or 2");
   if (damped && d->damping == WIG_DAMP_ODM && !(d->l_material > 0))
     return fail(WIG_ERR_ARG, "ODM needs l_material > 0");
+  if (d->potential_phase != WIG_PHASE_MOYAL && d->potential_phase != WIG_PHASE_KVN)
+    return fail(WIG_ERR_ARG, "unknown potential_phase %d", d->potential_phase);
+  if (d->potential_phase == WIG_PHASE_KVN && damped && d->damping == WIG_DAMP_ODM)
+    return fail(WIG_ERR_UNSUPPORTED, "the KvN (Fokker-Planck) potential factor takes no ODM damping");
   const std::string V = expr_or(d->potential, "0."), K = expr_or(d->kinetic, "0.5*p*p"),
-                    F = expr_or(d->fp_damping, "fabs(p)");
-  if (!safe_expr(V) || !safe_expr(K) || !safe_expr(F))
+                    F = expr_or(d->fp_damping, "fabs(p)"), DV = expr_or(d->dpotential, "0.");
+  if (!safe_expr(V) || !safe_expr(K) || !safe_expr(F) || !safe_expr(DV))
     return fail(WIG_ERR_ARG, "expression strings may not contain ; { } # quotes or unbalanced ()");
   const int NX = d->n_x, NP = d->n_p, cm = d->constants;
   P->damp = (damped && d->damping == WIG_DAMP_CALDEIRA_LEGGETT) ? 1 : 0;
@@ -387,14 +391,16 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
   src += "\nstruct UserPhys {\n  double cf[8];\n";
   src += "  __device__ __forceinline__ double Potential(double t, double x) const { return (" + V + "); }\n";
   src += "  __device__ __forceinline__ double KineticEnergy(double p) const { return (" + K + "); }\n";
-  src += "  __device__ __forceinline__ double f(double p) const { return (" + F + "); }\n};\n";
+  src += "  __device__ __forceinline__ double f(double p) const { return (" + F + "); }\n";
+  src += "  __device__ __forceinline__ double DPotential(double t, double x) const { return (" + DV + "); }\n};\n";
   char macros[512];
   snprintf(macros, sizeof(macros),
            "#define WIG_NX %d\n#define WIG_NP %d\n#define WIG_XROWS %d\n#define WIG_XNT %d\n"
            "#define WIG_KIN_STRING %d\n#define WIG_PC %d\n#define WIG_PNT %d\n"
-           "#define WIG_DAMP %d\n#define WIG_RNT %d\n#define WIG_XMINB %d\n#define WIG_PMINB %d\n",
+           "#define WIG_DAMP %d\n#define WIG_RNT %d\n#define WIG_XMINB %d\n#define WIG_PMINB %d\n"
+           "#define WIG_KVN %d\n",
            NX, NP, P->xrows, P->xnt, d->kinetic_from_string ? 1 : 0, P->pc, P->pnt, P->damp, P->rnt,
-           P->xminb, P->pminb);
+           P->xminb, P->pminb, d->potential_phase == WIG_PHASE_KVN ? 1 : 0);
   src += macros;
   src += kJitWignerSource;
   P->src.swap(src);
@@ -571,7 +577,7 @@ static int wig_run_begin(wig_handle* h, WigRunState* S, void* W_dev, int64_t t_i
   S->t_index0 = t_index0;
   S->n_prop = n_prop;
   S->flags = flags;
-  S->damped = h->d.gamma != 0.;
+  S->damped = h->d.gamma != 0. && !h->d.skip_normalise;   // whether damped steps renormalise
   if (flags & WIG_RUN_PROFILE) {
     if (int rc = wig_profile_prepare(h, n_prop)) return rc;
   } else {

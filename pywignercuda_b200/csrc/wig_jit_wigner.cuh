@@ -15,6 +15,9 @@
 #ifndef WIG_XMINB
 #define WIG_XMINB 4
 #endif
+#ifndef WIG_KVN
+#define WIG_KVN 0
+#endif
 #include "wig_wigner.cuh"
 
 __device__ __forceinline__ UserPhys user_phys(const wig::WigArgs& a) {
@@ -32,7 +35,7 @@ wig_xpass(wig::WigArgs a, double2* W, int scale_mode, double* obs_row) {
 
 extern "C" __global__ void __launch_bounds__(WIG_PNT, WIG_PMINB)
 wig_ppass(wig::WigArgs a, double2* W, double t) {
-  wig::ppass_body<UserPhys, WIG_NX, WIG_NP, WIG_PC, WIG_PNT, WIG_DAMP>(a, user_phys(a), W, t, a.partials);
+  wig::ppass_body<UserPhys, WIG_NX, WIG_NP, WIG_PC, WIG_PNT, WIG_DAMP, WIG_KVN>(a, user_phys(a), W, t, a.partials);
 }
 
 extern "C" __global__ void __launch_bounds__(WIG_RNT)

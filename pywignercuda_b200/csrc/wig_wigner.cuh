@@ -241,9 +241,12 @@ __device__ __forceinline__ void cl_apply_D(const WigArgs& a, double2* B, const d
 }
 
 // p-pass: a tile of C columns x NP rows per CTA.  DAMP: 0 none, 1 Caldeira-Leggett.
+// KVN: 0 the Moyal factor (expPotential_source :80-126), 1 the classical
+// Liouville factor of GPU_FokkerPlank2D_FFT, phase dt (-V'(t, x) theta)
+// (exp_PotentialKvN_source :27-75).
 // Shared memory: A [padded C*NP], B [padded C*NP] and the two per-row CL
 // tables [2*NP doubles] when DAMP == 1.
-template <class Phys, int NX, int NP, int C, int NT, int DAMP>
+template <class Phys, int NX, int NP, int C, int NT, int DAMP, int KVN = 0>
 __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, double2* __restrict__ W,
                                            double t, double* __restrict__ partials) {
   typedef ColMap<C> M;
@@ -271,8 +274,9 @@ __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, dou
     const int jj = (col + NX / 2) % NX;
     const double x = a.dx * (jj - 0.5 * NX);
     const double theta = a.dtheta * (ii - 0.5 * NP);
-    const double phase = a.dt * ((ph.Potential(t, x - a.hbar * theta / 2.) -
-                                  ph.Potential(t, x + a.hbar * theta / 2.)) / a.hbar);
+    const double phase = KVN ? a.dt * (-ph.DPotential(t, x) * theta)
+                             : a.dt * ((ph.Potential(t, x - a.hbar * theta / 2.) -
+                                        ph.Potential(t, x + a.hbar * theta / 2.)) / a.hbar);
     const double r = a.r_theta[k];
     double sn, cs;
     sincos(phase, &sn, &cs);

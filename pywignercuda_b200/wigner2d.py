@@ -188,6 +188,7 @@ class GPU_Wigner2D_FFT(Propagator_Base):
     (``GPU_Wigner2D_FFT.py:1713-1964``)."""
 
     _odm2 = False
+    _kvn = False
 
     def __init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass, D_Theta, D_Lambda,
                  gammaDamping, potentialString, dPotentialString, kinematicString, normalization='Wigner'):
@@ -238,6 +239,8 @@ class GPU_Wigner2D_FFT(Propagator_Base):
         d.constants = self.constants_mode
         d.precision = _lib.PREC_C128
         d.n_lindblad = 2 if self._odm2 else 1
+        d.potential_phase = _lib.PHASE_KVN if self._kvn else _lib.PHASE_MOYAL
+        d.skip_normalise = 1 if (self._kvn and self.normalization != 'Wigner') else 0
         d.x_amplitude, d.p_amplitude = float(self.X_amplitude), float(self.P_amplitude)
         d.hbar, d.mass, d.dt = float(self.hBar), float(self.mass), float(self.dt)
         d.d_theta, d.d_lambda, d.gamma = float(self.D_Theta), float(self.D_Lambda), float(self.gammaDamping)
@@ -246,8 +249,8 @@ class GPU_Wigner2D_FFT(Propagator_Base):
         d.weight1 = float(getattr(self, 'weightLindbland1', 1.0))
         d.weight2 = float(getattr(self, 'weightLindbland2', 0.0))
         self._strings = [s.encode() for s in (self.potentialString, self.kinematicString,
-                                              self.fp_Damping_String)]
-        d.potential, d.kinetic, d.fp_damping = self._strings
+                                              self.fp_Damping_String, self.dPotentialString)]
+        d.potential, d.kinetic, d.fp_damping, d.dpotential = self._strings
         d.x_table, d.p_table = dptr(self._x_tab), dptr(self._p_tab)
         d.theta_table, d.lambda_table = dptr(self._theta_tab), dptr(self._lambda_tab)
         d.dv_table, d.v0_table = dptr(self._dv_tab), dptr(self._v0_tab)
@@ -370,3 +373,22 @@ class GPU_Wigner2D_ODM2(GPU_Wigner2D_FFT):
         GPU_Wigner2D_FFT.__init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass,
                                   D_Theta, D_Lambda, gammaDamping, potentialString, dPotentialString,
                                   kinematicString, normalization)
+
+
+class GPU_FokkerPlank2D_FFT(GPU_Wigner2D_FFT):
+    """Classical (Koopman-von Neumann / Liouville) propagator in phase space
+    with diffusion and Caldeira-Leggett damping (``GPU_Wigner2D_FFT.py:2242-2459``):
+    the Wigner step with the Moyal potential factor replaced by
+    exp(+i dt V'(t, x) theta), V' from ``dPotentialString``
+    (``exp_PotentialKvN_source`` :27-75); damped steps renormalise only when
+    ``normalization == 'Wigner'`` (:2404-2406).  The kinetic pass is the Wigner
+    one (p lambda / m); an instance may set ``kinematicString`` first, as the
+    reference's compile step expects it."""
+
+    _kvn = True
+
+    def __init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass, D_Theta, D_Lambda,
+                 gammaDamping, potentialString, dPotentialString, normalization='Wigner'):
+        GPU_Wigner2D_FFT.__init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass,
+                                  D_Theta, D_Lambda, gammaDamping, potentialString, dPotentialString,
+                                  getattr(self, 'kinematicString', '0.5*p*p'), normalization)

@@ -1,6 +1,7 @@
 """Generate the golden fixtures in this directory from the reference's own code.
 
-Runs ``GPU_Wigner2D_FFT`` / ``GPU_Wigner2D_ODM2`` / ``GPU_Dirac2D`` from the
+Runs ``GPU_Wigner2D_FFT`` / ``GPU_Wigner2D_ODM2`` / ``GPU_FokkerPlank2D_FFT`` /
+``GPU_Dirac2D`` from the
 reference checkout through ``oracle.ref_harness`` (the reference's Python-2
 host code and its CUDA-C kernel strings, compiled for the CPU; ``numpy.fft``
 standing in for cuFFT) and stores, per case:
@@ -69,6 +70,18 @@ WIGNER_CASES = {
                         gamma=0.07 / 4., damping='ODM', fp_damping=' p*p/sqrt( p*p + 0.5 ) ',
                         epsilon=0.5, L_material=3., odm2=True, weight1=1.0, weight2=0.5,
                         time_steps=60, init=('ho', 0, 1., 0., 3.)),
+    # GPU_FokkerPlank2D_FFT: classical (KvN) potential factor from the dPotential string,
+    # time-dependent force, Caldeira-Leggett, normalisation 'Wigner'
+    'fokkerplanck_kvn': dict(n_x=512, n_p=128, x_amplitude=10., p_amplitude=10., dt=0.005,
+                             potential='0.05*pow(x,4) - pow(x,2) + 0.3*sin(3.*t)*x',
+                             dpotential='0.2*pow(x,3) - 2.*x + 0.3*sin(3.*t)', gamma=0.05,
+                             d_theta=0.05, damping='CaldeiraLeggett', fp_damping=' p*p/sqrt( p*p + 0.5 ) ',
+                             kvn=True, normalization='Wigner', time_steps=100, init=('cat', 2.5, 0.7)),
+    # ... with any other normalisation: damped steps are not renormalised
+    'fokkerplanck_kvn_nonorm': dict(n_x=512, n_p=128, x_amplitude=10., p_amplitude=10., dt=0.01,
+                                    potential='0.5*pow(x,2)', dpotential='x', gamma=0.1, d_theta=0.1,
+                                    damping='CaldeiraLeggett', fp_damping='fabs(p)', kvn=True,
+                                    normalization='none', time_steps=60, init=('ho', 0, 1., 2., 0.)),
 }
 
 DIRAC_CASES = {
@@ -94,7 +107,8 @@ def run_wigner_case(name, c):
     prm_keys = {k: v for k, v in c.items() if k not in ('time_steps', 'init')}
     prm = WignerParams(**prm_keys)
     odm2 = c.get('odm2', False)
-    base = m.GPU_Wigner2D_ODM2 if odm2 else m.GPU_Wigner2D_FFT
+    kvn = c.get('kvn', False)
+    base = m.GPU_Wigner2D_ODM2 if odm2 else (m.GPU_FokkerPlank2D_FFT if kvn else m.GPU_Wigner2D_FFT)
 
     class Instance(base):
         def __init__(self):
@@ -104,7 +118,12 @@ def run_wigner_case(name, c):
             self.epsilon = prm.epsilon
             self.L_material = prm.L_material
             self.SetTimeTrack(prm.dt, c['time_steps'], 10 ** 9, fileName='/tmp/_golden_%s.hdf5' % name)
-            if odm2:
+            if kvn:
+                self.kinematicString = prm.kinetic
+                base.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude, prm.hbar,
+                              prm.mass, prm.d_theta, prm.d_lambda, prm.gamma, prm.potential,
+                              prm.dpotential, normalization=prm.normalization)
+            elif odm2:
                 base.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude, prm.hbar,
                               prm.mass, prm.d_theta, prm.d_lambda, prm.gamma, prm.weight1,
                               prm.weight2, prm.potential, prm.dpotential, prm.kinetic)

@@ -9,7 +9,7 @@ from oracle.dirac2d import DiracParams, spinor_particle_spin_up
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
 WIGNER_NAMES = ['wigner_ho_plain', 'wigner_cl_doublewell', 'wigner_cl_timedep', 'wigner_odm',
-                'wigner_odm2']
+                'wigner_odm2', 'fokkerplanck_kvn', 'fokkerplanck_kvn_nonorm']
 DIRAC_NAMES = ['dirac_coulomb', 'dirac_magnetic']
 
 

@@ -7,9 +7,9 @@ from oracle.dirac2d import DiracParams
 
 
 def wigner_instance(prm: WignerParams, W0, time_steps, skip_frames=10 ** 9, exact=False):
-    from pywignercuda_b200 import GPU_Wigner2D_FFT, GPU_Wigner2D_ODM2
+    from pywignercuda_b200 import GPU_Wigner2D_FFT, GPU_Wigner2D_ODM2, GPU_FokkerPlank2D_FFT
     from pywignercuda_b200 import _lib
-    base = GPU_Wigner2D_ODM2 if prm.odm2 else GPU_Wigner2D_FFT
+    base = GPU_Wigner2D_ODM2 if prm.odm2 else (GPU_FokkerPlank2D_FFT if prm.kvn else GPU_Wigner2D_FFT)
 
     class Instance(base):
         constants_mode = _lib.CONST_EXACT if exact else _lib.CONST_CUDA_F
@@ -21,7 +21,12 @@ def wigner_instance(prm: WignerParams, W0, time_steps, skip_frames=10 ** 9, exac
             self.epsilon = prm.epsilon
             self.L_material = prm.L_material
             self.SetTimeTrack(prm.dt, time_steps, skip_frames, fileName='')
-            if prm.odm2:
+            if prm.kvn:
+                self.kinematicString = prm.kinetic
+                base.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude, prm.hbar,
+                              prm.mass, prm.d_theta, prm.d_lambda, prm.gamma, prm.potential,
+                              prm.dpotential, normalization=prm.normalization)
+            elif prm.odm2:
                 base.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude, prm.hbar,
                               prm.mass, prm.d_theta, prm.d_lambda, prm.gamma, prm.weight1,
                               prm.weight2, prm.potential, prm.dpotential, prm.kinetic)

@@ -87,6 +87,27 @@ def test_expression_injection_refused(expr):
     assert rc == 1
 
 
+def test_kvn_phase_compiles_and_is_validated():
+    d = wig_desc(256, 256)
+    d.potential_phase = _lib.PHASE_KVN
+    d.dpotential = b'0.2*pow(x,3) - 2.*x + 0.3*sin(3.*t)'
+    rc, log = jit(d)
+    assert rc == 0, log
+    d.damping = _lib.DAMP_ODM
+    d.l_material, d.n_lindblad = 1., 1
+    rc, log = jit(d)
+    assert rc == 6 and 'ODM' in log, log            # WIG_ERR_UNSUPPORTED
+    d = wig_desc(256, 256)
+    d.potential_phase = 7
+    rc, log = jit(d)
+    assert rc == 1 and 'potential_phase' in log, log
+    d = wig_desc(256, 256)
+    d.potential_phase = _lib.PHASE_KVN
+    d.dpotential = b'x); }'
+    rc, log = jit(d)
+    assert rc == 1, log
+
+
 def test_odm_kernels_compile():
     d = wig_desc(1024, 1024, damping=_lib.DAMP_ODM, fp=b' p*p/sqrt( p*p + 0.5 ) ')
     d.n_lindblad, d.l_material = 2, 3.

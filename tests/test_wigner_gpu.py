@@ -7,15 +7,14 @@ import pytest
 from oracle.common import rel_l2
 from oracle.wigner2d import (WignerParams, WignerOracle, wigner_harmonic_oscillator,
                              wigner_cat_state)
-from golden_cases import wigner_case, obs_close
+from golden_cases import WIGNER_NAMES, wigner_case, obs_close
 from instances import wigner_instance, wigner_obs
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-10
 
 
-@pytest.mark.parametrize('name', ['wigner_ho_plain', 'wigner_cl_doublewell', 'wigner_cl_timedep',
-                                  'wigner_odm', 'wigner_odm2'])
+@pytest.mark.parametrize('name', WIGNER_NAMES)
 def test_golden(name):
     g, prm, W0, steps = wigner_case(name)
     inst = wigner_instance(prm, W0, steps)
