@@ -5,8 +5,8 @@ Headline (value): the FP32 batched form on 64 independent instances --
 square grids drawn from {128, 256, 512, 1024} with numpy default_rng(0),
 V = a x^4 + b x^2 (a ~ U[0.01, 0.1], b ~ U[-1, 0.5]), Caldeira-Leggett
 gamma ~ U[0, 0.2] with D_theta = 2 gamma m kT (kT = 0.5), coherent states at
-x0 ~ U[-2, 2], p0 ~ U[-1, 1], amplitudes 10, dt = 0.005 -- 22.3 M grid points,
-180 MB of complex64 state (larger than the 126 MB L2), all instances in one
+x0 ~ U[-2, 2], p0 ~ U[-1, 1], amplitudes 10, dt = 0.005 -- 23.4 M grid points,
+187 MB of complex64 state (larger than the 126 MB L2), all instances in one
 x-pass and one p-pass launch per step, the run replayed as one CUDA graph,
 tile shape from the autotuner.  One bench "step" = one propagation of every
 instance.
@@ -17,12 +17,17 @@ dt = 0.005), 16 replicas stepped in lock-step (256 MB > L2); the ratio of the
 two is the metric's "FP32 batched vs plain complex128".  drift_vs_fp64 states
 the FP32 run's norm / energy error against a complex128 run of every instance.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload batch|c128|dirac]
+Other workloads: --workload c128 (the plain line alone), dirac (Dirac2D 512^2,
+16 replicas), gp (GPU_Wigner2D_GPitaevskii: Strang splitting + mean-field term
+on the 1024^2 double well, 16 replicas).
 
-N > 1 (torchrun): each rank runs its own copy of the workload (weak scaling;
-the instances are independent, no data-path collective); time = max over
-ranks.  --impl reference times the oracle's CPU restatement of the reference
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload batch|c128|dirac|gp]
+
+N > 1 (torchrun): the batch has 64 N instances partitioned by cost across the
+ranks (weak scaling; no data-path collective, the observables are gathered to
+rank 0); the replica workloads run their replicas on every rank; time = max
+over ranks.  --impl reference times the oracle's CPU restatement of the reference
 propagator (complex128, numpy + scipy.fft, all host cores) on a sample of the
 same batch; rank 0 only.
 """
@@ -353,6 +358,83 @@ def run_c128(args, world, rank, local, steps=None, emit=True):
     return res
 
 
+GP_COEF = 0.5
+GP_BYTES = 160   # per grid point per Strang step: 3 passes x 32 B, 2 column-sum reads x 16 B, 2 x (8 + 8) B phase
+
+
+def make_gp_instance(time_steps):
+    from pywignercuda_b200 import GPU_Wigner2D_GPitaevskii
+
+    class MeanField(GPU_Wigner2D_GPitaevskii):
+        def __init__(self):
+            self.dampingFunction = 'CaldeiraLeggett'
+            self.GPitaevskiiCoeff = GP_COEF
+            self.fp_Damping_String = 'fabs(p)'
+            self.SetTimeTrack(DT, time_steps, 10 ** 9, fileName='')
+            GPU_Wigner2D_GPitaevskii.__init__(self, NX, NP, AMP, AMP, 1., 1., D_THETA, 0., GAMMA, POT, DPOT,
+                                              '0.5*p*p')
+    return MeanField()
+
+
+def run_gp(args, world, rank, local):
+    """GPU_Wigner2D_GPitaevskii on the 1024x1024 double well: Strang splitting,
+    mean-field coefficient 0.5, Caldeira-Leggett, complex128, R replicas."""
+    import ctypes
+    import torch
+    from pywignercuda_b200 import _lib
+    from oracle.gpitaevskii import GPitaevskiiOracle
+    from oracle.wigner2d import WignerParams
+    lib = _lib.load()
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    R, steps = args.replicas, args.steps
+    insts = [make_gp_instance(steps) for _ in range(R)]
+    W0 = cat_state(insts[0])
+    Ws = [torch.from_numpy(W0.astype(np.complex128)).to(dev) for _ in range(R)]
+    stream = torch.cuda.current_stream(dev)
+    hs = (ctypes.c_void_p * R)(*[i._handle.value for i in insts])
+    ws = (ctypes.c_void_p * R)(*[w.data_ptr() for w in Ws])
+    _lib.check(lib.wig_run_many(hs, ws, R, 0, args.warmup, 0, None, stream.cuda_stream), 'warm-up')
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        _lib.check(lib.wig_run_many(hs, ws, R, args.warmup, steps, _lib.WIG_RUN_CONTINUE, None,
+                                    stream.cuda_stream), 'timed')
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = barrier_max(world, e0.elapsed_time(e1))
+    value = world * R * NX * NP * steps / (ms / 1e3)
+    peak, peak_kind = peaks()
+    achieved = GP_BYTES * NX * NP / (ms / 1e3 / (R * steps)) / 1e9
+    line = {'metric': 'Wigner2D grid-pt-steps/s (Strang + Gross-Pitaevskii, complex128)', 'value': value,
+            'unit': UNIT, 'n_gpus': world, 'steps': steps, 'warmup': args.warmup, 'ms_per_step': ms / steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c128',
+            'data': 'synthetic',
+            'config': {'workload': 'GPU_Wigner2D_GPitaevskii 1024x1024 double well V=0.05x^4-x^2, a_GP=0.5, '
+                                   'Caldeira-Leggett gamma=0.1 D_theta=0.1 f=|p|, cat state, dt=0.005',
+                       'replicas_per_gpu': R, 'l2': 'per-step working set %d MB > 126 MB L2' % (R * 24)},
+            'roofline': {'bound': 'hbm', 'kernel': 'Strang step (9 launches, step average)',
+                         'algorithmic_bytes_per_point': GP_BYTES, 'achieved': achieved, 'peak': peak,
+                         'unit': 'GB/s', 'frac': achieved / peak, 'peak_kind': peak_kind, 'traffic': None},
+            'gpu_launches': R * 9 * steps, 'clocks': clk.summary()}
+    if rank == 0 and args.cpu_baseline:
+        prm = WignerParams(NX, NP, AMP, AMP, DT, potential=POT, dpotential=DPOT, kinetic='0.5*p*p', gamma=GAMMA,
+                           d_theta=D_THETA, damping='CaldeiraLeggett', fp_damping='fabs(p)')
+        orc = GPitaevskiiOracle(prm, GP_COEF)
+        W = orc.initial_normalise(W0)
+        t0, n = time.perf_counter(), 0
+        while time.perf_counter() - t0 < 10. or n < 1:
+            W, _ = orc.step_gp(W, n * DT)
+            n += 1
+        el = time.perf_counter() - t0
+        line['cpu_baseline'] = {'value': NX * NP * n / el, 'unit': UNIT, 'cores': os.cpu_count(), 'kind': 'port',
+                                'sample': '%d Strang + GP steps of one 1024^2 instance (%.1f s)' % (n, el)}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def run_batch(args, world, rank, local):
     """Headline: the FP32 batched form on the 64-instance mixed-grid batch.  With
     N ranks the batch has 64 N instances (the same generator; N = 1 is the
@@ -536,7 +618,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--replicas', type=int, default=REPLICAS)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
-    ap.add_argument('--workload', default='batch', choices=['batch', 'c128', 'dirac'])
+    ap.add_argument('--workload', default='batch', choices=['batch', 'c128', 'dirac', 'gp'])
     ap.add_argument('--profile-only', action='store_true',
                     help='batch workload: only the timed section (for profiler launch lists)')
     args = ap.parse_args()
@@ -549,6 +631,8 @@ def main():
             run_dirac(args, world, rank, local)
         elif args.workload == 'c128':
             run_c128(args, world, rank, local)
+        elif args.workload == 'gp':
+            run_gp(args, world, rank, local)
         else:
             run_batch(args, world, rank, local)
     finally:

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define WIG_ABI_VERSION 2
+#define WIG_ABI_VERSION 3
 
 enum wig_status {
   WIG_OK = 0,
@@ -59,6 +59,14 @@ enum wig_constants {
 };
 
 enum wig_precision { WIG_PREC_C128 = 0, WIG_PREC_F32 = 1 };
+
+enum wig_splitting {
+  WIG_SPLIT_LIE = 0,       /* kinetic then potential (GPU_Wigner2D_FFT.Run :1884-1913)           */
+  WIG_SPLIT_STRANG_GP = 1  /* half potential, kinetic, half potential, each half with the
+                              Gross-Pitaevskii term when gp_coefficient != 0; observables after
+                              every step (GPU_Wigner2D_GPitaevskii.Run, GPU_Wigner2D_GPitaevskii.py
+                              :1897-1990)                                                         */
+};
 
 enum wig_potential_phase {
   WIG_PHASE_MOYAL = 0, /* exp(-i dt [V(x - hbar theta/2) - V(x + hbar theta/2)] / hbar)
@@ -94,11 +102,14 @@ typedef struct wig_desc {
   int32_t potential_phase;     /* wig_potential_phase (KvN: damping none or Caldeira-Leggett) */
   int32_t skip_normalise;      /* 1: damped steps are not renormalised (GPU_FokkerPlank2D_FFT
                                   with normalization != 'Wigner', :2404-2406)           */
+  int32_t splitting;           /* wig_splitting (Strang: Moyal phase only)              */
+  int32_t reserved0;
   double x_amplitude, p_amplitude;
   double hbar, mass, dt;
   double d_theta, d_lambda, gamma;
   double epsilon, l_material;  /* ODM (SetA_ODM :1206)                              */
   double weight1, weight2;     /* ODM2 Lindblad weights (:2169-2176)                 */
+  double gp_coefficient;       /* GPitaevskiiCoeff a_GP (WIG_SPLIT_STRANG_GP)          */
   const char* potential;       /* potentialString, C expression in (t, x)           */
   const char* kinetic;         /* kinematicString, C expression in p                */
   const char* fp_damping;      /* fp_Damping_String, C expression in p              */
@@ -295,6 +306,12 @@ int wiga_destroy(wiga_handle* h);
 
 /* Compile-only check (no GPU) of the adjoint kernels for the descriptor's grid. */
 int wiga_jit_check(const wiga_desc* desc, char* log, int64_t log_cap);
+
+/* WIG_SPLIT_STRANG_GP with gp_coefficient != 0: the per-step sum_x P(x)^2 dx of
+ * the x-marginal P after each kinetic step of the last wig_run on this handle
+ * (GPU_Wigner2D_GPitaevskii ProbabilitySquare_average, :1951); n <= that run's
+ * n_prop values into out (host).  Synchronises the handle's last stream. */
+int wig_run_probability_square(wig_handle* h, double* out, int64_t n);
 
 /* Compile-only check of an instance's kernels: builds the JIT source the way
  * wig_create / dirac_create do and compiles it with NVRTC for sm_100a without

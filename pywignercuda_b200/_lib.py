@@ -12,7 +12,7 @@ from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_uint3
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libwigner_b200.so')
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 WIG_NOBS = 11
 DIRAC_NOBS = 10
 WIG_RUN_CONTINUE = 1
@@ -24,6 +24,7 @@ CONST_CUDA_F, CONST_EXACT = 0, 1
 PREC_C128 = 0
 PREC_F32 = 1
 PHASE_MOYAL, PHASE_KVN = 0, 1
+SPLIT_LIE, SPLIT_STRANG_GP = 0, 1
 
 
 class WignerError(RuntimeError):
@@ -68,10 +69,11 @@ class WigDesc(ctypes.Structure):
     _fields_ = [('abi_version', c_int32), ('n_x', c_int32), ('n_p', c_int32), ('damping', c_int32),
                 ('kinetic_from_string', c_int32), ('constants', c_int32), ('precision', c_int32),
                 ('n_lindblad', c_int32), ('potential_phase', c_int32), ('skip_normalise', c_int32),
+                ('splitting', c_int32), ('reserved0', c_int32),
                 ('x_amplitude', c_double), ('p_amplitude', c_double), ('hbar', c_double),
                 ('mass', c_double), ('dt', c_double), ('d_theta', c_double), ('d_lambda', c_double),
                 ('gamma', c_double), ('epsilon', c_double), ('l_material', c_double),
-                ('weight1', c_double), ('weight2', c_double),
+                ('weight1', c_double), ('weight2', c_double), ('gp_coefficient', c_double),
                 ('potential', c_char_p), ('kinetic', c_char_p), ('fp_damping', c_char_p), ('dpotential', c_char_p),
                 ('x_table', _DP), ('p_table', _DP), ('theta_table', _DP), ('lambda_table', _DP),
                 ('dv_table', _DP), ('v0_table', _DP), ('coef', c_double * 8)]
@@ -109,6 +111,7 @@ SIGNATURES = [
     ('wig_run_many', c_int, [POINTER(c_void_p), POINTER(c_void_p), c_int64, c_int64, c_int64, c_uint32,
                              POINTER(_DP), c_void_p]),
     ('wig_profile', c_int, [c_void_p, _DP, POINTER(c_int64)]),
+    ('wig_run_probability_square', c_int, [c_void_p, _DP, c_int64]),
     ('wig_destroy', c_int, [c_void_p]),
     ('dirac_create', c_int, [POINTER(DiracDesc), POINTER(c_void_p)]),
     ('dirac_run', c_int, [c_void_p, c_void_p, c_int64, c_int64, _DP, c_void_p]),

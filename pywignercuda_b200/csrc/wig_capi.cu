@@ -208,6 +208,12 @@ int launch(CUfunction f, unsigned grid, unsigned block, unsigned smem, cudaStrea
   return WIG_OK;
 }
 
+int launch2d(CUfunction f, unsigned gx, unsigned gy, unsigned block, unsigned smem, cudaStream_t st, void** args) {
+  CUresult r = g_drv.launch(f, gx, gy, 1, block, 1, 1, smem, (CUstream)st, args, nullptr);
+  if (r != CUDA_SUCCESS) return fail(WIG_ERR_CUDA, "cuLaunchKernel: %s", cu_err(r));
+  return WIG_OK;
+}
+
 // ------------------------------------------------------------------ helpers
 bool pow2_in_range(int n) { return n >= 16 && n <= 4096 && (n & (n - 1)) == 0; }
 int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -294,6 +300,16 @@ struct wig_handle {
   wig::WigArgs a{};
   CUfunction f_x = nullptr, f_p = nullptr, f_r = nullptr, f_fin = nullptr, f_scale = nullptr;
   CUfunction f_ox = nullptr, f_op = nullptr;   // ODM passes
+  // Strang / Gross-Pitaevskii (GPU_Wigner2D_GPitaevskii)
+  int strang = 0, gp = 0, smem_ph = 0, smem_gph = 0, n_chunks = 0;
+  CUfunction f_ph = nullptr, f_phf = nullptr, f_gcs = nullptr, f_gm = nullptr, f_gph = nullptr;
+  double2* gp_chunks = nullptr;                // [n_p/16][n_x] column sums
+  double* gp_P = nullptr;                      // [n_x] marginal
+  double* gp_phase = nullptr;                  // [n_p][n_x]
+  double* psq = nullptr;                       // per-step sum_x P^2 dx of the last run
+  size_t psq_cap = 0;
+  int64_t psq_n = 0;
+  cudaStream_t last_stream = nullptr;
   int odm = 0, smem_odm_x = 0, smem_odm_p = 0;
   double2* odm_T = nullptr;                    // 5 planes of ODM intermediates
   double odm_coef[2] = {0., 0.}, odm_sign[2] = {1., -1.};
@@ -312,6 +328,7 @@ struct wig_handle {
 // Validation, tiling and the JIT source of one Wigner instance (no CUDA calls).
 struct WigPlan {
   int xrows, xnt, pc, pnt, rnt, n_cta_x, n_cta_p, n_cta_r, smem_x, smem_p, damp;
+  int strang, gp, smem_ph, smem_gph;
   int xminb, pminb;
   int odm, smem_odm_x, smem_odm_p;
   double dX, dP, dTheta, dLambda;
@@ -340,6 +357,13 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
     return fail(WIG_ERR_ARG, "unknown potential_phase %d", d->potential_phase);
   if (d->potential_phase == WIG_PHASE_KVN && damped && d->damping == WIG_DAMP_ODM)
     return fail(WIG_ERR_UNSUPPORTED, "the KvN (Fokker-Planck) potential factor takes no ODM damping");
+  if (d->splitting != WIG_SPLIT_LIE && d->splitting != WIG_SPLIT_STRANG_GP)
+    return fail(WIG_ERR_ARG, "unknown splitting %d", d->splitting);
+  if (d->splitting == WIG_SPLIT_STRANG_GP && d->potential_phase != WIG_PHASE_MOYAL)
+    return fail(WIG_ERR_UNSUPPORTED, "Strang splitting takes the Moyal potential factor only");
+  if (d->splitting != WIG_SPLIT_STRANG_GP && d->gp_coefficient != 0.)
+    return fail(WIG_ERR_ARG, "gp_coefficient needs WIG_SPLIT_STRANG_GP");
+  if (!std::isfinite(d->gp_coefficient)) return fail(WIG_ERR_ARG, "gp_coefficient must be finite");
   const std::string V = expr_or(d->potential, "0."), K = expr_or(d->kinetic, "0.5*p*p"),
                     F = expr_or(d->fp_damping, "fabs(p)"), DV = expr_or(d->dpotential, "0.");
   if (!safe_expr(V) || !safe_expr(K) || !safe_expr(F) || !safe_expr(DV))
@@ -377,6 +401,10 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
   P->smem_p = P->damp ? 2 * tile_p + 2 * NP * (int)sizeof(double) : tile_p;
   P->smem_odm_x = 2 * tile_x;
   P->smem_odm_p = 2 * tile_p;
+  P->strang = d->splitting == WIG_SPLIT_STRANG_GP ? 1 : 0;
+  P->gp = (P->strang && d->gp_coefficient != 0.) ? 1 : 0;
+  P->smem_ph = tile_p;                                                     // first half: no damping
+  P->smem_gph = (wig::padded_size(NX) + wig::padded_size(P->xrows * NX)) * (int)sizeof(double2);
 
   // ---- JIT source
   P->dX = 2. * d->x_amplitude / (double)NX;
@@ -398,9 +426,9 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
            "#define WIG_NX %d\n#define WIG_NP %d\n#define WIG_XROWS %d\n#define WIG_XNT %d\n"
            "#define WIG_KIN_STRING %d\n#define WIG_PC %d\n#define WIG_PNT %d\n"
            "#define WIG_DAMP %d\n#define WIG_RNT %d\n#define WIG_XMINB %d\n#define WIG_PMINB %d\n"
-           "#define WIG_KVN %d\n",
+           "#define WIG_KVN %d\n#define WIG_STRANG %d\n",
            NX, NP, P->xrows, P->xnt, d->kinetic_from_string ? 1 : 0, P->pc, P->pnt, P->damp, P->rnt,
-           P->xminb, P->pminb, d->potential_phase == WIG_PHASE_KVN ? 1 : 0);
+           P->xminb, P->pminb, d->potential_phase == WIG_PHASE_KVN ? 1 : 0, P->strang);
   src += macros;
   src += kJitWignerSource;
   P->src.swap(src);
@@ -447,6 +475,13 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   if (!rc) rc = get_fn(mod, "wig_setup", &f_setup, 0);
   if (!rc && h->odm) rc = get_fn(mod, "wig_odm_xpass", &h->f_ox, h->smem_odm_x);
   if (!rc && h->odm) rc = get_fn(mod, "wig_odm_ppass", &h->f_op, h->smem_odm_p);
+  h->strang = P.strang; h->gp = P.gp; h->smem_ph = P.smem_ph; h->smem_gph = P.smem_gph;
+  h->n_chunks = NP / 16;
+  if (!rc && h->strang) rc = get_fn(mod, "wig_ppass_half", &h->f_ph, h->smem_ph);
+  if (!rc && h->strang) rc = get_fn(mod, "wig_ppass_half_final", &h->f_phf, h->smem_p);
+  if (!rc && h->gp) rc = get_fn(mod, "wig_gp_colsum", &h->f_gcs, 0);
+  if (!rc && h->gp) rc = get_fn(mod, "wig_gp_marginal", &h->f_gm, 0);
+  if (!rc && h->gp) rc = get_fn(mod, "wig_gp_phase", &h->f_gph, h->smem_gph);
   if (rc) { delete h; return rc; }
 
   // ---- kernel arguments and tables
@@ -499,7 +534,14 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   double* lam_d = nullptr;
   if (!rc) rc = B.alloc(&lam_d, NX, lt.data());
   if (!rc && h->odm) rc = B.alloc(&h->odm_T, 5 * (size_t)NX * NP);
+  double* rth_d = nullptr;
+  if (!rc) rc = B.alloc(&rth_d, NP);
+  if (!rc && h->gp) rc = B.alloc(&h->gp_chunks, (size_t)h->n_chunks * NX);
+  if (!rc && h->gp) rc = B.alloc(&h->gp_P, NX);
+  if (!rc && h->gp) rc = B.alloc(&h->gp_phase, (size_t)NX * NP);
   if (rc) { B.free_all(); delete h; return rc; }
+  a.r_theta_half = rth_d;
+  a.gp_coef = kval(d->gp_coefficient, cm);
   a.lambda_tab = lam_d;
   a.hbar_exact = d->hbar;
   a.L_material = d->l_material;
@@ -511,7 +553,7 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   a.r_lambda = rl_d; a.r_theta = rt_d; a.mask1 = m1_d; a.mask2s = m2_d; a.sfp = sfp_d;
   a.tw_x = twx_d; a.tw_p = twp_d; a.partials = part_d; a.n_partials = 0;
   {
-    void* args[] = {&a, &rl_d, &rt_d, &m1_d, &m2_d, &sfp_d};
+    void* args[] = {&a, &rl_d, &rt_d, &m1_d, &m2_d, &sfp_d, &rth_d};
     rc = launch(f_setup, 8, 256, 0, 0, args);
     if (!rc) {
       cudaError_t e = cudaDeviceSynchronize();
@@ -556,6 +598,8 @@ static int wig_run_check(wig_handle* h, void* W_dev, int64_t n_prop) {
   WIG_CUDA(cudaGetDevice(&cur));
   if (cur != h->device) return fail(WIG_ERR_ARG, "wig_run: current device %d != handle device %d", cur, h->device);
   if (int rc = ensure_obs(&h->obs, &h->obs_cap, (size_t)(n_prop + 1) * WIG_NOBS)) return rc;
+  if (h->gp)
+    if (int rc = ensure_obs(&h->psq, &h->psq_cap, (size_t)std::max<int64_t>(n_prop, 1))) return rc;
   return WIG_OK;
 }
 
@@ -589,7 +633,59 @@ static int wig_run_begin(wig_handle* h, WigRunState* S, void* W_dev, int64_t t_i
   return WIG_OK;
 }
 
+// Gross-Pitaevskii phase of the current W into h->gp_phase: column sums, the
+// marginal (with the pending normalisation of scale_mode; psq_out may be null)
+// and the per-row phase.
+static int wig_gp_terms(wig_handle* h, WigRunState* S, int scale_mode, double* psq_out, cudaStream_t st) {
+  const int NX = h->d.n_x, NP = h->d.n_p, cnt = NX < 256 ? NX : 256;
+  void* cargs[] = {&S->W, &h->gp_chunks};   // grid: columns x row chunks of 16
+  if (int rc = launch2d(h->f_gcs, (unsigned)(NX / cnt), (unsigned)(NP / 16), (unsigned)cnt, 0, st, cargs)) return rc;
+  int nch = h->n_chunks;
+  void* margs[] = {&S->a, &h->gp_chunks, &nch, &scale_mode, &h->gp_P, &psq_out};
+  if (int rc = launch(h->f_gm, 1, 256, 0, st, margs)) return rc;
+  void* pargs[] = {&S->a, &h->gp_P, &h->gp_phase};
+  return launch(h->f_gph, h->n_cta_x, h->xnt, h->smem_gph, st, pargs);
+}
+
+// One step of GPU_Wigner2D_GPitaevskii.Run (:1897-1975): [GP terms] half
+// potential -> kinetic -> [GP terms] half potential -> damping.  The first
+// half consumes the previous partials (sample n, normalisation on load).
+static int wig_run_step_strang(wig_handle* h, WigRunState* S, int64_t n, cudaStream_t st) {
+  const int first = (S->flags & WIG_RUN_CONTINUE) ? 0 : 1;
+  int mode = (n == 0) ? first : (S->damped ? 2 : 0);
+  double* obs_row = h->obs + (size_t)n * WIG_NOBS;
+  const bool prof = h->ev_used != 0;
+  double t = (double)(S->t_index0 + n) * h->d.dt;
+  double* gph = h->gp ? h->gp_phase : nullptr;
+  if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n], st));
+  if (h->gp)
+    if (int rc = wig_gp_terms(h, S, mode, nullptr, st)) return rc;
+  void* hargs[] = {&S->a, &S->W, &t, &mode, &obs_row, &gph};
+  if (int rc = launch(h->f_ph, h->n_cta_p, h->pnt, h->smem_ph, st, hargs)) return rc;
+  int zero = 0;
+  double* none = nullptr;
+  void* xargs[] = {&S->a, &S->W, &zero, &none};
+  if (int rc = launch(h->f_x, h->n_cta_x, h->xnt, h->smem_x, st, xargs)) return rc;
+  if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 1], st));
+  if (h->gp)
+    if (int rc = wig_gp_terms(h, S, 0, h->psq + n, st)) return rc;
+  void* fargs[] = {&S->a, &S->W, &t, &gph};
+  if (int rc = launch(h->f_phf, h->n_cta_p, h->pnt, h->smem_p, st, fargs)) return rc;
+  if (h->odm) {
+    // Lindbladian_ODM_Order1 with weight 1, sign 1 (GPU_Wigner2D_GPitaevskii.Run :1966-1969)
+    void* oxargs[] = {&S->a, &S->W, &h->odm_T};
+    if (int rc = launch(h->f_ox, h->n_cta_x, h->xnt, h->smem_odm_x, st, oxargs)) return rc;
+    double coef = h->odm_coef[0], sign = 1.;
+    void* opargs[] = {&S->a, &S->W, &h->odm_T, &coef, &sign};
+    if (int rc = launch(h->f_op, h->n_cta_p, h->pnt, h->smem_odm_p, st, opargs)) return rc;
+  }
+  if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 2], st));
+  S->a.n_partials = h->n_cta_p;
+  return WIG_OK;
+}
+
 static int wig_run_step(wig_handle* h, WigRunState* S, int64_t n, cudaStream_t st) {
+  if (h->strang) return wig_run_step_strang(h, S, n, st);
   const int first = (S->flags & WIG_RUN_CONTINUE) ? 0 : 1;
   int mode = (n == 0) ? first : (S->damped ? 2 : 0);
   double* obs_row = h->obs + (size_t)n * WIG_NOBS;
@@ -645,11 +741,23 @@ extern "C" int wig_run(wig_handle* h, void* W_dev, int64_t t_index0, int64_t n_p
   for (int64_t n = 0; n < n_prop; ++n)
     if (int rc = wig_run_step(h, &S, n, st)) return rc;
   if (int rc = wig_run_end(h, &S, st)) return rc;
+  h->psq_n = n_prop;
+  h->last_stream = st;
   if (obs_host) {
     if (int rc = wig_copy_obs(h, n_prop, obs_host, st)) return rc;
     WIG_CUDA(cudaStreamSynchronize(st));
     return check_finite(obs_host, (size_t)(n_prop + 1) * WIG_NOBS, "wig_run observables");
   }
+  return WIG_OK;
+}
+
+extern "C" int wig_run_probability_square(wig_handle* h, double* out, int64_t n) {
+  if (!h || !out || n < 0) return fail(WIG_ERR_ARG, "wig_run_probability_square: bad arguments");
+  if (!h->gp) return fail(WIG_ERR_ARG, "wig_run_probability_square: the handle has no Gross-Pitaevskii term");
+  if (n > h->psq_n) return fail(WIG_ERR_ARG, "wig_run_probability_square: %lld values asked, the last run made %lld",
+                                (long long)n, (long long)h->psq_n);
+  WIG_CUDA(cudaStreamSynchronize(h->last_stream));
+  if (n) WIG_CUDA(cudaMemcpy(out, h->psq, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
   return WIG_OK;
 }
 

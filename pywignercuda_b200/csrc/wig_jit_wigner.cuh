@@ -18,6 +18,9 @@
 #ifndef WIG_KVN
 #define WIG_KVN 0
 #endif
+#ifndef WIG_STRANG
+#define WIG_STRANG 0
+#endif
 #include "wig_wigner.cuh"
 
 __device__ __forceinline__ UserPhys user_phys(const wig::WigArgs& a) {
@@ -37,6 +40,41 @@ extern "C" __global__ void __launch_bounds__(WIG_PNT, WIG_PMINB)
 wig_ppass(wig::WigArgs a, double2* W, double t) {
   wig::ppass_body<UserPhys, WIG_NX, WIG_NP, WIG_PC, WIG_PNT, WIG_DAMP, WIG_KVN>(a, user_phys(a), W, t, a.partials);
 }
+
+#if WIG_STRANG
+// Strang-split step of GPU_Wigner2D_GPitaevskii (:1897-1975): first half p-pass
+// (consumes the previous partials, normalises on load, records the sample),
+// then -- after the kinetic x-pass -- the final half p-pass with the damping
+// and the partial sums.  gp_phase: the Gross-Pitaevskii phase array or null.
+extern "C" __global__ void __launch_bounds__(WIG_PNT, WIG_PMINB)
+wig_ppass_half(wig::WigArgs a, double2* W, double t, int scale_mode, double* obs_row, const double* gp_phase) {
+  wig::ppass_body<UserPhys, WIG_NX, WIG_NP, WIG_PC, WIG_PNT, 0, 0, 1, 0>(a, user_phys(a), W, t, a.partials,
+                                                                        scale_mode, obs_row, gp_phase);
+}
+
+extern "C" __global__ void __launch_bounds__(WIG_PNT, WIG_PMINB)
+wig_ppass_half_final(wig::WigArgs a, double2* W, double t, const double* gp_phase) {
+  wig::ppass_body<UserPhys, WIG_NX, WIG_NP, WIG_PC, WIG_PNT, WIG_DAMP, 0, 1, 1>(a, user_phys(a), W, t, a.partials,
+                                                                                0, nullptr, gp_phase);
+}
+
+#define WIG_GP_RCH 16
+#define WIG_GP_CNT (WIG_NX < 256 ? WIG_NX : 256)
+extern "C" __global__ void __launch_bounds__(WIG_GP_CNT)
+wig_gp_colsum(const double2* W, double2* chunks) {
+  wig::colsum_body<WIG_NX, WIG_NP, WIG_GP_RCH, WIG_GP_CNT>(W, chunks);
+}
+
+extern "C" __global__ void __launch_bounds__(256)
+wig_gp_marginal(wig::WigArgs a, const double2* chunks, int n_chunks, int scale_mode, double* P, double* psq) {
+  wig::gp_marginal_body<WIG_NX, 256>(a, chunks, n_chunks, scale_mode, P, psq);
+}
+
+extern "C" __global__ void __launch_bounds__(WIG_XNT)
+wig_gp_phase(wig::WigArgs a, const double* P, double* phase_out) {
+  wig::gp_phase_body<WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT>(a, P, phase_out);
+}
+#endif
 
 extern "C" __global__ void __launch_bounds__(WIG_RNT)
 wig_reduce(wig::WigArgs a, const double2* W) {
@@ -69,8 +107,9 @@ wig_odm_ppass(wig::WigArgs a, double2* W, const double2* T, double coef, double 
 //   r_theta   exp(-D_Theta theta^2 dt)           expPotential_source :117
 //   mask1/2   1 - exp(-(x -+ x_max)^2/(10 dx)^2)  expPotential_source :121-123
 //   sfp       sign(p) f(p)                       theta_fp_source :422-428
+//   r_theta_half exp(-0.5 D_Theta theta^2 dt)    (Strang half step)
 extern "C" __global__ void wig_setup(wig::WigArgs a, double* r_lambda, double* r_theta, double* mask1,
-                                     double* mask2s, double* sfp) {
+                                     double* mask2s, double* sfp, double* r_theta_half) {
   const UserPhys ph = user_phys(a);
   const int NX = WIG_NX, NP = WIG_NP;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < NX; k += gridDim.x * blockDim.x) {
@@ -86,6 +125,7 @@ extern "C" __global__ void wig_setup(wig::WigArgs a, double* r_lambda, double* r
     const int ii = (k + NP / 2) % NP;
     const double theta = dtheta * (ii - 0.5 * NP);
     r_theta[k] = exp(-D_Theta * theta * theta * dt);
+    r_theta_half[k] = exp(-0.5 * D_Theta * theta * theta * dt);   // GPU_Wigner2D_GPitaevskii :66
     const double p = dp * (ii - 0.5 * NP);
     sfp[k] = (p >= 0.) ? ph.f(p) : -ph.f(p);
   }

@@ -55,6 +55,9 @@ struct WigArgs {
   // ODM Lindblad damping (SetA_ODM :1206-1244, _Lindbladian_ODM :1516-1634), exact host values
   const double* lambda_tab; // [n_x] exact shifted Lambda
   double hbar_exact, L_material;
+  // Strang splitting / Gross-Pitaevskii (GPU_Wigner2D_GPitaevskii)
+  const double* r_theta_half;  // [n_p] exp(-0.5 D_Theta theta^2 dt)  (expPotential_source :66)
+  double gp_coef;              // a_GP as the kernels see it
   double coef[8];           // cf[0..7] of the expression strings
 };
 
@@ -246,9 +249,18 @@ __device__ __forceinline__ void cl_apply_D(const WigArgs& a, double2* B, const d
 // (exp_PotentialKvN_source :27-75).
 // Shared memory: A [padded C*NP], B [padded C*NP] and the two per-row CL
 // tables [2*NP doubles] when DAMP == 1.
-template <class Phys, int NX, int NP, int C, int NT, int DAMP, int KVN = 0>
+// Strang / Gross-Pitaevskii variant (GPU_Wigner2D_GPitaevskii.Run :1897-1975):
+// HALF = 1 takes half the Moyal phase and exp(-0.5 D_Theta theta^2 dt)
+// (expPotential_source Kernel :59-88); FINAL = 0 stops after the column IFFT
+// (no damping, no partial sums).  scale_mode / obs_row: reduce the previous
+// pass's partials, apply the pending normalisation on load and record that
+// sample (the x-pass does this in the Lie step).  gp_phase (may be null): the
+// Gross-Pitaevskii phase per (theta row, x column), applied as exp(i phase)
+// (expPotential_GrossPitaevskii_source Kernel :466-495).
+template <class Phys, int NX, int NP, int C, int NT, int DAMP, int KVN = 0, int HALF = 0, int FINAL = 1>
 __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, double2* __restrict__ W,
-                                           double t, double* __restrict__ partials) {
+                                           double t, double* __restrict__ partials, int scale_mode = 0,
+                                           double* obs_row = nullptr, const double* __restrict__ gp_phase = nullptr) {
   typedef ColMap<C> M;
   constexpr int TILE = padded_size(C * NP);
   extern __shared__ double2 sm[];
@@ -258,12 +270,17 @@ __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, dou
   double* sfp = reinterpret_cast<double*>(sm + 2 * TILE);
   double* ths = sfp + NP;
   const int col0 = blockIdx.x * C;
+  double2 s = make_double2(1., 0.);
+  if (scale_mode != 0 || (obs_row != nullptr && blockIdx.x == 0))
+    s = consume_partials<NT>(a, scale_mode, blockIdx.x == 0 ? obs_row : nullptr, red);
   if (DAMP == 1) {
     for (int k = threadIdx.x; k < NP; k += NT) { sfp[k] = a.sfp[k]; ths[k] = a.theta_s[k]; }
   }
   for (int e = threadIdx.x; e < C * NP; e += NT) {
     const int k = e / C, c = e - k * C;
-    A[pad8(e)] = W[(size_t)k * NX + col0 + c];
+    double2 v = W[(size_t)k * NX + col0 + c];
+    if (scale_mode != 0) v = cmul(v, s);
+    A[pad8(e)] = v;
   }
   __syncthreads();
   cta_fft<double2, NP, C, NT, false, M>(A, a.tw_p);
@@ -275,18 +292,30 @@ __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, dou
     const double x = a.dx * (jj - 0.5 * NX);
     const double theta = a.dtheta * (ii - 0.5 * NP);
     const double phase = KVN ? a.dt * (-ph.DPotential(t, x) * theta)
-                             : a.dt * ((ph.Potential(t, x - a.hbar * theta / 2.) -
-                                        ph.Potential(t, x + a.hbar * theta / 2.)) / a.hbar);
-    const double r = a.r_theta[k];
+                       : (HALF ? 0.5 * a.dt : a.dt) * ((ph.Potential(t, x - a.hbar * theta / 2.) -
+                                                        ph.Potential(t, x + a.hbar * theta / 2.)) / a.hbar);
+    const double r = HALF ? a.r_theta_half[k] : a.r_theta[k];
     double sn, cs;
     sincos(phase, &sn, &cs);
     double2 v = cmul(A[pad8(e)], make_double2(r * cs, -r * sn));
     v = cscale(v, a.mask1[col]);
     v = cscale(v, a.mask2s[col]);
+    if (gp_phase != nullptr) {
+      double gs, gc;
+      sincos(gp_phase[(size_t)k * NX + col], &gs, &gc);
+      v = cmul(v, make_double2(gc, gs));
+    }
     A[pad8(e)] = v;
   }
   __syncthreads();
   cta_fft<double2, NP, C, NT, true, M>(A, a.tw_p);
+  if (!FINAL) {
+    for (int e = threadIdx.x; e < C * NP; e += NT) {
+      const int k = e / C, c = e - k * C;
+      W[(size_t)k * NX + col0 + c] = A[pad8(e)];
+    }
+    return;
+  }
   if (DAMP == 1) {
     for (int e = threadIdx.x; e < C * NP; e += NT) B[pad8(e)] = A[pad8(e)];
     cl_apply_D<NP, C, NT>(a, B, sfp, ths);
@@ -309,6 +338,81 @@ __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, dou
   }
   block_sum<NT, NACC>(acc, red);
   if (threadIdx.x < NACC) partials[(size_t)blockIdx.x * NACC + threadIdx.x] = red[0][threadIdx.x];
+}
+
+// ------------------------------------------------------------------ Gross-Pitaevskii terms
+// (MakeGrossPitaevskiiTerms :1717-1736 with ProbabilityX :1743-1748)
+// Column sums of W over a chunk of RCH rows: out[chunk][x] (grid NX/NT x NP/RCH).
+template <int NX, int NP, int RCH, int NT>
+__device__ __forceinline__ void colsum_body(const double2* __restrict__ W, double2* __restrict__ out) {
+  const int x = blockIdx.x * NT + threadIdx.x, r0 = blockIdx.y * RCH;
+  if (x >= NX) return;
+  double sr = 0., si = 0.;
+#pragma unroll 8
+  for (int r = 0; r < RCH; ++r) {
+    const double2 v = W[(size_t)(r0 + r) * NX + x];
+    sr += v.x;
+    si += v.y;
+  }
+  out[(size_t)blockIdx.y * NX + x] = make_double2(sr, si);
+}
+
+// P(x) = dP Re(s sum_p W) from the chunk sums (fixed order), s the pending
+// normalisation of scale_mode (1 / 2 as consume_partials, 0: none); one CTA.
+// psq (may be null) = sum_x P(x)^2 dX (ProbabilitySquare_average, :1951).
+template <int NX, int NT>
+__device__ __forceinline__ void gp_marginal_body(const WigArgs& a, const double2* __restrict__ chunks,
+                                                 int n_chunks, int scale_mode, double* __restrict__ P,
+                                                 double* __restrict__ psq) {
+  __shared__ double red[NT / 32][NACC];
+  const double2 s = consume_partials<NT>(a, scale_mode, nullptr, red);
+  double acc[NACC];
+#pragma unroll
+  for (int v = 0; v < NACC; ++v) acc[v] = 0.;
+  for (int x = threadIdx.x; x < NX; x += NT) {
+    double sr = 0., si = 0.;
+    for (int c = 0; c < n_chunks; ++c) {
+      const double2 v = chunks[(size_t)c * NX + x];
+      sr += v.x;
+      si += v.y;
+    }
+    const double px = a.dP * (s.x * sr - s.y * si);
+    P[x] = px;
+    acc[0] += px * px;
+  }
+  block_sum<NT, NACC>(acc, red);
+  if (psq != nullptr && threadIdx.x == 0) *psq = red[0][0] * a.dX;
+}
+
+// Gross-Pitaevskii phase of ROWS theta rows per CTA:
+//   phase(theta_i, x) = -0.5 dt a_GP Re[P(x - theta_i/2) - P(x + theta_i/2)] / hbar,
+// the shifted marginals by the shift theorem on the exact Lambda / Theta grids:
+// Re IFFT_x[FFT_x(P) (-2 i sin(lambda theta_i / 2))] / N_x.
+template <int NX, int NP, int ROWS, int NT>
+__device__ __forceinline__ void gp_phase_body(const WigArgs& a, const double* __restrict__ P,
+                                              double* __restrict__ phase_out) {
+  typedef RowMap<NX> M;
+  extern __shared__ double2 sm[];
+  double2* Ph = sm;                              // FFT of the marginal (one sequence)
+  double2* R = sm + padded_size(NX);             // ROWS rows
+  for (int x = threadIdx.x; x < NX; x += NT) Ph[M::idx(0, x)] = make_double2(P[x], 0.);
+  __syncthreads();
+  cta_fft<double2, NX, 1, NT, false, M>(Ph, a.tw_x);
+  const int row0 = blockIdx.x * ROWS;
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    const double th = a.theta_s[row0 + r] * (double)NP;    // exact shifted Theta
+    const double sn = sin(0.5 * a.lambda_tab[k] * th);
+    const double2 f = Ph[M::idx(0, k)];
+    R[M::idx(r, k)] = make_double2(2. * sn * f.y, -2. * sn * f.x);
+  }
+  __syncthreads();
+  cta_fft<double2, NX, ROWS, NT, true, M>(R, a.tw_x);
+  const double c = -0.5 * a.dt * a.gp_coef / a.hbar * (1.0 / (double)NX);
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    phase_out[(size_t)(row0 + r) * NX + k] = c * R[M::idx(r, k)].x;
+  }
 }
 
 // ------------------------------------------------------------------ ODM Lindblad

@@ -189,6 +189,7 @@ class GPU_Wigner2D_FFT(Propagator_Base):
 
     _odm2 = False
     _kvn = False
+    _strang_gp = False
 
     def __init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass, D_Theta, D_Lambda,
                  gammaDamping, potentialString, dPotentialString, kinematicString, normalization='Wigner'):
@@ -213,7 +214,7 @@ class GPU_Wigner2D_FFT(Propagator_Base):
         return _lib.DAMP_NONE
 
     def _build(self):
-        if getattr(self, 'grossPitaevskiiCoefficient', 0.) != 0.:
+        if not self._strang_gp and getattr(self, 'grossPitaevskiiCoefficient', 0.) != 0.:
             raise _lib.WignerUnsupportedError('the Gross-Pitaevskii term is not part of this propagator')
         if not hasattr(self, 'fp_Damping_String'):
             self.fp_Damping_String = 'fabs(p)'
@@ -235,12 +236,14 @@ class GPU_Wigner2D_FFT(Propagator_Base):
         d.abi_version = _lib.ABI_VERSION
         d.n_x, d.n_p = int(self.X_gridDIM), int(self.P_gridDIM)
         d.damping = self._damping_code()
-        d.kinetic_from_string = 1 if self._odm2 else 0
+        d.kinetic_from_string = 1 if (self._odm2 or self._strang_gp) else 0
         d.constants = self.constants_mode
         d.precision = _lib.PREC_C128
         d.n_lindblad = 2 if self._odm2 else 1
         d.potential_phase = _lib.PHASE_KVN if self._kvn else _lib.PHASE_MOYAL
         d.skip_normalise = 1 if (self._kvn and self.normalization != 'Wigner') else 0
+        d.splitting = _lib.SPLIT_STRANG_GP if self._strang_gp else _lib.SPLIT_LIE
+        d.gp_coefficient = float(getattr(self, 'GPitaevskiiCoeff', 0.)) if self._strang_gp else 0.
         d.x_amplitude, d.p_amplitude = float(self.X_amplitude), float(self.P_amplitude)
         d.hbar, d.mass, d.dt = float(self.hBar), float(self.mass), float(self.dt)
         d.d_theta, d.d_lambda, d.gamma = float(self.D_Theta), float(self.D_Lambda), float(self.gammaDamping)
@@ -392,3 +395,54 @@ class GPU_FokkerPlank2D_FFT(GPU_Wigner2D_FFT):
         GPU_Wigner2D_FFT.__init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass,
                                   D_Theta, D_Lambda, gammaDamping, potentialString, dPotentialString,
                                   getattr(self, 'kinematicString', '0.5*p*p'), normalization)
+
+
+class GPU_Wigner2D_GPitaevskii(GPU_Wigner2D_FFT):
+    """Wigner propagator with the Strang splitting and the Gross-Pitaevskii
+    term of ``GPU_Wigner2D_GPitaevskii.py:1767-2060``: per step, half potential
+    (with the mean-field phase from the x-marginal when ``GPitaevskiiCoeff``
+    != 0), kinetic (from ``kinematicString``), half potential, damping
+    (Caldeira-Leggett or ODM) and, if damped, normalisation.  An instance sets
+    ``GPitaevskiiCoeff`` (and ``dampingFunction``, ``fp_Damping_String``, ...)
+    before calling the constructor.  ``Run()`` records the observables after
+    every step (``timeSteps + 1`` steps) and, with the mean-field term,
+    ``ProbabilitySquare_average`` = sum_x P(x)^2 dx after each kinetic step."""
+
+    _strang_gp = True
+
+    def __init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass, D_Theta, D_Lambda,
+                 gammaDamping, potentialString, dPotentialString, kinematicString, normalization='Wigner'):
+        if not hasattr(self, 'GPitaevskiiCoeff'):
+            self.GPitaevskiiCoeff = 0.
+        GPU_Wigner2D_FFT.__init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass,
+                                  D_Theta, D_Lambda, gammaDamping, potentialString, dPotentialString,
+                                  kinematicString, normalization)
+
+    def probability_square(self, n):
+        """sum_x P(x)^2 dx after each of the last ``propagate`` call's first n steps."""
+        out = np.empty(n)
+        check(_lib.load().wig_run_probability_square(self._handle, dptr(out), n), 'wig_run_probability_square')
+        return out
+
+    def Run(self):
+        torch = _torch()
+        W0 = np.ascontiguousarray(self.W_init, dtype=np.complex128)
+        if W0.shape != (self.P_gridDIM, self.X_gridDIM):
+            raise _lib.WignerArgumentError('W_init must have shape (P_gridDIM, X_gridDIM)')
+        n = int(self.timeSteps) + 1                        # Run :1897 loops over 0..timeSteps
+        dev = torch.device('cuda', self._device)
+        with torch.cuda.device(dev):
+            W = torch.from_numpy(W0.copy()).to(dev)
+            obs = self.propagate(W, n)                     # row k: before step k; row k + 1: after it
+            psq = self.probability_square(n) if self.GPitaevskiiCoeff != 0. else np.zeros(0)
+            W_end = W.cpu().numpy()
+        after = obs[1:n + 1]
+        self.timeRange = np.arange(n) * self.dt
+        self.Norm_average = after[:, 0].copy()
+        (self.X_average, self.X2_average, self.P_average, self.P2_average, self.XP_average,
+         self.dPotentialdX_average, self.PdPotentialdX_average, self.XdPotentialdX_average,
+         self.Hamiltonian_average, self.negativeArea) = [after[:, k].copy() for k in range(1, 11)]
+        self.ProbabilitySquare_average = psq
+        self.W_end_complex = W_end
+        self.W_end = W_end.real.copy()
+        return 0

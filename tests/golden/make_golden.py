@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory from the reference's own code.
 
 Runs ``GPU_Wigner2D_FFT`` / ``GPU_Wigner2D_ODM2`` / ``GPU_FokkerPlank2D_FFT`` /
-``GPU_Dirac2D`` from the
+``GPU_Wigner2D_GPitaevskii`` / ``GPU_Dirac2D`` from the
 reference checkout through ``oracle.ref_harness`` (the reference's Python-2
 host code and its CUDA-C kernel strings, compiled for the CPU; ``numpy.fft``
 standing in for cuFFT) and stores, per case:
@@ -84,6 +84,23 @@ WIGNER_CASES = {
                                     normalization='none', time_steps=60, init=('ho', 0, 1., 2., 0.)),
 }
 
+# GPU_Wigner2D_GPitaevskii (Strang splitting, Gross-Pitaevskii term)
+GP_CASES = {
+    'gp_cl': dict(n_x=512, n_p=128, x_amplitude=10., p_amplitude=10., dt=0.01, potential='0.5*pow(x,2)',
+                  dpotential='x', kinetic='0.5*p*p', gamma=0.05, d_theta=0.05, damping='CaldeiraLeggett',
+                  fp_damping=' p*p/sqrt( p*p + 0.5 ) ', gp_coefficient=0.5, time_steps=80,
+                  init=('ho', 0, 1., 1., 0.)),
+    'gp_odm': dict(n_x=512, n_p=128, x_amplitude=10., p_amplitude=10., dt=0.005,
+                   potential='0.05*pow(x,4) - pow(x,2)', dpotential='0.2*pow(x,3) - 2.*x', kinetic='0.5*p*p',
+                   gamma=0.02, damping='ODM', fp_damping=' p*p/sqrt( p*p + 0.5 ) ', epsilon=0.5, L_material=3.,
+                   gp_coefficient=-0.3, time_steps=40, init=('ho', 0, 1., -2., 0.5)),
+    'gp_strang_plain': dict(n_x=512, n_p=128, x_amplitude=10., p_amplitude=10., dt=0.01,
+                            potential='0.05*pow(x,4) - pow(x,2) + 0.2*sin(2.*t)*x',
+                            dpotential='0.2*pow(x,3) - 2.*x + 0.2*sin(2.*t)', kinetic='0.5*p*p',
+                            d_lambda=0.001, gamma=0., gp_coefficient=0., time_steps=100,
+                            init=('cat', 2.5, 0.7)),
+}
+
 DIRAC_CASES = {
     # softened Coulomb, c = 137.036 (the physics of the 512^2 case, smaller grid)
     'dirac_coulomb': dict(n_x=128, n_y=128, x_amplitude=12., y_amplitude=12., dt=1e-4,
@@ -145,6 +162,37 @@ def run_wigner_case(name, c):
                 init_sum=np.array([W0.sum(), (W0 * W0).sum()]))
 
 
+def run_gp_case(name, c):
+    m = h.load_reference_module('GPU_Wigner2D_GPitaevskii')
+    prm_keys = {k: v for k, v in c.items() if k not in ('time_steps', 'init', 'gp_coefficient')}
+    prm = WignerParams(**prm_keys)
+
+    class Instance(m.GPU_Wigner2D_GPitaevskii):
+        def __init__(self):
+            self.dampingFunction = prm.damping
+            self.GPitaevskiiCoeff = c['gp_coefficient']
+            self.fp_Damping_String = prm.fp_damping
+            self.epsilon = prm.epsilon
+            self.L_material = prm.L_material
+            self.SetTimeTrack(prm.dt, c['time_steps'], 10 ** 9, fileName='/tmp/_golden_%s.hdf5' % name)
+            m.GPU_Wigner2D_GPitaevskii.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude,
+                                                prm.hbar, prm.mass, prm.d_theta, prm.d_lambda, prm.gamma,
+                                                prm.potential, prm.dpotential, prm.kinetic)
+    W0 = wigner_initial(prm, c['init'])
+    with h.quiet():
+        inst = Instance()
+        inst.W_init = W0.copy()
+        inst.Run()
+    obs = np.stack([inst.X_average, inst.X2_average, inst.P_average, inst.P2_average,
+                    inst.XP_average, inst.dPotentialdX_average, inst.PdPotentialdX_average,
+                    inst.XdPotentialdX_average, inst.Hamiltonian_average, inst.negativeArea], 1)
+    W = np.asarray(inst.W_end.real)
+    psq = np.asarray(inst.ProbabilitySquare_average, dtype=np.float64)
+    return dict(params=json.dumps(c), obs=obs, psq=psq, end_dec=W[::2, ::2].copy(),
+                end_sums=np.array([W.sum(), (W * W).sum()]),
+                init_sum=np.array([W0.sum(), (W0 * W0).sum()]))
+
+
 def run_dirac_case(name, c):
     d = h.load_reference_module('GPU_Dirac2D')
     prm_keys = {k: v for k, v in c.items() if k not in ('time_steps', 'p_init')}
@@ -173,11 +221,17 @@ def run_dirac_case(name, c):
 
 def main(names):
     cases = dict(WIGNER_CASES)
+    cases.update(GP_CASES)
     cases.update(DIRAC_CASES)
     for name in names or list(cases):
         t0 = time.time()
         c = cases[name]
-        out = run_dirac_case(name, c) if name in DIRAC_CASES else run_wigner_case(name, c)
+        if name in DIRAC_CASES:
+            out = run_dirac_case(name, c)
+        elif name in GP_CASES:
+            out = run_gp_case(name, c)
+        else:
+            out = run_wigner_case(name, c)
         path = os.path.join(HERE, name + '.npz')
         np.savez_compressed(path, **out)
         print('%-22s %6.1fs  %7.1f KB' % (name, time.time() - t0, os.path.getsize(path) / 1e3))

@@ -47,3 +47,20 @@ def obs_close(got, ref, rtol):
     a Gaussian state, ~1e-14 -- is compared at an absolute 1e-3 * rtol)."""
     scale = np.maximum(np.abs(ref).max(0), 1e-3)
     return float((np.abs(got - ref).max(0) / scale).max())
+
+
+GP_NAMES = ['gp_cl', 'gp_odm', 'gp_strang_plain']
+
+
+def gp_case(name):
+    """(fixture, WignerParams, gp_coefficient, W0, iterations) of a
+    GPU_Wigner2D_GPitaevskii case; Run() makes timeSteps + 1 iterations."""
+    g = load(name)
+    c = dict(g['params'])
+    steps, init, a_gp = c.pop('time_steps'), c.pop('init'), c.pop('gp_coefficient')
+    prm = WignerParams(**c)
+    if init[0] == 'ho':
+        W0 = np.ascontiguousarray(wigner_harmonic_oscillator(prm, *init[1:]))
+    else:
+        W0 = wigner_cat_state(prm, *init[1:])
+    return g, prm, a_gp, W0, steps + 1

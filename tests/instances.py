@@ -64,3 +64,23 @@ def dirac_instance(prm: DiracParams, psi0, time_steps, skip_frames=10 ** 9):
 def dirac_obs(inst):
     return np.stack([inst.X_average, inst.Y_average, inst.Alpha1_average, inst.Alpha2_average,
                      inst.Beta_average, inst.KEnergy_average, inst.Potential_0_average], 1)
+
+
+def gp_instance(prm: WignerParams, a_gp, W0, time_steps):
+    """A GPU_Wigner2D_GPitaevskii instance the way a notebook builds one."""
+    from pywignercuda_b200 import GPU_Wigner2D_GPitaevskii
+
+    class Instance(GPU_Wigner2D_GPitaevskii):
+        def __init__(self):
+            self.dampingFunction = prm.damping
+            self.GPitaevskiiCoeff = a_gp
+            self.fp_Damping_String = prm.fp_damping
+            self.epsilon = prm.epsilon
+            self.L_material = prm.L_material
+            self.SetTimeTrack(prm.dt, time_steps, 10 ** 9, fileName='')
+            GPU_Wigner2D_GPitaevskii.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude,
+                                              prm.hbar, prm.mass, prm.d_theta, prm.d_lambda, prm.gamma,
+                                              prm.potential, prm.dpotential, prm.kinetic)
+    inst = Instance()
+    inst.W_init = np.array(W0, copy=True)
+    return inst

@@ -108,6 +108,24 @@ def test_kvn_phase_compiles_and_is_validated():
     assert rc == 1, log
 
 
+def test_strang_gp_compiles_and_is_validated():
+    d = wig_desc(256, 128)
+    d.splitting = _lib.SPLIT_STRANG_GP
+    d.kinetic_from_string = 1
+    d.gp_coefficient = 0.5
+    rc, log = jit(d)
+    assert rc == 0, log
+    for k in ('wig_ppass_half', 'wig_ppass_half_final', 'wig_gp_colsum', 'wig_gp_marginal', 'wig_gp_phase'):
+        assert k in log, k
+    d.potential_phase = _lib.PHASE_KVN
+    rc, log = jit(d)
+    assert rc == 6 and 'Strang' in log, log
+    d = wig_desc(256, 128)
+    d.gp_coefficient = 0.5                           # GP term without the Strang splitting
+    rc, log = jit(d)
+    assert rc == 1 and 'gp_coefficient' in log, log
+
+
 def test_odm_kernels_compile():
     d = wig_desc(1024, 1024, damping=_lib.DAMP_ODM, fp=b' p*p/sqrt( p*p + 0.5 ) ')
     d.n_lindblad, d.l_material = 2, 3.

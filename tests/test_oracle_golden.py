@@ -13,7 +13,7 @@ from oracle.common import rel_l2
 from oracle.strang_notebook import StrangNotebook, KNOWN_MIN_W, KNOWN_NORM
 from oracle.wigner2d import WignerOracle
 from oracle.dirac2d import DiracOracle
-from golden_cases import WIGNER_NAMES, DIRAC_NAMES, wigner_case, dirac_case, obs_close
+from golden_cases import WIGNER_NAMES, DIRAC_NAMES, GP_NAMES, wigner_case, dirac_case, gp_case, obs_close
 
 TOL = 1e-10
 
@@ -44,3 +44,14 @@ def test_dirac_oracle_matches_reference(name):
     obs, P = DiracOracle(prm).run(psi0, steps)
     assert obs_close(obs[:, :7], g['obs'], TOL) < TOL
     assert rel_l2(P[:, ::2, ::2], g['end_dec']) < TOL
+
+
+@pytest.mark.parametrize('name', GP_NAMES)
+def test_gp_oracle_matches_reference(name):
+    from oracle.gpitaevskii import GPitaevskiiOracle
+    g, prm, a_gp, W0, n = gp_case(name)
+    obs, W, psq = GPitaevskiiOracle(prm, a_gp).run(W0, n)
+    assert obs_close(obs[:, 1:], g['obs'], 1e-12) < 1e-12
+    assert rel_l2(W.real[::2, ::2], g['end_dec']) < 1e-12
+    if a_gp != 0.:
+        assert np.max(np.abs(psq - g['psq']) / np.abs(g['psq'])) < 1e-12
