@@ -313,6 +313,31 @@ int wiga_jit_check(const wiga_desc* desc, char* log, int64_t log_cap);
  * n_prop values into out (host).  Synchronises the handle's last stream. */
 int wig_run_probability_square(wig_handle* h, double* out, int64_t n);
 
+/* ---- Imaginary-time (Bloch) steps of GPU_Wigner2D_GPitaevskii_Bloch
+ * (GPU_Wigner2D_GPitaevskii.py:2064-2545) on a WIG_SPLIT_STRANG_GP handle.
+ * stats[WIG_BLOCH_NSTATS]: <x>, <x^2>, <p>, <p^2>, <K(p) + V(0, x)> (K from the
+ * kinetic string, as the class's Hamiltonian), purity Re / Im
+ * (2 pi hbar dXdP sum W^2, Purity_GPU :1738-1741), the mean-field energy
+ * 0.5 a_GP sum_x P(x)^2 dx (NonLinearEnergy :1757-1758), 1 if some
+ * p-marginal value is negative (computed when W0 != NULL), the norm used. */
+#define WIG_BLOCH_NSTATS 10
+
+/* stats of W (complex128 (n_p, n_x), device); normalise != 0 first divides W by
+ * (sum W dX) dP as Run does with its initial state (:2129-2131).  Synchronous. */
+int wig_bloch_stats(wig_handle* h, void* W_dev, int32_t normalise, double* stats, void* stream);
+
+/* One imaginary-time step of size dtb at t = t_index dt, in place: [mean-field
+ * exponent] half potential (Kernel_Bloch, exp(-dtb/4 [V(x - hbar theta/2) +
+ * V(x + hbar theta/2)])) -> kinetic (exp(-dtb/2 [K(p + hbar lambda/2) +
+ * K(p - hbar lambda/2)])) -> [mean-field exponent] half potential; then, when
+ * W0 != NULL (Run_ExitedState1), W -= (2 pi hbar dXdP sum W W0) W0; then
+ * W /= sum W (dX dP); stats of the result.  The caller keeps the reference's
+ * accept / reject logic (energy must fall, |purity| < 1, and for the excited
+ * state no negative p-marginal; otherwise halve dtb and restore W).
+ * Synchronous. */
+int wig_bloch_step(wig_handle* h, void* W_dev, int64_t t_index, double dtb, const void* W0_dev, double* stats,
+                   void* stream);
+
 /* Compile-only check of an instance's kernels: builds the JIT source the way
  * wig_create / dirac_create do and compiles it with NVRTC for sm_100a without
  * loading it (no GPU needed).  log (may be NULL) receives the NVRTC log with

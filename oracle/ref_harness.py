@@ -196,6 +196,9 @@ class GPUArray:
     def get(self):
         return self.a.copy()
 
+    def copy(self):
+        return GPUArray(np.array(self.a, copy=True))
+
     def conj(self):
         return GPUArray(np.conj(self.a))
 

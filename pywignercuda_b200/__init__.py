@@ -7,9 +7,10 @@ from ._lib import (WignerError, WignerArgumentError, WignerCompileError, WignerC
                    WignerTimeoutError, WignerNonFiniteError, WignerUnsupportedError,
                    WignerMemoryError)
 from .wigner2d import (Propagator_Base, GPU_Wigner2D_FFT, GPU_Wigner2D_ODM2, GPU_FokkerPlank2D_FFT,  # noqa: F401
-                       GPU_Wigner2D_GPitaevskii)
+                       GPU_Wigner2D_GPitaevskii, GPU_Wigner2D_GPitaevskii_Bloch)
 from .dirac2d import GPU_Dirac2D  # noqa: F401
 
-__all__ = ['GPU_Wigner2D_FFT', 'GPU_Wigner2D_ODM2', 'GPU_FokkerPlank2D_FFT', 'GPU_Wigner2D_GPitaevskii', 'GPU_Dirac2D',
+__all__ = ['GPU_Wigner2D_FFT', 'GPU_Wigner2D_ODM2', 'GPU_FokkerPlank2D_FFT', 'GPU_Wigner2D_GPitaevskii',
+           'GPU_Wigner2D_GPitaevskii_Bloch', 'GPU_Dirac2D',
            'Propagator_Base',
            'WignerError']

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, 'libwigner_b200.so')
 
 ABI_VERSION = 3
 WIG_NOBS = 11
+WIG_BLOCH_NSTATS = 10
 DIRAC_NOBS = 10
 WIG_RUN_CONTINUE = 1
 WIG_RUN_PROFILE = 2
@@ -112,6 +113,8 @@ SIGNATURES = [
                              POINTER(_DP), c_void_p]),
     ('wig_profile', c_int, [c_void_p, _DP, POINTER(c_int64)]),
     ('wig_run_probability_square', c_int, [c_void_p, _DP, c_int64]),
+    ('wig_bloch_stats', c_int, [c_void_p, c_void_p, c_int32, _DP, c_void_p]),
+    ('wig_bloch_step', c_int, [c_void_p, c_void_p, c_int64, c_double, c_void_p, _DP, c_void_p]),
     ('wig_destroy', c_int, [c_void_p]),
     ('dirac_create', c_int, [POINTER(DiracDesc), POINTER(c_void_p)]),
     ('dirac_run', c_int, [c_void_p, c_void_p, c_int64, c_int64, _DP, c_void_p]),

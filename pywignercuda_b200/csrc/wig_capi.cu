@@ -303,6 +303,11 @@ struct wig_handle {
   // Strang / Gross-Pitaevskii (GPU_Wigner2D_GPitaevskii)
   int strang = 0, gp = 0, smem_ph = 0, smem_gph = 0, n_chunks = 0;
   CUfunction f_ph = nullptr, f_phf = nullptr, f_gcs = nullptr, f_gm = nullptr, f_gph = nullptr;
+  // Bloch (imaginary time)
+  CUfunction f_bph = nullptr, f_bx = nullptr, f_gb = nullptr, f_br = nullptr, f_rs = nullptr, f_ba = nullptr;
+  double* bloch_part = nullptr;                // [n_cta_r][wig::NBL]
+  double2* rowsums = nullptr;                  // [n_p]
+  double* bloch_psq = nullptr;                 // [1]
   double2* gp_chunks = nullptr;                // [n_p/16][n_x] column sums
   double* gp_P = nullptr;                      // [n_x] marginal
   double* gp_phase = nullptr;                  // [n_p][n_x]
@@ -482,6 +487,12 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   if (!rc && h->gp) rc = get_fn(mod, "wig_gp_colsum", &h->f_gcs, 0);
   if (!rc && h->gp) rc = get_fn(mod, "wig_gp_marginal", &h->f_gm, 0);
   if (!rc && h->gp) rc = get_fn(mod, "wig_gp_phase", &h->f_gph, h->smem_gph);
+  if (!rc && h->strang) rc = get_fn(mod, "wig_bloch_ppass", &h->f_bph, h->smem_ph);
+  if (!rc && h->strang) rc = get_fn(mod, "wig_bloch_xpass", &h->f_bx, h->smem_x);
+  if (!rc && h->strang) rc = get_fn(mod, "wig_bloch_reduce", &h->f_br, 0);
+  if (!rc && h->strang) rc = get_fn(mod, "wig_rowsum", &h->f_rs, 0);
+  if (!rc && h->strang) rc = get_fn(mod, "wig_bloch_axpy", &h->f_ba, 0);
+  if (!rc && h->gp) rc = get_fn(mod, "wig_gp_bloch", &h->f_gb, h->smem_gph);
   if (rc) { delete h; return rc; }
 
   // ---- kernel arguments and tables
@@ -539,6 +550,9 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   if (!rc && h->gp) rc = B.alloc(&h->gp_chunks, (size_t)h->n_chunks * NX);
   if (!rc && h->gp) rc = B.alloc(&h->gp_P, NX);
   if (!rc && h->gp) rc = B.alloc(&h->gp_phase, (size_t)NX * NP);
+  if (!rc && h->strang) rc = B.alloc(&h->bloch_part, (size_t)h->n_cta_r * wig::NBL);
+  if (!rc && h->strang) rc = B.alloc(&h->rowsums, (size_t)NP);
+  if (!rc && h->gp) rc = B.alloc(&h->bloch_psq, (size_t)1);
   if (rc) { B.free_all(); delete h; return rc; }
   a.r_theta_half = rth_d;
   a.gp_coef = kval(d->gp_coefficient, cm);
@@ -749,6 +763,168 @@ extern "C" int wig_run(wig_handle* h, void* W_dev, int64_t t_index0, int64_t n_p
     return check_finite(obs_host, (size_t)(n_prop + 1) * WIG_NOBS, "wig_run observables");
   }
   return WIG_OK;
+}
+
+// ------------------------------------------------------------------ Bloch (imaginary time)
+// GPU_Wigner2D_GPitaevskii_Bloch.Run / Run_ExitedState1 (:2105-2545): the device
+// work of one step; the host keeps the reference's accept / reject and
+// step-halving logic.
+static int bloch_check(wig_handle* h, void* W_dev, double* stats, const char* what) {
+  if (!h || !W_dev || !stats) return fail(WIG_ERR_ARG, "%s: null argument", what);
+  if (!h->strang) return fail(WIG_ERR_ARG, "%s: the handle needs splitting = WIG_SPLIT_STRANG_GP", what);
+  if (((uintptr_t)W_dev & 15) != 0) return fail(WIG_ERR_ARG, "%s: W must be 16-byte aligned", what);
+  int cur;
+  WIG_CUDA(cudaGetDevice(&cur));
+  if (cur != h->device) return fail(WIG_ERR_ARG, "%s: current device %d != handle device %d", what, cur, h->device);
+  return WIG_OK;
+}
+
+// sums[NBL] over the grid (CTA partials summed on the host in CTA order)
+static int bloch_sums(wig_handle* h, double2* W, const double2* W0, double* sums, cudaStream_t st) {
+  void* args[] = {&h->a, &W, &W0, &h->bloch_part};
+  if (int rc = launch(h->f_br, h->n_cta_r, h->rnt, 0, st, args)) return rc;
+  std::vector<double> part((size_t)h->n_cta_r * wig::NBL);
+  WIG_CUDA(cudaMemcpyAsync(part.data(), h->bloch_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  WIG_CUDA(cudaStreamSynchronize(st));
+  for (int v = 0; v < wig::NBL; ++v) sums[v] = 0.;
+  for (int c = 0; c < h->n_cta_r; ++c)
+    for (int v = 0; v < wig::NBL; ++v) sums[v] += part[(size_t)c * wig::NBL + v];
+  return WIG_OK;
+}
+
+static int bloch_axpy(wig_handle* h, double2* W, const double2* W0, double2 c, double2 s, cudaStream_t st) {
+  long n = (long)h->d.n_x * h->d.n_p;
+  void* args[] = {&W, &W0, &n, &c, &s};
+  return launch(h->f_ba, clampi((int)(n / (4 * h->rnt)), 1, 592), h->rnt, 0, st, args);
+}
+
+static double2 cdiv1(double2 z) {   // 1 / z (Smith)
+  double2 r;
+  if (fabs(z.x) >= fabs(z.y)) {
+    const double rat = z.y / z.x, scl = 1.0 / (z.x + z.y * rat);
+    r.x = scl; r.y = -rat * scl;
+  } else {
+    const double rat = z.x / z.y, scl = 1.0 / (z.y + z.x * rat);
+    r.x = rat * scl; r.y = -scl;
+  }
+  return r;
+}
+
+// stats of the (normalised) W: [0..4] <x>, <x^2>, <p>, <p^2>, <K(p) + V(0, x)>;
+// [5, 6] purity 2 pi hbar dXdP sum W^2; [7] mean-field energy 0.5 a_GP sum_x P^2 dx;
+// [8] 1 if a row sum (p-marginal) is negative (with_marginal), else 0; [9] the
+// norm dXdP sum W before normalisation (Re).
+static int bloch_stats_of(wig_handle* h, double2* W, bool with_marginal, double* stats, cudaStream_t st) {
+  double sums[wig::NBL];
+  if (int rc = bloch_sums(h, W, nullptr, sums, st)) return rc;
+  const double dXdP = h->a.dX * h->a.dP;
+  for (int k = 0; k < 5; ++k) stats[k] = dXdP * sums[2 + k];
+  const double pf = 2. * M_PI * h->d.hbar * dXdP;
+  stats[5] = pf * sums[7];
+  stats[6] = pf * sums[8];
+  stats[7] = 0.;
+  if (h->gp) {
+    const int NX = h->d.n_x, NP = h->d.n_p, cnt = NX < 256 ? NX : 256;
+    void* cargs[] = {&W, &h->gp_chunks};
+    if (int rc = launch2d(h->f_gcs, (unsigned)(NX / cnt), (unsigned)(NP / 16), (unsigned)cnt, 0, st, cargs)) return rc;
+    int nch = h->n_chunks, zero = 0;
+    double* psq_d = h->bloch_psq;
+    void* margs[] = {&h->a, &h->gp_chunks, &nch, &zero, &h->gp_P, &psq_d};
+    if (int rc = launch(h->f_gm, 1, 256, 0, st, margs)) return rc;
+    double psq_h = 0.;
+    WIG_CUDA(cudaMemcpyAsync(&psq_h, psq_d, sizeof(double), cudaMemcpyDeviceToHost, st));
+    WIG_CUDA(cudaStreamSynchronize(st));
+    stats[7] = 0.5 * h->d.gp_coefficient * psq_h;   // NonLinearEnergy (:1757-1758)
+  }
+  stats[8] = 0.;
+  if (with_marginal) {
+    void* rargs[] = {&W, &h->rowsums};
+    if (int rc = launch(h->f_rs, h->d.n_p, 256, 0, st, rargs)) return rc;
+    std::vector<double2> rows(h->d.n_p);
+    WIG_CUDA(cudaMemcpyAsync(rows.data(), h->rowsums, rows.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    WIG_CUDA(cudaStreamSynchronize(st));
+    for (const double2& r : rows)
+      if (r.x * h->a.dX < 0.) { stats[8] = 1.; break; }
+  }
+  return WIG_OK;
+}
+
+// divide W by norm = sum W * c0 (c0 = dX dP applied as (S dX) dP when initial, S (dX dP) per step)
+static int bloch_normalise(wig_handle* h, double2* W, bool initial, double* norm_re, cudaStream_t st) {
+  double sums[wig::NBL];
+  if (int rc = bloch_sums(h, W, nullptr, sums, st)) return rc;
+  double2 S = make_double2(sums[0], sums[1]), nrm;
+  if (initial) nrm = make_double2(S.x * h->a.dX * h->a.dP, S.y * h->a.dX * h->a.dP);
+  else { const double d = h->a.dX * h->a.dP; nrm = make_double2(S.x * d, S.y * d); }
+  *norm_re = nrm.x;
+  return bloch_axpy(h, W, nullptr, make_double2(0., 0.), cdiv1(nrm), st);
+}
+
+extern "C" int wig_bloch_stats(wig_handle* h, void* W_dev, int32_t normalise, double* stats, void* stream) {
+  if (int rc = bloch_check(h, W_dev, stats, "wig_bloch_stats")) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* W = (double2*)W_dev;
+  double nre = 0.;
+  if (normalise)
+    if (int rc = bloch_normalise(h, W, true, &nre, st)) return rc;
+  if (int rc = bloch_stats_of(h, W, false, stats, st)) return rc;
+  stats[9] = nre;
+  return check_finite(stats, WIG_BLOCH_NSTATS, "wig_bloch_stats");
+}
+
+extern "C" int wig_bloch_step(wig_handle* h, void* W_dev, int64_t t_index, double dtb, const void* W0_dev,
+                              double* stats, void* stream) {
+  if (int rc = bloch_check(h, W_dev, stats, "wig_bloch_step")) return rc;
+  if (!(dtb > 0.) || !std::isfinite(dtb)) return fail(WIG_ERR_ARG, "wig_bloch_step: dtb must be > 0");
+  if (W0_dev && ((uintptr_t)W0_dev & 15) != 0) return fail(WIG_ERR_ARG, "wig_bloch_step: W0 must be 16-byte aligned");
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* W = (double2*)W_dev;
+  const double2* W0 = (const double2*)W0_dev;
+  const double t = (double)t_index * h->d.dt;
+  const int NX = h->d.n_x, NP = h->d.n_p, cnt = NX < 256 ? NX : 256;
+  auto gexp = [&](double** out) -> int {   // mean-field exponent of the current W
+    *out = nullptr;
+    if (!h->gp) return WIG_OK;
+    void* cargs[] = {&W, &h->gp_chunks};
+    if (int rc = launch2d(h->f_gcs, (unsigned)(NX / cnt), (unsigned)(NP / 16), (unsigned)cnt, 0, st, cargs)) return rc;
+    int nch = h->n_chunks, zero = 0;
+    double* nopsq = nullptr;
+    void* margs[] = {&h->a, &h->gp_chunks, &nch, &zero, &h->gp_P, &nopsq};
+    if (int rc = launch(h->f_gm, 1, 256, 0, st, margs)) return rc;
+    double dt_ = dtb;
+    void* gargs[] = {&h->a, &h->gp_P, &dt_, &h->gp_phase};
+    if (int rc = launch(h->f_gb, h->n_cta_x, h->xnt, h->smem_gph, st, gargs)) return rc;
+    *out = h->gp_phase;
+    return WIG_OK;
+  };
+  double* ge = nullptr;
+  double tt = t, dd = dtb;
+  if (int rc = gexp(&ge)) return rc;
+  {
+    void* args[] = {&h->a, &W, &tt, &dd, &ge};
+    if (int rc = launch(h->f_bph, h->n_cta_p, h->pnt, h->smem_ph, st, args)) return rc;
+  }
+  {
+    void* args[] = {&h->a, &W, &dd};
+    if (int rc = launch(h->f_bx, h->n_cta_x, h->xnt, h->smem_x, st, args)) return rc;
+  }
+  if (int rc = gexp(&ge)) return rc;
+  {
+    void* args[] = {&h->a, &W, &tt, &dd, &ge};
+    if (int rc = launch(h->f_bph, h->n_cta_p, h->pnt, h->smem_ph, st, args)) return rc;
+  }
+  if (W0) {
+    // Run_ExitedState1 (:2429-2434): W -= c W0, c = 2 pi hbar dXdP sum W W0
+    double sums[wig::NBL];
+    if (int rc = bloch_sums(h, W, W0, sums, st)) return rc;
+    const double pf = 2. * M_PI * h->d.hbar * h->a.dX * h->a.dP;
+    if (int rc = bloch_axpy(h, W, W0, make_double2(pf * sums[9], pf * sums[10]), make_double2(1., 0.), st)) return rc;
+  }
+  double nre = 0.;
+  if (int rc = bloch_normalise(h, W, false, &nre, st)) return rc;
+  if (int rc = bloch_stats_of(h, W, W0 != nullptr, stats, st)) return rc;
+  stats[9] = nre;
+  return check_finite(stats, WIG_BLOCH_NSTATS, "wig_bloch_step");
 }
 
 extern "C" int wig_run_probability_square(wig_handle* h, double* out, int64_t n) {

@@ -74,6 +74,37 @@ extern "C" __global__ void __launch_bounds__(WIG_XNT)
 wig_gp_phase(wig::WigArgs a, const double* P, double* phase_out) {
   wig::gp_phase_body<WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT>(a, P, phase_out);
 }
+
+// Bloch (imaginary-time) step pieces, GPU_Wigner2D_GPitaevskii_Bloch (:2064-2545)
+extern "C" __global__ void __launch_bounds__(WIG_PNT, WIG_PMINB)
+wig_bloch_ppass(wig::WigArgs a, double2* W, double t, double dtb, const double* gexp) {
+  wig::bloch_ppass_body<UserPhys, WIG_NX, WIG_NP, WIG_PC, WIG_PNT>(a, user_phys(a), W, t, dtb, gexp);
+}
+
+extern "C" __global__ void __launch_bounds__(WIG_XNT, WIG_XMINB)
+wig_bloch_xpass(wig::WigArgs a, double2* W, double dtb) {
+  wig::bloch_xpass_body<UserPhys, WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT>(a, user_phys(a), W, dtb);
+}
+
+extern "C" __global__ void __launch_bounds__(WIG_XNT)
+wig_gp_bloch(wig::WigArgs a, const double* P, double dtb, double* out) {
+  wig::gp_bloch_body<WIG_NX, WIG_NP, WIG_XROWS, WIG_XNT>(a, P, dtb, out);
+}
+
+extern "C" __global__ void __launch_bounds__(WIG_RNT)
+wig_bloch_reduce(wig::WigArgs a, const double2* W, const double2* W0, double* partials) {
+  wig::bloch_reduce_body<UserPhys, WIG_NX, WIG_NP, WIG_RNT>(a, user_phys(a), W, W0, partials);
+}
+
+extern "C" __global__ void __launch_bounds__(256)
+wig_rowsum(const double2* W, double2* out) {
+  wig::rowsum_body<WIG_NX, 256>(W, out);
+}
+
+extern "C" __global__ void __launch_bounds__(WIG_RNT)
+wig_bloch_axpy(double2* W, const double2* W0, long n, double2 c, double2 s) {
+  wig::bloch_axpy_body<WIG_RNT>(W, W0, n, c, s);
+}
 #endif
 
 extern "C" __global__ void __launch_bounds__(WIG_RNT)

@@ -415,6 +415,159 @@ __device__ __forceinline__ void gp_phase_body(const WigArgs& a, const double* __
   }
 }
 
+// ------------------------------------------------------------------ Bloch (imaginary time)
+// GPU_Wigner2D_GPitaevskii_Bloch (:2064-2342): the Strang step with real
+// exponentials and a run-time step dtb (Kernel_Bloch of expPotential_source
+// :90-114 and expPLambdaKinetic_source :155-178).
+// p-half: W(theta, x) *= exp(-0.25 dtb [V(x - hbar theta/2) + V(x + hbar theta/2)])
+//         * exp(gexp(theta, x)) (mean-field, may be null); no masks, no diffusion.
+template <class Phys, int NX, int NP, int C, int NT>
+__device__ __forceinline__ void bloch_ppass_body(const WigArgs& a, const Phys& ph, double2* __restrict__ W,
+                                                 double t, double dtb, const double* __restrict__ gexp) {
+  typedef ColMap<C> M;
+  extern __shared__ double2 sm[];
+  double2* A = sm;
+  const int col0 = blockIdx.x * C;
+  for (int e = threadIdx.x; e < C * NP; e += NT) {
+    const int k = e / C, c = e - k * C;
+    A[pad8(e)] = W[(size_t)k * NX + col0 + c];
+  }
+  __syncthreads();
+  cta_fft<double2, NP, C, NT, false, M>(A, a.tw_p);
+  const double inv_n = 1.0 / (double)NP;
+  for (int e = threadIdx.x; e < C * NP; e += NT) {
+    const int k = e / C, c = e - k * C;
+    const int col = col0 + c;
+    const int ii = (k + NP / 2) % NP, jj = (col + NX / 2) % NX;
+    const double x = a.dx * (jj - 0.5 * NX);
+    const double theta = a.dtheta * (ii - 0.5 * NP);
+    double f = exp(-0.25 * dtb * (ph.Potential(t, x - a.hbar * theta / 2.) + ph.Potential(t, x + a.hbar * theta / 2.)));
+    if (gexp != nullptr) f *= exp(gexp[(size_t)k * NX + col]);
+    A[pad8(e)] = cscale(A[pad8(e)], f * inv_n);
+  }
+  __syncthreads();
+  cta_fft<double2, NP, C, NT, true, M>(A, a.tw_p);
+  for (int e = threadIdx.x; e < C * NP; e += NT) {
+    const int k = e / C, c = e - k * C;
+    W[(size_t)k * NX + col0 + c] = A[pad8(e)];
+  }
+}
+
+// x-pass: W(p, lambda) *= exp(-0.5 dtb [K(p + hbar lambda/2) + K(p - hbar lambda/2)]).
+template <class Phys, int NX, int NP, int ROWS, int NT>
+__device__ __forceinline__ void bloch_xpass_body(const WigArgs& a, const Phys& ph, double2* __restrict__ W,
+                                                 double dtb) {
+  typedef RowMap<NX> M;
+  extern __shared__ double2 sm[];
+  const int row0 = blockIdx.x * ROWS;
+  double2* Wb = W + (size_t)row0 * NX;
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    sm[M::idx(r, k)] = Wb[e];
+  }
+  __syncthreads();
+  cta_fft<double2, NX, ROWS, NT, false, M>(sm, a.tw_x);
+  const double inv_n = 1.0 / (double)NX;
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    const int ii = (row0 + r + NP / 2) % NP, jj = (k + NX / 2) % NX;
+    const double lambda = a.dlambda * (jj - 0.5 * NX);
+    const double p = a.dp * (ii - 0.5 * NP);
+    const double f = exp(-0.5 * dtb * (ph.KineticEnergy(p + a.hbar * lambda / 2.) +
+                                      ph.KineticEnergy(p - a.hbar * lambda / 2.)));
+    const int id = M::idx(r, k);
+    sm[id] = cscale(sm[id], f * inv_n);
+  }
+  __syncthreads();
+  cta_fft<double2, NX, ROWS, NT, true, M>(sm, a.tw_x);
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    Wb[e] = sm[M::idx(r, k)];
+  }
+}
+
+// Mean-field exponent of Kernel_Bloch (expPotential_GrossPitaevskii_source
+// :497-517): -0.25 dtb a_GP [P(x - theta/2) + P(x + theta/2)], the shifted
+// marginals summed by the shift theorem: Re IFFT_x[FFT_x(P) 2 cos(lambda theta/2)] / N_x.
+template <int NX, int NP, int ROWS, int NT>
+__device__ __forceinline__ void gp_bloch_body(const WigArgs& a, const double* __restrict__ P, double dtb,
+                                              double* __restrict__ out) {
+  typedef RowMap<NX> M;
+  extern __shared__ double2 sm[];
+  double2* Ph = sm;
+  double2* R = sm + padded_size(NX);
+  for (int x = threadIdx.x; x < NX; x += NT) Ph[M::idx(0, x)] = make_double2(P[x], 0.);
+  __syncthreads();
+  cta_fft<double2, NX, 1, NT, false, M>(Ph, a.tw_x);
+  const int row0 = blockIdx.x * ROWS;
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    const double th = a.theta_s[row0 + r] * (double)NP;
+    const double cs = 2. * cos(0.5 * a.lambda_tab[k] * th);
+    const double2 f = Ph[M::idx(0, k)];
+    R[M::idx(r, k)] = make_double2(cs * f.x, cs * f.y);
+  }
+  __syncthreads();
+  cta_fft<double2, NX, ROWS, NT, true, M>(R, a.tw_x);
+  const double c = -0.25 * dtb * a.gp_coef * (1.0 / (double)NX);
+  for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
+    const int r = e / NX, k = e - r * NX;
+    out[(size_t)(row0 + r) * NX + k] = c * R[M::idx(r, k)].x;
+  }
+}
+
+// Observables of a Bloch step (one CTA per block of the grid, partials per CTA):
+// sums of W, W x, W x^2, W p, W p^2, W [K(p) + V(0, x)] (the Bloch Hamiltonian,
+// :2097 -- the kinetic string, not p^2/2m), W^2 (purity, Purity_GPU :1738-1741),
+// W W0 (ExitedState1 projection, :2431) and the p-marginal rows are separate.
+constexpr int NBL = 12;   // Re/Im sum, x, x2, p, p2, H, Re/Im W^2, Re/Im W W0, spare
+template <class Phys, int NX, int NP, int NT>
+__device__ __forceinline__ void bloch_reduce_body(const WigArgs& a, const Phys& ph, const double2* __restrict__ W,
+                                                  const double2* __restrict__ W0, double* __restrict__ partials) {
+  __shared__ double red[NT / 32][NBL];
+  double acc[NBL];
+#pragma unroll
+  for (int v = 0; v < NBL; ++v) acc[v] = 0.;
+  for (int e = blockIdx.x * NT + threadIdx.x; e < NX * NP; e += gridDim.x * NT) {
+    const int i = e / NX, j = e - i * NX;
+    const double2 v = W[e];
+    const double x = a.x_tab[j], p = a.p_tab[i];
+    acc[0] += v.x; acc[1] += v.y;
+    acc[2] += v.x * x; acc[3] += v.x * (x * x);
+    acc[4] += v.x * p; acc[5] += v.x * (p * p);
+    acc[6] += v.x * (ph.KineticEnergy(p) + a.V0_tab[j]);
+    acc[7] += v.x * v.x - v.y * v.y; acc[8] += 2. * v.x * v.y;
+    if (W0 != nullptr) {
+      const double2 u = W0[e];
+      acc[9] += v.x * u.x - v.y * u.y; acc[10] += v.x * u.y + v.y * u.x;
+    }
+  }
+  block_sum<NT, NBL>(acc, red);
+  if (threadIdx.x < NBL) partials[(size_t)blockIdx.x * NBL + threadIdx.x] = red[0][threadIdx.x];
+}
+
+// Row sums of W (the p-marginal): out[i] = sum_x W[i][x] (ProbabilityP :1750-1755).
+template <int NX, int NT>
+__device__ __forceinline__ void rowsum_body(const double2* __restrict__ W, double2* __restrict__ out) {
+  __shared__ double red[NT / 32][2];
+  double acc[2] = {0., 0.};
+  const double2* r = W + (size_t)blockIdx.x * NX;
+  for (int j = threadIdx.x; j < NX; j += NT) { acc[0] += r[j].x; acc[1] += r[j].y; }
+  block_sum<NT, 2>(acc, red);
+  if (threadIdx.x == 0) out[blockIdx.x] = make_double2(red[0][0], red[0][1]);
+}
+
+// W <- s (W - c W0)  (projection and normalisation of a Bloch step)
+template <int NT>
+__device__ __forceinline__ void bloch_axpy_body(double2* __restrict__ W, const double2* __restrict__ W0,
+                                                long n, double2 c, double2 s) {
+  for (long e = (long)blockIdx.x * NT + threadIdx.x; e < n; e += (long)gridDim.x * NT) {
+    double2 v = W[e];
+    if (W0 != nullptr) v = csub(v, cmul(c, W0[e]));
+    W[e] = cmul(v, s);
+  }
+}
+
 // ------------------------------------------------------------------ ODM Lindblad
 // g_ODM(p) = sqrt(L f(|p| + hbar/(2L)))  (g_ODM :1196-1197); the five
 // momentum-space factor combinations of _Lindbladian_ODM (:1524-1623), with

@@ -446,3 +446,95 @@ class GPU_Wigner2D_GPitaevskii(GPU_Wigner2D_FFT):
         self.W_end_complex = W_end
         self.W_end = W_end.real.copy()
         return 0
+
+
+class GPU_Wigner2D_GPitaevskii_Bloch(GPU_Wigner2D_GPitaevskii):
+    """Imaginary-time (Bloch) propagator of ``GPU_Wigner2D_GPitaevskii.py:2064-2545``
+    for ground states (``Run``) and the first excited state (``Run_ExitedState1``):
+    Strang steps with real exponentials and the mean-field term (set
+    ``GPitaevskiiCoeff`` before the constructor), normalisation every step, and
+    the reference's step control -- a step counts only if the total energy
+    (Hamiltonian K(P) + V(0, X) plus the mean-field energy) falls and
+    |purity| < 1 (and, for the excited state, no p-marginal value is negative);
+    otherwise the step size is halved and the last counted state restored.
+    Deviations: ``GPitaevskiiCoeff = 0`` works (the reference's ``Run`` reads its
+    marginal buffer before creating it, :2145-2176); the excited-state check
+    uses the p-marginal itself (the reference's ``ProbabilityP`` indexes rows
+    with the row stride and writes past its output, :432-441, :1750-1755)."""
+
+    def __init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass, potentialString,
+                 kinematicString):
+        self.dampingFunction = 'CaldeiraLeggett'
+        self.fp_Damping_String = '0.'
+        GPU_Wigner2D_GPitaevskii.__init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass,
+                                          0., 0., 0., potentialString, '0.', kinematicString)
+
+    def _stats(self, W, normalise):
+        out = np.empty(_lib.WIG_BLOCH_NSTATS)
+        st = _torch().cuda.current_stream(W.device)
+        check(_lib.load().wig_bloch_stats(self._handle, W.data_ptr(), int(normalise), dptr(out), st.cuda_stream),
+              'wig_bloch_stats')
+        return out
+
+    def _step(self, W, t_index, dtb, W0=None):
+        out = np.empty(_lib.WIG_BLOCH_NSTATS)
+        st = _torch().cuda.current_stream(W.device)
+        check(_lib.load().wig_bloch_step(self._handle, W.data_ptr(), int(t_index), float(dtb),
+                                         W0.data_ptr() if W0 is not None else None, dptr(out), st.cuda_stream),
+              'wig_bloch_step')
+        return out
+
+    def _relax(self, W0_ground, time_steps):
+        torch = _torch()
+        init = np.ascontiguousarray(self.W_init, dtype=np.complex128)
+        if init.shape != (self.P_gridDIM, self.X_gridDIM):
+            raise _lib.WignerArgumentError('W_init must have shape (P_gridDIM, X_gridDIM)')
+        dev = torch.device('cuda', self._device)
+        with torch.cuda.device(dev):
+            W = torch.from_numpy(init.copy()).to(dev)
+            W_step = torch.from_numpy(init.copy()).to(dev)      # the reference keeps W_init here (:2135)
+            s0 = self._stats(W, True)
+            energy = s0[4] + s0[7]
+            dtb = float(self.dt)
+            avg, hist_e, hist_nle, hist_pur = [], [], [], []
+            for t_index in range(time_steps + 1):
+                s = self._step(W, t_index, dtb, W0_ground)
+                avg.append(s[:5].copy())
+                e_step = s[4] + s[7]
+                purity = complex(s[5], s[6])
+                if t_index > 0:
+                    if e_step < energy and abs(purity) < 1. and s[8] == 0.:
+                        W_step.copy_(W)
+                        hist_pur.append(purity.real)
+                        hist_e.append(e_step)
+                        energy = e_step
+                        hist_nle.append(s[7])
+                    else:
+                        dtb = dtb / 2.
+                        W.copy_(W_step)
+            torch.cuda.synchronize(dev)
+            W_end = W.cpu().numpy()
+        avg = np.array(avg)
+        self.timeRange = np.arange(time_steps + 1) * self.dt
+        (self.X_average, self.X2_average, self.P_average, self.P2_average,
+         self.Hamiltonian_average) = [avg[:, k].copy() for k in range(5)]
+        self.TotalEnergyHistory = np.array(hist_e)
+        if self.GPitaevskiiCoeff != 0.:
+            self.NonLinearEnergyHistory = np.array(hist_nle)
+        self.purity = np.array(hist_pur)
+        return W_end
+
+    def Run(self):
+        W_end = self._relax(None, int(self.timeSteps))
+        self.W_0_complex = W_end
+        self.W_0 = W_end.real.copy()
+        return 0
+
+    def Run_ExitedState1(self, timeSteps=None):
+        if not hasattr(self, 'W_0_complex'):
+            raise _lib.WignerArgumentError('Run() must find the ground state W_0 first')
+        torch = _torch()
+        W0 = torch.from_numpy(np.ascontiguousarray(self.W_0_complex)).to(torch.device('cuda', self._device))
+        W_end = self._relax(W0, int(self.timeSteps if timeSteps is None else timeSteps))
+        self.W_1 = W_end.real.copy()
+        return 0

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory from the reference's own code.
 
 Runs ``GPU_Wigner2D_FFT`` / ``GPU_Wigner2D_ODM2`` / ``GPU_FokkerPlank2D_FFT`` /
-``GPU_Wigner2D_GPitaevskii`` / ``GPU_Dirac2D`` from the
+``GPU_Wigner2D_GPitaevskii`` / ``GPU_Wigner2D_GPitaevskii_Bloch`` / ``GPU_Dirac2D`` from the
 reference checkout through ``oracle.ref_harness`` (the reference's Python-2
 host code and its CUDA-C kernel strings, compiled for the CPU; ``numpy.fft``
 standing in for cuFFT) and stores, per case:
@@ -101,6 +101,20 @@ GP_CASES = {
                             init=('cat', 2.5, 0.7)),
 }
 
+# GPU_Wigner2D_GPitaevskii_Bloch (imaginary time, adaptive step)
+BLOCH_CASES = {
+    'bloch_gp': dict(n_x=512, n_p=128, x_amplitude=10., p_amplitude=10., dt=0.02, potential='0.5*pow(x,2)',
+                     dpotential='x', kinetic='0.5*p*p', gp_coefficient=1.0, time_steps=60,
+                     init=('ho', 0, 1., 1., 0.5)),
+    # a second case: double well with a large step -- 9 of 40 steps are rejected and dt halved
+    'bloch_gp_doublewell': dict(n_x=512, n_p=128, x_amplitude=10., p_amplitude=10., dt=1.0,
+                                potential='0.05*pow(x,4) - pow(x,2)', dpotential='0.2*pow(x,3) - 2.*x',
+                                kinetic='0.5*p*p', gp_coefficient=0.3, time_steps=40,
+                                init=('ho', 0, 1., -2.5, 0.3)),
+}
+# (The reference's Bloch Run needs GPitaevskiiCoeff != 0: with 0 it reads its
+# marginal buffer before creating it, GPU_Wigner2D_GPitaevskii.py:2145-2176.)
+
 DIRAC_CASES = {
     # softened Coulomb, c = 137.036 (the physics of the 512^2 case, smaller grid)
     'dirac_coulomb': dict(n_x=128, n_y=128, x_amplitude=12., y_amplitude=12., dt=1e-4,
@@ -193,6 +207,32 @@ def run_gp_case(name, c):
                 init_sum=np.array([W0.sum(), (W0 * W0).sum()]))
 
 
+def run_bloch_case(name, c):
+    m = h.load_reference_module('GPU_Wigner2D_GPitaevskii')
+    prm_keys = {k: v for k, v in c.items() if k not in ('time_steps', 'init', 'gp_coefficient')}
+    prm = WignerParams(**prm_keys)
+
+    class Instance(m.GPU_Wigner2D_GPitaevskii_Bloch):
+        def __init__(self):
+            self.GPitaevskiiCoeff = c['gp_coefficient']
+            self.SetTimeTrack(prm.dt, c['time_steps'], 10 ** 9, fileName='/tmp/_golden_%s.hdf5' % name)
+            m.GPU_Wigner2D_GPitaevskii_Bloch.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude,
+                                                      prm.hbar, prm.mass, prm.potential, prm.kinetic)
+    W0 = wigner_initial(prm, c['init'])
+    with h.quiet():
+        inst = Instance()
+        inst.W_init = W0.copy()
+        inst.Run()
+    avg = np.stack([inst.X_average, inst.X2_average, inst.P_average, inst.P2_average,
+                    inst.Hamiltonian_average], 1)
+    W = np.asarray(inst.W_0.real)
+    nle = np.asarray(getattr(inst, 'NonLinearEnergyHistory', np.zeros(0)), dtype=np.float64)
+    return dict(params=json.dumps(c), avg=avg, energy=np.asarray(inst.TotalEnergyHistory, dtype=np.float64),
+                nle=nle, purity=np.asarray(inst.purity, dtype=np.float64), end_dec=W[::2, ::2].copy(),
+                end_sums=np.array([W.sum(), (W * W).sum()]),
+                init_sum=np.array([W0.sum(), (W0 * W0).sum()]))
+
+
 def run_dirac_case(name, c):
     d = h.load_reference_module('GPU_Dirac2D')
     prm_keys = {k: v for k, v in c.items() if k not in ('time_steps', 'p_init')}
@@ -222,6 +262,7 @@ def run_dirac_case(name, c):
 def main(names):
     cases = dict(WIGNER_CASES)
     cases.update(GP_CASES)
+    cases.update(BLOCH_CASES)
     cases.update(DIRAC_CASES)
     for name in names or list(cases):
         t0 = time.time()
@@ -230,6 +271,8 @@ def main(names):
             out = run_dirac_case(name, c)
         elif name in GP_CASES:
             out = run_gp_case(name, c)
+        elif name in BLOCH_CASES:
+            out = run_bloch_case(name, c)
         else:
             out = run_wigner_case(name, c)
         path = os.path.join(HERE, name + '.npz')

@@ -64,3 +64,17 @@ def gp_case(name):
     else:
         W0 = wigner_cat_state(prm, *init[1:])
     return g, prm, a_gp, W0, steps + 1
+
+
+BLOCH_NAMES = ['bloch_gp', 'bloch_gp_doublewell']
+
+
+def bloch_case(name):
+    """(fixture, WignerParams, gp_coefficient, W0, timeSteps) of a
+    GPU_Wigner2D_GPitaevskii_Bloch case."""
+    g = load(name)
+    c = dict(g['params'])
+    steps, init, a_gp = c.pop('time_steps'), c.pop('init'), c.pop('gp_coefficient')
+    prm = WignerParams(**c)
+    W0 = np.ascontiguousarray(wigner_harmonic_oscillator(prm, *init[1:]))
+    return g, prm, a_gp, W0, steps

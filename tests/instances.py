@@ -84,3 +84,18 @@ def gp_instance(prm: WignerParams, a_gp, W0, time_steps):
     inst = Instance()
     inst.W_init = np.array(W0, copy=True)
     return inst
+
+
+def bloch_instance(prm: WignerParams, a_gp, W0, time_steps):
+    """A GPU_Wigner2D_GPitaevskii_Bloch instance the way a notebook builds one."""
+    from pywignercuda_b200 import GPU_Wigner2D_GPitaevskii_Bloch
+
+    class Instance(GPU_Wigner2D_GPitaevskii_Bloch):
+        def __init__(self):
+            self.GPitaevskiiCoeff = a_gp
+            self.SetTimeTrack(prm.dt, time_steps, 10 ** 9, fileName='')
+            GPU_Wigner2D_GPitaevskii_Bloch.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude,
+                                                    prm.hbar, prm.mass, prm.potential, prm.kinetic)
+    inst = Instance()
+    inst.W_init = np.array(W0, copy=True)
+    return inst

@@ -115,7 +115,9 @@ def test_strang_gp_compiles_and_is_validated():
     d.gp_coefficient = 0.5
     rc, log = jit(d)
     assert rc == 0, log
-    for k in ('wig_ppass_half', 'wig_ppass_half_final', 'wig_gp_colsum', 'wig_gp_marginal', 'wig_gp_phase'):
+    for k in ('wig_ppass_half', 'wig_ppass_half_final', 'wig_gp_colsum', 'wig_gp_marginal', 'wig_gp_phase',
+              'wig_bloch_ppass', 'wig_bloch_xpass', 'wig_gp_bloch', 'wig_bloch_reduce', 'wig_rowsum',
+              'wig_bloch_axpy'):
         assert k in log, k
     d.potential_phase = _lib.PHASE_KVN
     rc, log = jit(d)

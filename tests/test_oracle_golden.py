@@ -13,7 +13,8 @@ from oracle.common import rel_l2
 from oracle.strang_notebook import StrangNotebook, KNOWN_MIN_W, KNOWN_NORM
 from oracle.wigner2d import WignerOracle
 from oracle.dirac2d import DiracOracle
-from golden_cases import WIGNER_NAMES, DIRAC_NAMES, GP_NAMES, wigner_case, dirac_case, gp_case, obs_close
+from golden_cases import (WIGNER_NAMES, DIRAC_NAMES, GP_NAMES, BLOCH_NAMES, wigner_case, dirac_case, gp_case,
+                          bloch_case, obs_close)
 
 TOL = 1e-10
 
@@ -55,3 +56,18 @@ def test_gp_oracle_matches_reference(name):
     assert rel_l2(W.real[::2, ::2], g['end_dec']) < 1e-12
     if a_gp != 0.:
         assert np.max(np.abs(psq - g['psq']) / np.abs(g['psq'])) < 1e-12
+
+
+@pytest.mark.parametrize('name', BLOCH_NAMES)
+def test_bloch_oracle_matches_reference(name):
+    from oracle.gpitaevskii import BlochOracle
+    g, prm, a_gp, W0, steps = bloch_case(name)
+    # imaginary-time factors exp(-dt/4 (V + V)) span a wide range at large dt: 1e-10
+    tol = 1e-10
+    r = BlochOracle(prm, a_gp).run_bloch(W0, steps)
+    assert obs_close(r['avg'], g['avg'], tol) < tol
+    assert r['energy'].shape == g['energy'].shape            # same accepted / rejected steps
+    assert np.max(np.abs(r['energy'] - g['energy'])) < tol * np.max(np.abs(g['energy']))
+    assert np.max(np.abs(r['purity'] - g['purity'])) < tol
+    assert np.max(np.abs(r['nle'] - g['nle'])) < tol * np.max(np.abs(g['nle']))
+    assert rel_l2(r['W'].real[::2, ::2], g['end_dec']) < tol
