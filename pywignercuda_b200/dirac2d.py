@@ -11,7 +11,8 @@ components) and calls ``Run()``, which returns 0 and leaves ``Psi_end``,
 (momentum-space averages after ``Normalize_P``; no reference counterpart),
 ``NormKept_average`` (fraction of the norm the absorbing boundary kept in the
 preceding step) and ``frames`` (spinor or density every ``skipFrames`` steps,
-``save_Spinor`` / ``save_Density`` :703-737).
+``save_Spinor`` / ``save_Density`` :703-737).  With ``fileName`` set, the run
+writes the reference's file layout (``frames.py``).
 
 The propagation runs on the GPU through ``libwigner_b200.so``; device memory
 and the stream come from PyTorch.  There is no CPU path.
@@ -21,7 +22,7 @@ import ctypes
 import numpy as np
 from scipy.special import eval_genlaguerre, eval_laguerre, eval_legendre
 
-from . import _lib
+from . import _lib, frames
 from ._lib import DiracDesc, check, dptr
 from .wigner2d import _torch
 
@@ -193,18 +194,31 @@ class GPU_Dirac2D:
         dev = torch.device('cuda', self._device)
         n = int(self.timeSteps)
         skip = max(int(self.skipFrames), 1)
-        self.frames = {0: self._frame(P0)}
+        fileName = getattr(self, 'fileName', '')
+        sink = None
+        if fileName:                                       # :974-1009
+            sink = frames.open_write(fileName)
+            frames.dirac_header(sink, self)
+        emit = frames.dirac_frame(self.frameSaveMode) if sink is not None else \
+            frames.dirac_frame_nosink(self.frameSaveMode)
+        self.frames = {0: np.array(emit(sink, 0, P0), copy=True)}   # the initial spinor (:1030-1033)
         obs = np.empty((n, _lib.DIRAC_NOBS))
         with torch.cuda.device(dev):
             psi = torch.from_numpy(P0.copy()).to(dev)
-            t = 0
-            while t < n:
-                nxt = min(n, (t // skip + 1) * skip)
-                obs[t:nxt] = self.propagate(psi, nxt - t, t_index0=t)
-                t = nxt
-                if t % skip == 0:
-                    self.frames[t] = self._frame(psi.cpu().numpy())
-            self.Psi_end = psi.cpu().numpy()
+            writer = frames.FrameWriter(psi, sink, emit, keep=self.frames)
+            try:
+                t = 0
+                while t < n:
+                    nxt = min(n, (t // skip + 1) * skip)
+                    obs[t:nxt] = self.propagate(psi, nxt - t, t_index0=t)
+                    t = nxt
+                    if t % skip == 0:                      # after step t (:1105-1111)
+                        writer.capture(t, psi)
+                self.Psi_end = psi.cpu().numpy()
+            finally:
+                writer.close()
+        if sink is not None:
+            sink.close()
         self.Psi_init = P0
         self.timeRange = np.arange(1, n + 1)
         (self.X_average, self.Y_average, self.Alpha1_average, self.Alpha2_average, self.Beta_average,
@@ -212,7 +226,15 @@ class GPU_Dirac2D:
          self.NormKept_average) = [obs[:, k].copy() for k in range(10)]
         return 0
 
-    def _frame(self, psi):
-        if self.frameSaveMode == 'Spinor':
-            return np.array(psi, copy=True)
-        return np.fft.fftshift(self.Density_From_Spinor(psi)).astype(np.float32)
+    def load_Density(self, n, fileName=None):
+        """The density frame of step ``n`` (``load_Density`` :739-749)."""
+        return frames.read(fileName or self.fileName, '/' + str(n))
+
+    def load_Spinor(self, n, fileName=None):
+        """The spinor frame of step ``n`` (``load_Spinor`` :751-769)."""
+        f = frames.open_read(fileName or self.fileName)
+        try:
+            return np.array([np.array(f['%d/real/%d' % (k, n)][...]) + 1j * np.array(f['%d/imag/%d' % (k, n)][...])
+                             for k in range(1, 5)])
+        finally:
+            f.close()

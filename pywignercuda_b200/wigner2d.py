@@ -12,8 +12,9 @@ and leaves ``timeRange``, ``X_average``, ``X2_average``, ``P_average``,
 ``PdPotentialdX_average``, ``XdPotentialdX_average``, ``Hamiltonian_average``,
 ``negativeArea`` and ``W_end`` on the instance (``:1918-1954``), plus
 ``Norm_average`` (dX dP sum W of each sample) and ``frames`` (the W saved every
-``skipFrames`` steps, ``save_Frame`` :660-663; written to HDF5 as the reference
-does when h5py is importable and ``fileName`` is set).
+``skipFrames`` steps, ``save_Frame`` :660-663).  With ``fileName`` set, the run
+writes the reference's file layout (``frames.py``): HDF5 when h5py is
+importable, else ``fileName + '.npz'`` with the same keys.
 
 The propagation runs on the GPU through ``libwigner_b200.so``; device memory
 and the stream come from PyTorch.  There is no CPU path.
@@ -22,13 +23,8 @@ import ctypes
 
 import numpy as np
 
-from . import _lib
+from . import _lib, frames
 from ._lib import WigDesc, check, dptr
-
-try:                                   # HDF5 output is optional (h5py may be absent)
-    import h5py as _h5py
-except ImportError:                    # pragma: no cover - depends on the image
-    _h5py = None
 
 
 def _torch():
@@ -291,19 +287,24 @@ class GPU_Wigner2D_FFT(Propagator_Base):
                                   st.cuda_stream), 'wig_run')
         return obs
 
-    def _frame_sink(self):
-        if _h5py is not None and self.fileName:
-            import os
-            try:
-                os.remove(self.fileName)
-            except OSError:
-                pass
-            f = _h5py.File(self.fileName, 'w')
-            f['dx'], f['dtheta'], f['dp'], f['dlambda'] = self.dX, self.dTheta, self.dP, self.dLambda
-            f['x_gridDIM'], f['p_gridDIM'] = self.X_gridDIM, self.P_gridDIM
-            f['dt'], f['timeSteps'], f['skipFrames'] = self.dt, self.timeSteps, self.skipFrames
-            return f
-        return None
+    def _frame_writer(self, W):
+        """The output file (when ``fileName`` is set) with its header, and the
+        asynchronous frame writer that fills ``frames`` and the file."""
+        sink = None
+        if self.fileName:
+            sink = frames.open_write(self.fileName)
+            frames.wigner_header(sink, self)
+        self.frames = {}
+        emit = frames.wigner_frame if sink is not None else (lambda f, key, W: W)
+        return sink, frames.FrameWriter(W, sink, emit, keep=self.frames)
+
+    def WignerFunctionFromFile(self, n, fileName=None):
+        """The frame saved at step ``n`` (``WignerFunctionFromFile`` :908-917)."""
+        return frames.read(fileName or self.fileName, '/' + str(n))
+
+    def LoadEhrenfestFromFile(self):
+        """The observables and the first / last states of a run's file (:919-940)."""
+        frames.load_ehrenfest(self, self.fileName)
 
     def Run(self):
         torch = _torch()
@@ -316,25 +317,24 @@ class GPU_Wigner2D_FFT(Propagator_Base):
             n_total = int(self.timeSteps) + 1             # Run :1776 loops over 0..timeSteps
             skip = max(int(self.skipFrames), 1)
             obs = np.empty((n_total + 1, _lib.WIG_NOBS))
-            self.frames = {}
-            sink = self._frame_sink()
+            sink, writer = self._frame_writer(W)
             saved = []
             t, cont = 0, False
-            while t < n_total:
-                if t % skip == 0 and t <= self.timeSteps:
-                    if not cont:                           # W must be normalised first
-                        obs[0] = self.propagate(W, 0)[0]
-                        cont = True
-                    frame = W.cpu().numpy()
-                    self.frames[t] = frame
-                    saved.append(t)
-                    if sink is not None:
-                        sink.create_dataset(str(t), data=frame)
-                nxt = min(n_total, (t // skip + 1) * skip)
-                o = self.propagate(W, nxt - t, t_index0=t, continue_run=cont)
-                obs[t:nxt + 1] = o
-                t, cont = nxt, True
-            W_end = W.cpu().numpy()
+            try:
+                while t < n_total:
+                    if t % skip == 0 and t <= self.timeSteps:
+                        if not cont:                       # W must be normalised first
+                            obs[0] = self.propagate(W, 0)[0]
+                            cont = True
+                        writer.capture(t, W)               # the sample before step t (:1880-1882)
+                        saved.append(t)
+                    nxt = min(n_total, (t // skip + 1) * skip)
+                    o = self.propagate(W, nxt - t, t_index0=t, continue_run=cont)
+                    obs[t:nxt + 1] = o
+                    t, cont = nxt, True
+                W_end = W.cpu().numpy()
+            finally:
+                writer.close()
         n = int(self.timeSteps) + 1
         self.timeRange = np.arange(n) * self.dt
         self.timeRangeIndexSaved = saved
@@ -345,19 +345,7 @@ class GPU_Wigner2D_FFT(Propagator_Base):
         self.W_end_complex = W_end
         self.W_end = W_end.real.copy()
         if sink is not None:
-            sink['timeRange'] = self.timeRange
-            sink['timeRangeIndexSaved'] = saved
-            for key, arr in (('X_Ehrenfest', self.X_average), ('X2_Ehrenfest', self.X2_average),
-                             ('P_Ehrenfest', self.P_average), ('P2_Ehrenfest', self.P2_average),
-                             ('XP_Ehrenfest', self.XP_average),
-                             ('dPotentialdX_Ehrenfest', self.dPotentialdX_average),
-                             ('PdPotentialdX_average', self.PdPotentialdX_average),
-                             ('XdPotentialdX_average', self.XdPotentialdX_average),
-                             ('Hamiltonian_average', self.Hamiltonian_average)):
-                sink['/Ehrenfest/' + key] = arr
-            sink['W_init'] = np.asarray(self.W_init).real
-            sink['W_end'] = self.W_end
-            sink['negativeArea'] = self.negativeArea
+            frames.wigner_tail(sink, self)
             sink.close()
         return 0
 
@@ -430,21 +418,43 @@ class GPU_Wigner2D_GPitaevskii(GPU_Wigner2D_FFT):
         if W0.shape != (self.P_gridDIM, self.X_gridDIM):
             raise _lib.WignerArgumentError('W_init must have shape (P_gridDIM, X_gridDIM)')
         n = int(self.timeSteps) + 1                        # Run :1897 loops over 0..timeSteps
+        skip = max(int(self.skipFrames), 1)
         dev = torch.device('cuda', self._device)
+        after = np.empty((n, _lib.WIG_NOBS))
+        psq = []
+        saved = []
         with torch.cuda.device(dev):
             W = torch.from_numpy(W0.copy()).to(dev)
-            obs = self.propagate(W, n)                     # row k: before step k; row k + 1: after it
-            psq = self.probability_square(n) if self.GPitaevskiiCoeff != 0. else np.zeros(0)
-            W_end = W.cpu().numpy()
-        after = obs[1:n + 1]
+            sink, writer = self._frame_writer(W)
+            try:
+                t = 0                                      # steps done
+                while t < n:
+                    # frames follow step tIndex for tIndex % skipFrames == 0 (:1996-1999)
+                    nxt = 1 if t == 0 else ((t - 1) // skip + 1) * skip + 1
+                    end = min(nxt, n)
+                    o = self.propagate(W, end - t, t_index0=t, continue_run=t > 0)
+                    after[t:end] = o[1:]                   # row k + 1: after step k of the chunk
+                    if self.GPitaevskiiCoeff != 0.:
+                        psq.append(self.probability_square(end - t))
+                    if end == nxt:
+                        writer.capture(nxt - 1, W)
+                        saved.append(nxt - 1)
+                    t = end
+                W_end = W.cpu().numpy()
+            finally:
+                writer.close()
         self.timeRange = np.arange(n) * self.dt
+        self.timeRangeIndexSaved = saved
         self.Norm_average = after[:, 0].copy()
         (self.X_average, self.X2_average, self.P_average, self.P2_average, self.XP_average,
          self.dPotentialdX_average, self.PdPotentialdX_average, self.XdPotentialdX_average,
          self.Hamiltonian_average, self.negativeArea) = [after[:, k].copy() for k in range(1, 11)]
-        self.ProbabilitySquare_average = psq
+        self.ProbabilitySquare_average = np.concatenate(psq) if psq else np.zeros(0)
         self.W_end_complex = W_end
         self.W_end = W_end.real.copy()
+        if sink is not None:
+            frames.wigner_tail(sink, self, extra=(('ProbabilitySquare_average', 'ProbabilitySquare_average'),))
+            sink.close()
         return 0
 
 
@@ -468,6 +478,11 @@ class GPU_Wigner2D_GPitaevskii_Bloch(GPU_Wigner2D_GPitaevskii):
         self.fp_Damping_String = '0.'
         GPU_Wigner2D_GPitaevskii.__init__(self, X_gridDIM, P_gridDIM, X_amplitude, P_amplitude, hBar, mass,
                                           0., 0., 0., potentialString, '0.', kinematicString)
+        # the Bloch class's Hamiltonian uses the kinetic string (:2097-2101)
+        self.Hamiltonian = self.fft_shift2D(self.KineticEnergy(self.P) + self.Potential(0, self.X) + 0. * self.P)
+
+    def KineticEnergy(self, p):
+        return _eval(self.kinematicString, p=p, cf=self._coef())
 
     def _stats(self, W, normalise):
         out = np.empty(_lib.WIG_BLOCH_NSTATS)
@@ -528,6 +543,20 @@ class GPU_Wigner2D_GPitaevskii_Bloch(GPU_Wigner2D_GPitaevskii):
         W_end = self._relax(None, int(self.timeSteps))
         self.W_0_complex = W_end
         self.W_0 = W_end.real.copy()
+        if self.fileName:                                  # :2112-2115, :2300-2330
+            f = frames.open_write(self.fileName)
+            frames.wigner_header(f, self)
+            f['timeRange'] = self.timeRange
+            f['timeRangeIndexSaved'] = np.zeros(0, dtype=np.int64)
+            for key, attr in (('X_Ehrenfest', 'X_average'), ('X2_Ehrenfest', 'X2_average'),
+                              ('P_Ehrenfest', 'P_average'), ('P2_Ehrenfest', 'P2_average'),
+                              ('Hamiltonian_average', 'Hamiltonian_average')):
+                f['/Ehrenfest/' + key] = getattr(self, attr)
+            f['/Potential'] = np.broadcast_to(self.Potential(0, self.X_range), self.X_range.shape)
+            f['/PotentialString'] = self.potentialString
+            f['W_init'] = np.real(np.asarray(self.W_init))
+            f['W_0'] = self.W_0
+            f.close()
         return 0
 
     def Run_ExitedState1(self, timeSteps=None):
@@ -537,4 +566,6 @@ class GPU_Wigner2D_GPitaevskii_Bloch(GPU_Wigner2D_GPitaevskii):
         W0 = torch.from_numpy(np.ascontiguousarray(self.W_0_complex)).to(torch.device('cuda', self._device))
         W_end = self._relax(W0, int(self.timeSteps if timeSteps is None else timeSteps))
         self.W_1 = W_end.real.copy()
+        if self.fileName:                                  # :2532 adds W_1 to Run's file
+            frames.append(self.fileName, 'W_1', self.W_1)
         return 0

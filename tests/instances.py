@@ -6,7 +6,7 @@ from oracle.wigner2d import WignerParams
 from oracle.dirac2d import DiracParams
 
 
-def wigner_instance(prm: WignerParams, W0, time_steps, skip_frames=10 ** 9, exact=False):
+def wigner_instance(prm: WignerParams, W0, time_steps, skip_frames=10 ** 9, exact=False, file_name=''):
     from pywignercuda_b200 import GPU_Wigner2D_FFT, GPU_Wigner2D_ODM2, GPU_FokkerPlank2D_FFT
     from pywignercuda_b200 import _lib
     base = GPU_Wigner2D_ODM2 if prm.odm2 else (GPU_FokkerPlank2D_FFT if prm.kvn else GPU_Wigner2D_FFT)
@@ -20,7 +20,7 @@ def wigner_instance(prm: WignerParams, W0, time_steps, skip_frames=10 ** 9, exac
             self.fp_Damping_String = prm.fp_damping
             self.epsilon = prm.epsilon
             self.L_material = prm.L_material
-            self.SetTimeTrack(prm.dt, time_steps, skip_frames, fileName='')
+            self.SetTimeTrack(prm.dt, time_steps, skip_frames, fileName=file_name)
             if prm.kvn:
                 self.kinematicString = prm.kinetic
                 base.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude, prm.hbar,
@@ -45,7 +45,7 @@ def wigner_obs(inst):
                      inst.XdPotentialdX_average, inst.Hamiltonian_average, inst.negativeArea], 1)
 
 
-def dirac_instance(prm: DiracParams, psi0, time_steps, skip_frames=10 ** 9):
+def dirac_instance(prm: DiracParams, psi0, time_steps, skip_frames=10 ** 9, file_name='', mode='Density'):
     from pywignercuda_b200 import GPU_Dirac2D
 
     class Instance(GPU_Dirac2D):
@@ -53,9 +53,9 @@ def dirac_instance(prm: DiracParams, psi0, time_steps, skip_frames=10 ** 9):
             self.mass, self.c, self.hBar = prm.mass, prm.c, prm.hbar
             self.Potential_0_String, self.Potential_1_String = prm.A0, prm.A1
             self.Potential_2_String, self.Potential_3_String = prm.A2, prm.A3
-            self.fileName = ''
+            self.fileName = file_name
             GPU_Dirac2D.__init__(self, (prm.n_x, prm.n_y), (prm.x_amplitude, prm.y_amplitude), prm.dt,
-                                 time_steps, skip_frames, frameSaveMode='Density')
+                                 time_steps, skip_frames, frameSaveMode=mode)
     inst = Instance()
     inst.Psi_init = np.array(psi0, copy=True)
     return inst
@@ -66,7 +66,7 @@ def dirac_obs(inst):
                      inst.Beta_average, inst.KEnergy_average, inst.Potential_0_average], 1)
 
 
-def gp_instance(prm: WignerParams, a_gp, W0, time_steps):
+def gp_instance(prm: WignerParams, a_gp, W0, time_steps, skip_frames=10 ** 9, file_name=''):
     """A GPU_Wigner2D_GPitaevskii instance the way a notebook builds one."""
     from pywignercuda_b200 import GPU_Wigner2D_GPitaevskii
 
@@ -77,7 +77,7 @@ def gp_instance(prm: WignerParams, a_gp, W0, time_steps):
             self.fp_Damping_String = prm.fp_damping
             self.epsilon = prm.epsilon
             self.L_material = prm.L_material
-            self.SetTimeTrack(prm.dt, time_steps, 10 ** 9, fileName='')
+            self.SetTimeTrack(prm.dt, time_steps, skip_frames, fileName=file_name)
             GPU_Wigner2D_GPitaevskii.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude,
                                               prm.hbar, prm.mass, prm.d_theta, prm.d_lambda, prm.gamma,
                                               prm.potential, prm.dpotential, prm.kinetic)
@@ -86,14 +86,14 @@ def gp_instance(prm: WignerParams, a_gp, W0, time_steps):
     return inst
 
 
-def bloch_instance(prm: WignerParams, a_gp, W0, time_steps):
+def bloch_instance(prm: WignerParams, a_gp, W0, time_steps, file_name=''):
     """A GPU_Wigner2D_GPitaevskii_Bloch instance the way a notebook builds one."""
     from pywignercuda_b200 import GPU_Wigner2D_GPitaevskii_Bloch
 
     class Instance(GPU_Wigner2D_GPitaevskii_Bloch):
         def __init__(self):
             self.GPitaevskiiCoeff = a_gp
-            self.SetTimeTrack(prm.dt, time_steps, 10 ** 9, fileName='')
+            self.SetTimeTrack(prm.dt, time_steps, 10 ** 9, fileName=file_name)
             GPU_Wigner2D_GPitaevskii_Bloch.__init__(self, prm.n_x, prm.n_p, prm.x_amplitude, prm.p_amplitude,
                                                     prm.hbar, prm.mass, prm.potential, prm.kinetic)
     inst = Instance()
