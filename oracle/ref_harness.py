@@ -77,6 +77,7 @@ namespace pycuda {
 template <class T> using complex = std::complex<T>;
 template <class T> inline T real(const std::complex<T>& z) { return z.real(); }
 template <class T> inline T imag(const std::complex<T>& z) { return z.imag(); }
+template <class T> inline std::complex<T> conj(const std::complex<T>& z) { return std::conj(z); }
 }
 struct harness_uint3 { unsigned x, y, z; };
 static harness_uint3 threadIdx, blockIdx, blockDim, gridDim;

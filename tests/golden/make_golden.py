@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory from the reference's own code.
 
 Runs ``GPU_Wigner2D_FFT`` / ``GPU_Wigner2D_ODM2`` / ``GPU_FokkerPlank2D_FFT`` /
-``GPU_Wigner2D_GPitaevskii`` / ``GPU_Wigner2D_GPitaevskii_Bloch`` / ``GPU_Dirac2D`` from the
+``GPU_Wigner2D_GPitaevskii`` / ``GPU_Wigner2D_GPitaevskii_Bloch`` / ``GPU_Dirac2D`` / ``GPU_Dirac3D`` from the
 reference checkout through ``oracle.ref_harness`` (the reference's Python-2
 host code and its CUDA-C kernel strings, compiled for the CPU; ``numpy.fft``
 standing in for cuFFT) and stores, per case:
@@ -10,9 +10,10 @@ standing in for cuFFT) and stores, per case:
 * ``obs``     -- the per-step arrays ``Run()`` leaves on the instance, in the
   reference's column order (Wigner: X, X2, P, P2, XP, dPotentialdX,
   PdPotentialdX, XdPotentialdX, Hamiltonian, negativeArea; Dirac: X, Y,
-  Alpha1, Alpha2, Beta, KEnergy, Potential_0);
+  Alpha1, Alpha2, Beta, KEnergy, Potential_0; Dirac3D: X, Y, Z, Alpha1, Alpha2,
+  Alpha3, Potential_0, Px, Py, Pz, K_Energy);
 * ``end_dec`` -- the final state (``W_end`` or ``Psi_end``) decimated by 2 in
-  each grid axis (keeps the files small), and ``end_sums`` -- full-grid sums
+  each grid axis (Dirac3D: by 4 in z) to keep the files small, and ``end_sums`` -- full-grid sums
   (sum, sum of squares of the real part; for Dirac per component sum |psi|^2).
 
 Initial states are built by the oracle's initial-state helpers (the same
@@ -39,6 +40,7 @@ from oracle import ref_harness as h                       # noqa: E402
 from oracle.wigner2d import (WignerParams, wigner_harmonic_oscillator,  # noqa: E402
                              wigner_cat_state)
 from oracle.dirac2d import DiracParams, spinor_particle_spin_up       # noqa: E402
+from oracle.dirac3d import Dirac3DParams, spinor_particle_spin_up_3d  # noqa: E402
 
 WIGNER_CASES = {
     # harmonic oscillator, no damping (the physics of the 256^2 plain case)
@@ -124,6 +126,19 @@ DIRAC_CASES = {
     'dirac_magnetic': dict(n_x=128, n_y=128, x_amplitude=12., y_amplitude=12., dt=0.01,
                            mass=1., c=1., A0=' 0.1*x ', A1='-0.5*y', A2=' 0.5*x', A3=' 0.2 ',
                            time_steps=100, p_init=(1., 0.5)),
+}
+
+# GPU_Dirac3D on cubic grids only: its plan cufftPlanMany(3, [X, Y, Z]) matches the (Z, Y, X)
+# arrays when X == Z (the harness transforms the arrays as laid out)
+DIRAC3D_CASES = {
+    # softened Coulomb, c = 137.036, packet moving along x and z
+    'dirac3d_coulomb': dict(n_x=32, n_y=32, n_z=32, x_amplitude=8., y_amplitude=8., z_amplitude=8., dt=1e-4,
+                            mass=1., c=137.036, A0='-1./sqrt(x*x+y*y+z*z+0.5)', A1='0.', A2='0.', A3='0.',
+                            time_steps=20, p_init=(3., 0., 1.)),
+    # vector potential (field along z plus A3), time-dependent trap, unequal amplitudes, c = 20
+    'dirac3d_field': dict(n_x=32, n_y=32, n_z=32, x_amplitude=8., y_amplitude=6., z_amplitude=7., dt=2e-3,
+                          mass=1., c=20., A0='0.5*(x*x+y*y+z*z)*(1.+0.1*sin(5.*t))', A1='-0.5*y', A2='0.5*x',
+                          A3='0.2*z', time_steps=20, p_init=(1., -0.5, 0.5)),
 }
 
 
@@ -259,16 +274,47 @@ def run_dirac_case(name, c):
                 init_sum=np.array([np.sum(np.abs(p) ** 2) for p in psi0]))
 
 
+def run_dirac3d_case(name, c):
+    d = h.load_reference_module('GPU_Dirac3D')
+    prm = Dirac3DParams(**{k: v for k, v in c.items() if k not in ('time_steps', 'p_init')})
+
+    class Instance(d.GPU_Dirac3D):
+        def __init__(self):
+            self.mass, self.c, self.hBar = prm.mass, prm.c, prm.hbar
+            self.Potential_0_String, self.Potential_1_String = prm.A0, prm.A1
+            self.Potential_2_String, self.Potential_3_String = prm.A2, prm.A3
+            self.fileName = '/tmp/_golden_%s.hdf5' % name
+            self.Compute_Ehrenfest_P = True
+            d.GPU_Dirac3D.__init__(self, (prm.n_x, prm.n_y, prm.n_z),
+                                   (prm.x_amplitude, prm.y_amplitude, prm.z_amplitude),
+                                   prm.dt, c['time_steps'], 10 ** 9, frameSaveMode='Density')
+    psi0 = spinor_particle_spin_up_3d(prm, c['p_init'], lambda x, y, z: np.exp(-(x * x + y * y + z * z) / 2.))
+    with h.quiet():
+        inst = Instance()
+        inst.Psi_init = psi0.copy()
+        inst.Run()
+    obs = np.stack([inst.X_average, inst.Y_average, inst.Z_average, inst.Alpha1_average, inst.Alpha2_average,
+                    inst.Alpha3_average, inst.Potential_0_average, inst.Px_average, inst.Py_average,
+                    inst.Pz_average, np.real(inst.K_Energy_average)], 1)
+    P = np.asarray(inst.Psi_end)
+    return dict(params=json.dumps(c), obs=obs, end_dec=P[:, ::4, ::2, ::2].copy(),
+                end_sums=np.array([np.sum(np.abs(p) ** 2) for p in P]),
+                init_sum=np.array([np.sum(np.abs(p) ** 2) for p in psi0]))
+
+
 def main(names):
     cases = dict(WIGNER_CASES)
     cases.update(GP_CASES)
     cases.update(BLOCH_CASES)
     cases.update(DIRAC_CASES)
+    cases.update(DIRAC3D_CASES)
     for name in names or list(cases):
         t0 = time.time()
         c = cases[name]
         if name in DIRAC_CASES:
             out = run_dirac_case(name, c)
+        elif name in DIRAC3D_CASES:
+            out = run_dirac3d_case(name, c)
         elif name in GP_CASES:
             out = run_gp_case(name, c)
         elif name in BLOCH_CASES:

@@ -11,6 +11,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
 WIGNER_NAMES = ['wigner_ho_plain', 'wigner_cl_doublewell', 'wigner_cl_timedep', 'wigner_odm',
                 'wigner_odm2', 'fokkerplanck_kvn', 'fokkerplanck_kvn_nonorm']
 DIRAC_NAMES = ['dirac_coulomb', 'dirac_magnetic']
+DIRAC3D_NAMES = ['dirac3d_coulomb', 'dirac3d_field']
 
 
 def load(name):
@@ -38,6 +39,17 @@ def dirac_case(name):
     steps, p_init = c.pop('time_steps'), c.pop('p_init')
     prm = DiracParams(**c)
     psi0 = spinor_particle_spin_up(prm, tuple(p_init), lambda x, y: np.exp(-(x * x + y * y) / 2.))
+    return g, prm, psi0, steps
+
+
+def dirac3d_case(name):
+    """(fixture, Dirac3DParams, psi0, timeSteps) of a GPU_Dirac3D case."""
+    from oracle.dirac3d import Dirac3DParams, spinor_particle_spin_up_3d
+    g = load(name)
+    c = dict(g['params'])
+    steps, p_init = c.pop('time_steps'), c.pop('p_init')
+    prm = Dirac3DParams(**c)
+    psi0 = spinor_particle_spin_up_3d(prm, tuple(p_init), lambda x, y, z: np.exp(-(x * x + y * y + z * z) / 2.))
     return g, prm, psi0, steps
 
 

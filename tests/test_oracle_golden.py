@@ -13,8 +13,8 @@ from oracle.common import rel_l2
 from oracle.strang_notebook import StrangNotebook, KNOWN_MIN_W, KNOWN_NORM
 from oracle.wigner2d import WignerOracle
 from oracle.dirac2d import DiracOracle
-from golden_cases import (WIGNER_NAMES, DIRAC_NAMES, GP_NAMES, BLOCH_NAMES, wigner_case, dirac_case, gp_case,
-                          bloch_case, obs_close)
+from golden_cases import (WIGNER_NAMES, DIRAC_NAMES, DIRAC3D_NAMES, GP_NAMES, BLOCH_NAMES, wigner_case,
+                          dirac_case, dirac3d_case, gp_case, bloch_case, obs_close)
 
 TOL = 1e-10
 
@@ -71,3 +71,14 @@ def test_bloch_oracle_matches_reference(name):
     assert np.max(np.abs(r['purity'] - g['purity'])) < tol
     assert np.max(np.abs(r['nle'] - g['nle'])) < tol * np.max(np.abs(g['nle']))
     assert rel_l2(r['W'].real[::2, ::2], g['end_dec']) < tol
+
+
+@pytest.mark.parametrize('name', DIRAC3D_NAMES)
+def test_dirac3d_oracle_matches_reference(name):
+    from oracle.dirac3d import Dirac3DOracle
+    g, prm, psi0, steps = dirac3d_case(name)
+    assert np.allclose([np.sum(np.abs(p) ** 2) for p in psi0], g['init_sum'], rtol=1e-14)
+    obs, P = Dirac3DOracle(prm).run(psi0, steps)
+    assert obs_close(obs[:, :11], g['obs'], TOL) < TOL
+    assert rel_l2(P[:, ::4, ::2, ::2], g['end_dec']) < TOL
+    assert np.allclose([np.sum(np.abs(p) ** 2) for p in P], g['end_sums'], rtol=1e-12)
