@@ -83,6 +83,7 @@ enum wig_potential_phase {
 
 #define WIG_NOBS 11   /* norm, <x>, <x^2>, <p>, <p^2>, <xp>, <V'>, <pV'>, <xV'>, <H>, negative area */
 #define DIRAC_NOBS 10 /* <x>, <y>, <alpha1>, <alpha2>, <beta>, <K>, <A0>, <px>, <py>, norm_kept */
+#define DIRAC3_NOBS 12 /* <x>, <y>, <z>, <alpha1>, <alpha2>, <alpha3>, <A0>, <px>, <py>, <pz>, <K>, norm */
 
 typedef struct wig_handle wig_handle;
 typedef struct dirac_handle dirac_handle;
@@ -213,6 +214,49 @@ int dirac_run_host(dirac_handle* h, const void* psi_in_host, void* psi_out_host,
                    int64_t n_steps, double* obs_host, void* stream);
 
 int dirac_destroy(dirac_handle* h);
+
+/* Dirac3D instance: GPU_Dirac3D(gridDIM, amplitude, dt, ...) and the attributes
+ * mass, c, hBar, Potential_{0..3}_String (GPU_Dirac3D.py:616-757).  Grids are
+ * powers of two in [16, 512] per axis; the spinor is (4, n_z, n_y, n_x)
+ * complex128, each axis FFT-shifted. */
+typedef struct dirac3_handle dirac3_handle;
+typedef struct dirac3_desc {
+  int32_t abi_version;
+  int32_t n_x, n_y, n_z;
+  int32_t constants;           /* wig_constants */
+  int32_t precision;           /* wig_precision (WIG_PREC_C128) */
+  double x_amplitude, y_amplitude, z_amplitude;
+  double mass, c, hbar, dt;    /* mass > 0 */
+  const char* a0;              /* Potential_0_String, C expression in (t, x, y, z) */
+  const char* a1;
+  const char* a2;
+  const char* a3;
+  double coef[8];              /* values of cf[0] .. cf[7] in the expressions */
+} dirac3_desc;
+
+/* Replaces GPU_Dirac3D.__init__'s kernel compilation and plan (GPU_Dirac3D.py:690-757). */
+int dirac3_create(const dirac3_desc* desc, dirac3_handle** out);
+
+/* GPU_Dirac3D.Run's loop (:1325-1465): n_steps >= 1 propagations at
+ * t = (t_index0 + k) * dt, k = 1..n_steps, in place on the device spinor psi.
+ * Without WIG_RUN_CONTINUE the spinor is first normalised (Normalize_GPU,
+ * :1323) and the momentum-space norm of the t_index = 1 spectrum is taken
+ * again; with it, the run continues an earlier one on this handle.  obs_host
+ * (may be NULL) receives n_steps x DIRAC3_NOBS doubles, sample k taken before
+ * propagation k + 1 as Run records them (the momentum averages divided by the
+ * step-1 norm, Compute_Ehrenfest_P :1366-1395, always computed).  Synchronous
+ * when obs_host is given. */
+int dirac3_run(dirac3_handle* h, void* psi_dev, int64_t t_index0, int64_t n_steps, uint32_t flags,
+               double* obs_host, void* stream);
+
+/* dirac3_run on host buffers (the Psi_init upload :1296-1299, Psi_end download :1474). */
+int dirac3_run_host(dirac3_handle* h, const void* psi_in_host, void* psi_out_host, int64_t t_index0,
+                    int64_t n_steps, uint32_t flags, double* obs_host, void* stream);
+
+int dirac3_destroy(dirac3_handle* h);
+
+/* Compile-only check of a Dirac3D instance's kernels (no GPU needed). */
+int dirac3_jit_check(const dirac3_desc* desc, char* log, int64_t log_cap);
 
 /* ---------------------------------------------------------------- batched FP32
  * Many independent Wigner2D instances with polynomial potentials

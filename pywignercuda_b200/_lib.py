@@ -16,6 +16,7 @@ ABI_VERSION = 3
 WIG_NOBS = 11
 WIG_BLOCH_NSTATS = 10
 DIRAC_NOBS = 10
+DIRAC3_NOBS = 12
 WIG_RUN_CONTINUE = 1
 WIG_RUN_PROFILE = 2
 WIG_RUN_GRAPH = 4
@@ -104,6 +105,15 @@ class DiracDesc(ctypes.Structure):
                 ('coef', c_double * 8)]
 
 
+class Dirac3Desc(ctypes.Structure):
+    _fields_ = [('abi_version', c_int32), ('n_x', c_int32), ('n_y', c_int32), ('n_z', c_int32),
+                ('constants', c_int32), ('precision', c_int32),
+                ('x_amplitude', c_double), ('y_amplitude', c_double), ('z_amplitude', c_double),
+                ('mass', c_double), ('c', c_double), ('hbar', c_double), ('dt', c_double),
+                ('a0', c_char_p), ('a1', c_char_p), ('a2', c_char_p), ('a3', c_char_p),
+                ('coef', c_double * 8)]
+
+
 # (name, restype, argtypes) of every symbol include/wigner_b200.h declares
 SIGNATURES = [
     ('wig_create', c_int, [POINTER(WigDesc), POINTER(c_void_p)]),
@@ -122,6 +132,11 @@ SIGNATURES = [
                                POINTER(_DP), c_void_p]),
     ('dirac_run_host', c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, _DP, c_void_p]),
     ('dirac_destroy', c_int, [c_void_p]),
+    ('dirac3_create', c_int, [POINTER(Dirac3Desc), POINTER(c_void_p)]),
+    ('dirac3_run', c_int, [c_void_p, c_void_p, c_int64, c_int64, c_uint32, _DP, c_void_p]),
+    ('dirac3_run_host', c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_uint32, _DP, c_void_p]),
+    ('dirac3_destroy', c_int, [c_void_p]),
+    ('dirac3_jit_check', c_int, [POINTER(Dirac3Desc), c_char_p, c_int64]),
     ('wig_jit_check', c_int, [POINTER(WigDesc), c_char_p, c_int64]),
     ('dirac_jit_check', c_int, [POINTER(DiracDesc), c_char_p, c_int64]),
     ('wigb_create', c_int, [c_void_p, c_int64, c_int32, POINTER(c_void_p)]),

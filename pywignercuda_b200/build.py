@@ -24,7 +24,8 @@ NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 # generated include -> {string name: JIT entry file}
 JIT_SOURCES = {'wig_device_src.inc': {'kJitWignerSource': 'wig_jit_wigner.cuh', 'kJitDiracSource': 'wig_jit_dirac.cuh',
                                       'kJitBatchSource': 'wig_jit_batch.cuh'},
-               'wig_adjoint_src.inc': {'kJitAdjointSource': 'wig_jit_adjoint.cuh'}}
+               'wig_adjoint_src.inc': {'kJitAdjointSource': 'wig_jit_adjoint.cuh'},
+               'wig_dirac3_src.inc': {'kJitDirac3Source': 'wig_jit_dirac3.cuh'}}
 
 
 def inline(fn, seen=None):

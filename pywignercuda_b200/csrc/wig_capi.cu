@@ -289,6 +289,22 @@ int occupancy(CUfunction f, int threads, int dyn_smem) {
   return n < 1 ? 1 : n;
 }
 
+int ensure_obs(double** buf, size_t* cap, size_t need) {
+  if (need <= *cap) return WIG_OK;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  WIG_CUDA(cudaMalloc((void**)buf, need * sizeof(double)));
+  *cap = need;
+  return WIG_OK;
+}
+
+int check_finite(const double* v, size_t n, const char* what) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(v[i])) return fail(WIG_ERR_NONFINITE, "%s: non-finite value at index %zu", what, i);
+  return WIG_OK;
+}
+
 }  // namespace wighost
 
 using namespace wighost;
@@ -576,22 +592,6 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
     if (rc) { B.free_all(); delete h; return rc; }
   }
   *out = h;
-  return WIG_OK;
-}
-
-static int ensure_obs(double** buf, size_t* cap, size_t need) {
-  if (need <= *cap) return WIG_OK;
-  if (*buf) cudaFree(*buf);
-  *buf = nullptr;
-  *cap = 0;
-  WIG_CUDA(cudaMalloc((void**)buf, need * sizeof(double)));
-  *cap = need;
-  return WIG_OK;
-}
-
-static int check_finite(const double* v, size_t n, const char* what) {
-  for (size_t i = 0; i < n; ++i)
-    if (!std::isfinite(v[i])) return fail(WIG_ERR_NONFINITE, "%s: non-finite value at index %zu", what, i);
   return WIG_OK;
 }
 

@@ -43,6 +43,26 @@ float2 twiddle_f(int n, long long m);
 // forward tf[a G + g] = W_n^{g a}, inverse ti[(i G + b) G + t] = W_n^{b (t Q + i)}.
 void rf_twiddles(int n, std::vector<float2>* tw);
 
+int launch2d(CUfunction f, unsigned gx, unsigned gy, unsigned block, unsigned smem, cudaStream_t st, void** args);
+bool pow2_in_range(int n);                    // power of two in [16, 4096]
+int clampi(int v, int lo, int hi);
+int round_warp(int v);                        // up to a multiple of 32
+// A constant as the reference's kernels see it: '%f' text (or exact), and its value.
+std::string fmt_const(double v, int mode);
+double kval(double v, int mode);
+// numpy linspace(-a, a - 2a/n, n) put through fftshift
+std::vector<double> shifted_range(double amp, int n);
+// tw[m] = exp(-2 pi i m / n), m < n, extended precision
+std::vector<double2> twiddles(int n);
+std::string expr_or(const char* s, const char* dflt);
+// An expression string that can be pasted between parentheses of a function body.
+bool safe_expr(const std::string& e);
+extern const char* kMathPrelude;
+// Grow a device observable buffer to `need` doubles.
+int ensure_obs(double** buf, size_t* cap, size_t need);
+// WIG_ERR_NONFINITE unless all n values are finite.
+int check_finite(const double* v, size_t n, const char* what);
+
 template <class T>
 int dev_upload(T** dst, const T* src, size_t n) {
   WIG_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));

@@ -123,6 +123,13 @@ def read(fileName, key):
         f.close()
 
 
+def copy_frame(frame):
+    """A private copy of a frame (an array, or a tuple of arrays)."""
+    if isinstance(frame, tuple):
+        return tuple(np.array(a, copy=True) for a in frame)
+    return np.array(frame, copy=True)
+
+
 class FrameWriter:
     """Asynchronous frame capture for one state shape.
 
@@ -179,7 +186,7 @@ class FrameWriter:
                     done.synchronize()
                     frame = self.emit(self.sink, key, self.host[slot].numpy())
                     if self.keep is not None:
-                        self.keep[key] = np.array(frame, copy=True)
+                        self.keep[key] = copy_frame(frame)
             except Exception as exc:                       # surfaced by capture() / close()
                 self.error = exc
             finally:
@@ -280,3 +287,36 @@ def dirac_frame_nosink(mode):
     if mode == 'Spinor':
         return lambda f, key, psi: psi
     return lambda f, key, psi: dirac_density(psi)
+
+
+# ---------------------------------------------------------------- Dirac3D layout
+def dirac3_header(f, inst):
+    """The datasets ``GPU_Dirac3D.Run`` writes before the loop (GPU_Dirac3D.py:1279-1293),
+    with the z values under the z keys (the reference stores the y values there)."""
+    f['x_gridDIM'], f['y_gridDIM'], f['z_gridDIM'] = inst.X_gridDIM, inst.Y_gridDIM, inst.Z_gridDIM
+    f['x_amplitude'], f['y_amplitude'], f['z_amplitude'] = inst.X_amplitude, inst.Y_amplitude, inst.Z_amplitude
+    f['dx'], f['dy'], f['dz'] = inst.dX, inst.dY, inst.dZ
+    for k in range(4):
+        name = 'Potential_%d_String' % k
+        f[name] = getattr(inst, name)
+
+
+def dirac3_frame(mode, to_file=True):
+    """``save_Density`` (fftshift of sum_k |psi_k|^2 as float32) or, in ``'Spinor'`` mode,
+    ``save_Spinor_SliceYZ`` at slice 0, 0: ``'xy/<k>/real|imag/<t>'`` = psi_k[0, :, :] and
+    ``'xz/<k>/real|imag/<t>'`` = psi_k[:, 0, :] (GPU_Dirac3D.py:1041-1094).  The frame kept
+    in memory is the density, or the pair of slice arrays."""
+    def emit(f, key, psi):
+        if mode == 'Spinor':
+            xy, xz = np.array(psi[:, 0, :, :]), np.array(psi[:, :, 0, :])
+            if to_file:
+                for k in range(4):
+                    for plane, arr in (('xy', xy), ('xz', xz)):
+                        f['%s/%d/real/%s' % (plane, k + 1, key)] = arr[k].real
+                        f['%s/%d/imag/%s' % (plane, k + 1, key)] = arr[k].imag
+            return xy, xz
+        rho = dirac_density(psi)
+        if to_file:
+            f[str(key)] = rho
+        return rho
+    return emit

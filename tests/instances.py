@@ -99,3 +99,28 @@ def bloch_instance(prm: WignerParams, a_gp, W0, time_steps, file_name=''):
     inst = Instance()
     inst.W_init = np.array(W0, copy=True)
     return inst
+
+
+def dirac3d_instance(prm, psi0, time_steps, skip_frames=10 ** 9, file_name='', mode='Density'):
+    """A GPU_Dirac3D instance the way a notebook builds one."""
+    from pywignercuda_b200 import GPU_Dirac3D
+
+    class Instance(GPU_Dirac3D):
+        def __init__(self):
+            self.mass, self.c, self.hBar = prm.mass, prm.c, prm.hbar
+            self.Potential_0_String, self.Potential_1_String = prm.A0, prm.A1
+            self.Potential_2_String, self.Potential_3_String = prm.A2, prm.A3
+            self.fileName = file_name
+            self.Compute_Ehrenfest_P = True
+            GPU_Dirac3D.__init__(self, (prm.n_x, prm.n_y, prm.n_z), (prm.x_amplitude, prm.y_amplitude,
+                                                                     prm.z_amplitude),
+                                 prm.dt, time_steps, skip_frames, frameSaveMode=mode)
+    inst = Instance()
+    inst.Psi_init = np.array(psi0, copy=True)
+    return inst
+
+
+def dirac3d_obs(inst):
+    return np.stack([inst.X_average, inst.Y_average, inst.Z_average, inst.Alpha1_average, inst.Alpha2_average,
+                     inst.Alpha3_average, inst.Potential_0_average, inst.Px_average, inst.Py_average,
+                     inst.Pz_average, inst.K_Energy_average, inst.Norm_average], 1)
