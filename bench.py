@@ -19,10 +19,11 @@ the FP32 run's norm / energy error against a complex128 run of every instance.
 
 Other workloads: --workload c128 (the plain line alone), dirac (Dirac2D 512^2,
 16 replicas), gp (GPU_Wigner2D_GPitaevskii: Strang splitting + mean-field term
-on the 1024^2 double well, 16 replicas).
+on the 1024^2 double well, 16 replicas), dirac3d (GPU_Dirac3D 256^3, a 1 GB
+spinor).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload batch|c128|dirac|gp]
+                  [--workload batch|c128|dirac|dirac3d|gp]
 
 N > 1 (torchrun): the batch has 64 N instances partitioned by cost across the
 ranks (weak scaling; no data-path collective, the observables are gathered to
@@ -610,6 +611,96 @@ def run_dirac(args, world, rank, local):
         print(json.dumps(line))
 
 
+D3N = 256
+D3_BYTES = 512   # per grid point per step: 4 passes x (read + write of 4 complex128 components)
+
+
+def make_dirac3d_instance(n, time_steps):
+    from pywignercuda_b200 import GPU_Dirac3D
+
+    class Coulomb3D(GPU_Dirac3D):
+        def __init__(self):
+            self.mass, self.c, self.hBar = 1., 137.036, 1.
+            self.Potential_0_String = '-1./sqrt(x*x+y*y+z*z+0.5)'
+            self.Potential_1_String = self.Potential_2_String = self.Potential_3_String = '0.'
+            self.fileName = ''
+            self.Compute_Ehrenfest_P = True
+            GPU_Dirac3D.__init__(self, (n, n, n), (12., 12., 12.), 1e-4, time_steps, 10 ** 9)
+    return Coulomb3D()
+
+
+def run_dirac3d(args, world, rank, local):
+    """Dirac3D 256^3 (a 1 GB spinor), c = 137.036, softened Coulomb, packet
+    p0 = (5, 0, 1), dt = 1e-4, complex128, one instance per GPU (dirac3_run)."""
+    import torch
+    from pywignercuda_b200 import _lib
+    from oracle.dirac3d import Dirac3DOracle, Dirac3DParams
+    lib = _lib.load()
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    steps = args.steps
+    inst = make_dirac3d_instance(D3N, steps)
+    gauss = lambda x, y, z: np.exp(-(x * x + y * y + z * z) / 2.)
+    P0 = np.ascontiguousarray(inst.Spinor_Particle_SpinUp((5., 0., 1.), gauss), dtype=np.complex128)
+    psi = torch.from_numpy(P0).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    obs = np.empty((max(steps, args.warmup), _lib.DIRAC3_NOBS))
+    _lib.check(lib.dirac3_run(inst._handle, psi.data_ptr(), 0, args.warmup, 0, _lib.dptr(obs),
+                              stream.cuda_stream), 'warm-up')
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        _lib.check(lib.dirac3_run(inst._handle, psi.data_ptr(), args.warmup, steps, _lib.WIG_RUN_CONTINUE, None,
+                                  stream.cuda_stream), 'timed')
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = barrier_max(world, e0.elapsed_time(e1))
+    npts = D3N ** 3
+    value = world * npts * steps / (ms / 1e3)
+    peak, peak_kind = peaks()
+    achieved = D3_BYTES * npts / (ms / 1e3 / steps) / 1e9
+    # end to end: host spinor in, host spinor and observables out, through dirac3_run_host
+    host_in = P0
+    host_out = np.empty_like(P0)
+    obs_e2e = np.empty((steps, _lib.DIRAC3_NOBS))
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    _lib.check(lib.dirac3_run_host(inst._handle, host_in.ctypes.data, host_out.ctypes.data, 0, steps, 0,
+                                   _lib.dptr(obs_e2e), stream.cuda_stream), 'e2e')
+    e2e_s = barrier_max(world, time.perf_counter() - t0)
+    line = {'metric': 'Dirac3D spinor-pt-steps/s', 'value': value, 'unit': 'spinor-pt-steps/s',
+            'n_gpus': world, 'steps': steps, 'warmup': args.warmup, 'ms_per_step': ms / steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c128',
+            'data': 'synthetic',
+            'config': {'workload': 'Dirac3D 256^3, [-12,12)^3, c=137.036 softened Coulomb, p0=(5,0,1), dt=1e-4',
+                       'l2': 'spinor 1074 MB > 126 MB L2'},
+            'e2e': {'value': world * npts * steps / e2e_s, 'unit': 'spinor-pt-steps/s',
+                    'h2d_bytes_per_step': P0.nbytes / steps, 'd2h_bytes_per_step': (P0.nbytes + obs_e2e.nbytes) / steps},
+            'roofline': {'bound': 'hbm', 'kernel': 'd3_xpass + 2 d3_ypass + d3_zpass (step average)',
+                         'algorithmic_bytes_per_point': D3_BYTES, 'achieved': achieved, 'peak': peak,
+                         'unit': 'GB/s', 'frac': achieved / peak, 'peak_kind': peak_kind, 'traffic': None},
+            'gpu_launches': 4 * steps + 1, 'clocks': clk.summary()}
+    if rank == 0 and args.cpu_baseline:
+        n = 128
+        prm = Dirac3DParams(n, n, n, 12., 12., 12., 1e-4, c=137.036, A0='-1./sqrt(x*x+y*y+z*z+0.5)')
+        orc = Dirac3DOracle(prm)
+        from oracle.dirac3d import spinor_particle_spin_up_3d
+        P = spinor_particle_spin_up_3d(prm, (5., 0., 1.), gauss)
+        t0, k = time.perf_counter(), 0
+        while time.perf_counter() - t0 < 10. or k < 1:
+            orc.run(P, 1, t_index0=k, normalise=(k == 0))
+            k += 1
+        dt_cpu = time.perf_counter() - t0
+        line['cpu_baseline'] = {'value': n ** 3 * k / dt_cpu, 'unit': 'spinor-pt-steps/s',
+                                'cores': os.cpu_count(), 'kind': 'port',
+                                'sample': '%d steps of the oracle (numpy + scipy.fft) at 128^3, same physics' % k}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -618,7 +709,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--replicas', type=int, default=REPLICAS)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
-    ap.add_argument('--workload', default='batch', choices=['batch', 'c128', 'dirac', 'gp'])
+    ap.add_argument('--workload', default='batch', choices=['batch', 'c128', 'dirac', 'dirac3d', 'gp'])
     ap.add_argument('--profile-only', action='store_true',
                     help='batch workload: only the timed section (for profiler launch lists)')
     args = ap.parse_args()
@@ -633,6 +724,8 @@ def main():
             run_c128(args, world, rank, local)
         elif args.workload == 'gp':
             run_gp(args, world, rank, local)
+        elif args.workload == 'dirac3d':
+            run_dirac3d(args, world, rank, local)
         else:
             run_batch(args, world, rank, local)
     finally:

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -58,6 +59,18 @@ int d3_plan(const dirac3_desc* d, Dirac3Plan* P) {
   P->yc = clampi(2048 / NY, 2, NX);
   P->ynt = round_warp(clampi(NY * P->yc / 8, 32, 256));
   P->zc = clampi(1024 / NZ, 1, NX);
+  // WIG_D3_TILING="rows,yc,zc" overrides the tile shapes for tuning runs (powers of two, clamped)
+  if (const char* t = getenv("WIG_D3_TILING")) {
+    int v[3] = {0, 0, 0};
+    if (sscanf(t, "%d,%d,%d", &v[0], &v[1], &v[2]) == 3) {
+      auto p2 = [](int x) { return x > 0 && (x & (x - 1)) == 0; };
+      if (p2(v[0])) P->rows = clampi(v[0], 1, NY * NZ);
+      if (p2(v[1])) P->yc = clampi(v[1], 1, NX);
+      if (p2(v[2])) P->zc = clampi(v[2], 1, NX);
+      P->xnt = round_warp(clampi(4 * P->rows * NX / 8, 32, 256));
+      P->ynt = round_warp(clampi(NY * P->yc / 8, 32, 256));
+    }
+  }
   P->znt = round_warp(clampi(4 * P->zc * NZ / 8, 32, 256));
   P->snt = 256;
   P->gx = clampi(NY * NZ / P->rows, 1, kMaxCta);

@@ -14,18 +14,19 @@ __device__ __forceinline__ UserPhys user_phys(const wig::Dirac3Args& a) {
   return ph;
 }
 
-extern "C" __global__ void __launch_bounds__(D3_XNT)
+// three resident CTAs per SM (80 registers), four for the y-passes (64)
+extern "C" __global__ void __launch_bounds__(D3_XNT, 3)
 d3_xpass(wig::Dirac3Args a, double2* psi, int mode, int parity, int normalise, double t_A, double t_obs,
          long long prev_tindex, double* obs_prev) {
   wig::d3_xpass_body<UserPhys, D3_NX, D3_NY, D3_NZ, D3_ROWS, D3_XNT>(a, user_phys(a), psi, mode, parity, normalise,
                                                                     t_A, t_obs, prev_tindex, obs_prev);
 }
 
-extern "C" __global__ void __launch_bounds__(D3_YNT) d3_ypass_fwd(wig::Dirac3Args a, double2* psi) {
+extern "C" __global__ void __launch_bounds__(D3_YNT, 4) d3_ypass_fwd(wig::Dirac3Args a, double2* psi) {
   wig::d3_ypass_body<D3_NX, D3_NY, D3_NZ, D3_YC, D3_YNT, false>(a, psi);
 }
 
-extern "C" __global__ void __launch_bounds__(D3_YNT) d3_ypass_inv(wig::Dirac3Args a, double2* psi) {
+extern "C" __global__ void __launch_bounds__(D3_YNT, 4) d3_ypass_inv(wig::Dirac3Args a, double2* psi) {
   wig::d3_ypass_body<D3_NX, D3_NY, D3_NZ, D3_YC, D3_YNT, true>(a, psi);
 }
 

@@ -189,8 +189,8 @@ def test_dirac3d_jit_compiles_without_spills(shape):
         assert at, k
         props = ' '.join(lines[at[0] + 1:at[0] + 3])
         spill = int(props.split(' bytes spill stores')[0].split()[-1])
-        # the z-pass runs two CTAs per SM (128 registers): a few bytes may spill
-        assert spill <= (128 if k == 'd3_zpass' else 0), (k, props)
+        # the z- and x-passes run two and three CTAs per SM (128 / 80 registers): a few bytes may spill
+        assert spill <= {'d3_zpass': 128, 'd3_xpass': 16}.get(k, 0), (k, props)
 
 
 def test_dirac3d_descriptor_validated():
