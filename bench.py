@@ -613,6 +613,9 @@ def run_dirac(args, world, rank, local):
 
 D3N = 256
 D3_BYTES = 512   # per grid point per step: 4 passes x (read + write of 4 complex128 components)
+# DRAM bytes of one step at 256^3 from one ncu capture (dram__bytes rate x duration of each of the
+# four passes, profiles/dirac3d_passes_256cube.md)
+NCU_TRAFFIC_D3 = 2.090e9 + 2.088e9 + 2.096e9 + 2.089e9
 
 
 def make_dirac3d_instance(n, time_steps):
@@ -681,7 +684,9 @@ def run_dirac3d(args, world, rank, local):
                     'h2d_bytes_per_step': P0.nbytes / steps, 'd2h_bytes_per_step': (P0.nbytes + obs_e2e.nbytes) / steps},
             'roofline': {'bound': 'hbm', 'kernel': 'd3_xpass + 2 d3_ypass + d3_zpass (step average)',
                          'algorithmic_bytes_per_point': D3_BYTES, 'achieved': achieved, 'peak': peak,
-                         'unit': 'GB/s', 'frac': achieved / peak, 'peak_kind': peak_kind, 'traffic': None},
+                         'unit': 'GB/s', 'frac': achieved / peak, 'peak_kind': peak_kind,
+                         'traffic': NCU_TRAFFIC_D3, 'traffic_per': 'step (4 launches), ncu at 256^3',
+                         'algorithmic_bytes_per_step': D3_BYTES * npts},
             'gpu_launches': 4 * steps + 1, 'clocks': clk.summary()}
     if rank == 0 and args.cpu_baseline:
         n = 128
