@@ -101,7 +101,7 @@ def bloch_instance(prm: WignerParams, a_gp, W0, time_steps, file_name=''):
     return inst
 
 
-def dirac3d_instance(prm, psi0, time_steps, skip_frames=10 ** 9, file_name='', mode='Density'):
+def dirac3d_instance(prm, psi0, time_steps, skip_frames=10 ** 9, file_name='', mode='Density', constants_mode=None):
     """A GPU_Dirac3D instance the way a notebook builds one."""
     from pywignercuda_b200 import GPU_Dirac3D
 
@@ -115,6 +115,8 @@ def dirac3d_instance(prm, psi0, time_steps, skip_frames=10 ** 9, file_name='', m
             GPU_Dirac3D.__init__(self, (prm.n_x, prm.n_y, prm.n_z), (prm.x_amplitude, prm.y_amplitude,
                                                                      prm.z_amplitude),
                                  prm.dt, time_steps, skip_frames, frameSaveMode=mode)
+    if constants_mode is not None:
+        Instance.constants_mode = constants_mode
     inst = Instance()
     inst.Psi_init = np.array(psi0, copy=True)
     return inst

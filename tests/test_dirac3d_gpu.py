@@ -76,3 +76,35 @@ def test_dirac3d_spinor_slices(tmp_path):
     xy, xz = inst.load_Spinor(6)
     assert np.array_equal(xy, inst.Psi_end[:, 0]) and np.array_equal(xz, inst.Psi_end[:, :, 0])
     assert np.array_equal(inst.frames[6][0], xy)
+
+
+def test_dirac3d_exact_constants_vs_oracle():
+    """Exact constants (no '%f' rounding) on both sides, 32 x 16 x 32."""
+    from pywignercuda_b200 import _lib
+    prm = Dirac3DParams(32, 16, 32, 7.3, 5.1, 6.7, 1.7e-3, mass=1.3, c=17.3, A0='0.3*(x*x+y*y+z*z)',
+                        A1='-0.4*y', A2='0.4*x', A3='0.', constants='exact')
+    psi0 = spinor_particle_spin_up_3d(prm, (0.7, -0.3, 0.2), _gauss)
+    inst = dirac3d_instance(prm, psi0, 8, constants_mode=_lib.CONST_EXACT)
+    assert inst.Run() == 0
+    obs, P = Dirac3DOracle(prm).run(psi0, 8)
+    assert obs_close(dirac3d_obs(inst), obs, TOL) < TOL
+    assert rel_l2(inst.Psi_end, P) < TOL
+
+
+def test_dirac3d_run_host_matches_device_run():
+    """dirac3_run_host (host buffers in and out) equals dirac3_run on a device tensor, bit for bit."""
+    import torch
+    from pywignercuda_b200 import _lib
+    prm = _field_prm()
+    psi0 = np.ascontiguousarray(spinor_particle_spin_up_3d(prm, (1., -0.5, 0.5), _gauss), dtype=np.complex128)
+    inst = dirac3d_instance(prm, psi0, 5)
+    lib = _lib.load()
+    st = torch.cuda.current_stream().cuda_stream
+    out = np.empty_like(psi0)
+    obs_h = np.empty((5, _lib.DIRAC3_NOBS))
+    _lib.check(lib.dirac3_run_host(inst._handle, psi0.ctypes.data, out.ctypes.data, 0, 5, 0, _lib.dptr(obs_h), st),
+               'dirac3_run_host')
+    t = torch.from_numpy(psi0.copy()).cuda()
+    obs_d = inst.propagate(t, 5)
+    assert np.array_equal(out, t.cpu().numpy())
+    assert np.array_equal(obs_h, obs_d)
