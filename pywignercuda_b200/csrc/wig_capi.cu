@@ -350,7 +350,7 @@ struct wig_handle {
 struct WigPlan {
   int xrows, xnt, pc, pnt, rnt, n_cta_x, n_cta_p, n_cta_r, smem_x, smem_p, damp;
   int strang, gp, smem_ph, smem_gph;
-  int xminb, pminb;
+  int xminb, pminb, xr, pr;
   int odm, smem_odm_x, smem_odm_p;
   double dX, dP, dTheta, dLambda;
   std::string src;
@@ -411,6 +411,16 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
       if (v[5] > 0) P->pminb = v[5];
     }
   }
+  // WIG_RADIX="xr,pr": largest Stockham radix (8 or 16) of the x-pass / p-pass transforms, for tuning runs
+  P->xr = 8;
+  P->pr = 8;
+  if (const char* tv = getenv("WIG_RADIX")) {
+    int v[2];
+    if (sscanf(tv, "%d,%d", &v[0], &v[1]) == 2) {
+      if (v[0] == 8 || v[0] == 16) P->xr = v[0];
+      if (v[1] == 8 || v[1] == 16) P->pr = v[1];
+    }
+  }
   P->rnt = 256;
   P->n_cta_x = NP / P->xrows;
   P->n_cta_p = NX / P->pc;
@@ -447,9 +457,9 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
            "#define WIG_NX %d\n#define WIG_NP %d\n#define WIG_XROWS %d\n#define WIG_XNT %d\n"
            "#define WIG_KIN_STRING %d\n#define WIG_PC %d\n#define WIG_PNT %d\n"
            "#define WIG_DAMP %d\n#define WIG_RNT %d\n#define WIG_XMINB %d\n#define WIG_PMINB %d\n"
-           "#define WIG_KVN %d\n#define WIG_STRANG %d\n",
+           "#define WIG_KVN %d\n#define WIG_STRANG %d\n#define WIG_XR %d\n#define WIG_PR %d\n",
            NX, NP, P->xrows, P->xnt, d->kinetic_from_string ? 1 : 0, P->pc, P->pnt, P->damp, P->rnt,
-           P->xminb, P->pminb, d->potential_phase == WIG_PHASE_KVN ? 1 : 0, P->strang);
+           P->xminb, P->pminb, d->potential_phase == WIG_PHASE_KVN ? 1 : 0, P->strang, P->xr, P->pr);
   src += macros;
   src += kJitWignerSource;
   P->src.swap(src);

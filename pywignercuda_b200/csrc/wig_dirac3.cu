@@ -25,6 +25,9 @@ constexpr int kMaxCta = 148 * 16;   // grid-stride passes: at most 16 CTAs per S
 
 struct Dirac3Plan {
   int rows, xnt, yc, ynt, zc, znt, snt;
+  // largest Stockham radix / CTAs per SM of each pass: radix 16 only where it fits the register
+  // budget without spilling (the z-pass: 126 registers, 3.00 vs 3.08 ms per 256^3 step)
+  int xr = 8, yr = 8, zr = 16, xmb = 3, ymb = 4, zmb = 2;
   int gx, gy, gz, gn;
   int smem_x, smem_y, smem_z;
   double dX, dY, dZ, dPx, dPy, dPz;
@@ -72,6 +75,17 @@ int d3_plan(const dirac3_desc* d, Dirac3Plan* P) {
     }
   }
   P->znt = round_warp(clampi(4 * P->zc * NZ / 8, 32, 256));
+  // WIG_D3_RADIX="xr,yr,zr,xmb,ymb,zmb" overrides the radix caps (8 or 16) and CTAs per SM for tuning runs
+  if (const char* t = getenv("WIG_D3_RADIX")) {
+    int v[6] = {0, 0, 0, 0, 0, 0};
+    if (sscanf(t, "%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]) == 6) {
+      auto rad = [](int x, int d) { return (x == 8 || x == 16) ? x : d; };
+      P->xr = rad(v[0], P->xr); P->yr = rad(v[1], P->yr); P->zr = rad(v[2], P->zr);
+      if (v[3] > 0) P->xmb = clampi(v[3], 1, 8);
+      if (v[4] > 0) P->ymb = clampi(v[4], 1, 8);
+      if (v[5] > 0) P->zmb = clampi(v[5], 1, 8);
+    }
+  }
   P->snt = 256;
   P->gx = clampi(NY * NZ / P->rows, 1, kMaxCta);
   P->gy = clampi(4 * NZ * (NX / P->yc), 1, kMaxCta);
@@ -99,11 +113,14 @@ int d3_plan(const dirac3_desc* d, Dirac3Plan* P) {
     src += "  __device__ __forceinline__ double A" + std::to_string(i) +
            "(double t, double x, double y, double z) const { return (" + *As[i] + "); }\n";
   src += "};\n";
-  char macros[512];
+  char macros[768];
   snprintf(macros, sizeof(macros),
            "#define D3_NX %d\n#define D3_NY %d\n#define D3_NZ %d\n#define D3_ROWS %d\n#define D3_XNT %d\n"
-           "#define D3_YC %d\n#define D3_YNT %d\n#define D3_ZC %d\n#define D3_ZNT %d\n#define D3_SNT %d\n",
-           NX, NY, NZ, P->rows, P->xnt, P->yc, P->ynt, P->zc, P->znt, P->snt);
+           "#define D3_YC %d\n#define D3_YNT %d\n#define D3_ZC %d\n#define D3_ZNT %d\n#define D3_SNT %d\n"
+           "#define D3_XR %d\n#define D3_YR %d\n#define D3_ZR %d\n#define D3_XMB %d\n#define D3_YMB %d\n"
+           "#define D3_ZMB %d\n",
+           NX, NY, NZ, P->rows, P->xnt, P->yc, P->ynt, P->zc, P->znt, P->snt, P->xr, P->yr, P->zr, P->xmb,
+           P->ymb, P->zmb);
   src += macros;
   src += kJitDirac3Source;
   P->src.swap(src);

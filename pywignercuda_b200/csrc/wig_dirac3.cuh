@@ -138,7 +138,7 @@ __device__ __forceinline__ void d3_finalize_sample(const Dirac3Args& a, const do
 // mode 0: first of a run (load, scale by *a.scale when `normalise`, sums, row FFT);
 // mode 1: row IFFT, A(t_A), sums at t_obs, row FFT; mode 2: row IFFT, A(t_A), store.
 // Modes 1 and 2 finalise the previous sample (partials of parity ^ 1) into obs_prev.
-template <class Phys, int NX, int NY, int NZ, int ROWS, int NT>
+template <class Phys, int NX, int NY, int NZ, int ROWS, int NT, int MAXR = 8>
 __device__ __forceinline__ void d3_xpass_body(const Dirac3Args& a, const Phys& ph, double2* __restrict__ psi,
                                               int mode, int parity, int normalise, double t_A, double t_obs,
                                               long long prev_tindex, double* obs_prev) {
@@ -164,7 +164,7 @@ __device__ __forceinline__ void d3_xpass_body(const Dirac3Args& a, const Phys& p
     }
     __syncthreads();
     if (mode != 0) {
-      cta_fft<double2, NX, 4 * ROWS, NT, true, M>(sm, a.tw_x);
+      cta_fft<double2, NX, 4 * ROWS, NT, true, M, MAXR>(sm, a.tw_x);
       __syncthreads();   // explicit barrier before the pointwise mix, as in the z-pass
     }
     for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
@@ -192,7 +192,7 @@ __device__ __forceinline__ void d3_xpass_body(const Dirac3Args& a, const Phys& p
       }
     }
     __syncthreads();   // cta_fft's first stage reads shared memory before its first barrier
-    if (mode != 2) cta_fft<double2, NX, 4 * ROWS, NT, false, M>(sm, a.tw_x);
+    if (mode != 2) cta_fft<double2, NX, 4 * ROWS, NT, false, M, MAXR>(sm, a.tw_x);
     for (int e = threadIdx.x; e < 4 * ROWS * NX; e += NT) {
       const int b = e / NX, k = e - b * NX;
       const int m = b / ROWS, r = b - m * ROWS;
@@ -208,7 +208,7 @@ __device__ __forceinline__ void d3_xpass_body(const Dirac3Args& a, const Phys& p
 
 // ---------------------------------------------------------------- y-pass
 // One tile = component m, plane z, columns x0 .. x0 + C - 1, all NY rows.
-template <int NX, int NY, int NZ, int C, int NT, bool INV>
+template <int NX, int NY, int NZ, int C, int NT, bool INV, int MAXR = 8>
 __device__ __forceinline__ void d3_ypass_body(const Dirac3Args& a, double2* __restrict__ psi) {
   typedef ColMap<C> M;
   extern __shared__ double2 sm[];
@@ -221,7 +221,7 @@ __device__ __forceinline__ void d3_ypass_body(const Dirac3Args& a, double2* __re
       sm[pad8(e)] = base[(size_t)k * NX + c];
     }
     __syncthreads();
-    cta_fft<double2, NY, C, NT, INV, M>(sm, a.tw_y);
+    cta_fft<double2, NY, C, NT, INV, M, MAXR>(sm, a.tw_y);
     for (int e = threadIdx.x; e < NY * C; e += NT) {
       const int k = e / C, c = e - k * C;
       base[(size_t)k * NX + c] = sm[pad8(e)];
@@ -233,7 +233,7 @@ __device__ __forceinline__ void d3_ypass_body(const Dirac3Args& a, double2* __re
 // ---------------------------------------------------------------- z-pass
 // One tile = row y, columns x0 .. x0 + C - 1, all NZ planes, 4 components;
 // smem [z][m C + c].  K mix: DiracPropagatorK_source (:386-452), half the mass.
-template <int NX, int NY, int NZ, int C, int NT>
+template <int NX, int NY, int NZ, int C, int NT, int MAXR = 8>
 __device__ __forceinline__ void d3_zpass_body(const Dirac3Args& a, double2* __restrict__ psi) {
   typedef ColMap<4 * C> M;
   extern __shared__ double2 sm[];
@@ -253,7 +253,7 @@ __device__ __forceinline__ void d3_zpass_body(const Dirac3Args& a, double2* __re
       sm[pad8(e)] = psi[m * comp + (size_t)k * plane + (size_t)iy * NX + x0 + c];
     }
     __syncthreads();
-    cta_fft<double2, NZ, 4 * C, NT, false, M>(sm, a.tw_z);
+    cta_fft<double2, NZ, 4 * C, NT, false, M, MAXR>(sm, a.tw_z);
     // cta_fft ends with a barrier, yet on B200 the K mix below read stale spectra
     // (scattered tiles, about half the points at 16^3 and 32^3) unless this explicit
     // barrier follows the transform; with it the pass matches numpy to 3e-16
@@ -292,7 +292,7 @@ __device__ __forceinline__ void d3_zpass_body(const Dirac3Args& a, double2* __re
       sm[i4] = cscale(cadd(cadd(cmul(U23, q1), cmul(U24, q2)), cmul(U33, q4)), inv_n);
     }
     __syncthreads();   // cta_fft's first stage reads shared memory before its first barrier
-    cta_fft<double2, NZ, 4 * C, NT, true, M>(sm, a.tw_z);
+    cta_fft<double2, NZ, 4 * C, NT, true, M, MAXR>(sm, a.tw_z);
     for (int e = threadIdx.x; e < 4 * C * NZ; e += NT) {
       const int k = e / (4 * C), q = e - k * (4 * C);
       const int m = q / C, c = q - m * C;

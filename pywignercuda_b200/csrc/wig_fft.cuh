@@ -6,7 +6,7 @@
 // and interleaved column tiles (p-pass: sequence = one grid column, the tile
 // stored row-major, so element k of column c sits at k*NB + c).
 //
-// Stockham autosort, mixed radix 8/4/2: stage s combines R sub-transforms of
+// Stockham autosort, mixed radix 16/8/4/2: stage s combines R sub-transforms of
 // length Ns into length Ns*R.  Butterfly j (0 <= j < N/R) reads elements
 // j + r*N/R, applies twiddles W_{Ns R}^{(j mod Ns) r}, does an R-point DFT and
 // writes to (j/Ns)*Ns*R + (j mod Ns) + r*Ns.  Output is in natural order.
@@ -75,10 +75,134 @@ template <bool INV, class C> __device__ __forceinline__ void dft8(C* v) {
   for (int m = 0; m < 4; ++m) { v[2 * m] = a[m]; v[2 * m + 1] = b[m]; }
 }
 
+// ---------------------------------------------------------------- radix-8/16/32 kernels
+// (also the per-lane DFTs of the register FFT, wig_rfft.cuh)
+// cos(pi j / 16) for any integer j
+__host__ __device__ constexpr double cospi16(int j) {
+  j = ((j % 32) + 32) % 32;
+  if (j > 16) j = 32 - j;
+  const bool neg = j > 8;
+  if (neg) j = 16 - j;
+  double c = 0.;
+  switch (j) {
+    case 0: c = 1.; break;
+    case 1: c = 0.98078528040323044912618223613424; break;
+    case 2: c = 0.92387953251128675612818318939679; break;
+    case 3: c = 0.83146961230254523707878837761791; break;
+    case 4: c = 0.70710678118654752440084436210485; break;
+    case 5: c = 0.55557023301960222474283081394853; break;
+    case 6: c = 0.38268343236508977172845998403040; break;
+    case 7: c = 0.19509032201612826784828486847702; break;
+    default: c = 0.; break;
+  }
+  return neg ? -c : c;
+}
+
+// u * c for a compile-time constant c.  In FP32 the constant is applied as a
+// compensated pair hi + lo (hi = c rounded, lo = the rounding error), so the
+// product carries only the rounding of the arithmetic: a constant rounded to
+// float alone has |w|^2 != 1 by up to 6e-8, and a forward/inverse pair of FFTs
+// would then scale some spectral components by a fixed factor every step.
+__device__ __forceinline__ float mulk(float u, double c) {
+  const float hi = (float)c, lo = (float)(c - (double)hi);
+  return fmaf(u, hi, u * lo);
+}
+__device__ __forceinline__ double mulk(double u, double c) { return u * c; }
+// u * c + v * s (c, s compile-time constants)
+__device__ __forceinline__ float mulk2(float u, double c, float v, double s) {
+  const float ch = (float)c, cl = (float)(c - (double)ch), sh = (float)s, sl = (float)(s - (double)sh);
+  return fmaf(u, ch, fmaf(v, sh, fmaf(u, cl, v * sl)));
+}
+__device__ __forceinline__ double mulk2(double u, double c, double v, double s) { return fma(u, c, v * s); }
+
+// v * W_32^j, W_32 = exp(-2 pi i / 32) (forward) or its conjugate (inverse);
+// j is a compile-time constant after unrolling.
+template <bool INV, class C>
+__device__ __forceinline__ C twc32(C v, int j) {
+  j &= 31;
+  if (j == 0) return v;
+  if (j == 16) { v.x = -v.x; v.y = -v.y; return v; }
+  if (j == 8) return mul_mi<INV>(v);
+  if (j == 24) return mul_mi<!INV>(v);
+  const double c = cospi16(j), s = cospi16(8 - j);   // cos, sin of 2 pi j / 32
+  C r;
+  if ((j & 7) == 4) {   // |c| = |s| = sqrt(1/2): one product per component
+    const double h = 0.70710678118654752440084436210485;
+    const auto cx = c > 0. ? v.x : -v.x, cy = c > 0. ? v.y : -v.y;   // v c / h
+    const auto sx = s > 0. ? v.x : -v.x, sy = s > 0. ? v.y : -v.y;   // v s / h
+    if (INV) { r.x = mulk(cx - sy, h); r.y = mulk(sx + cy, h); }
+    else     { r.x = mulk(cx + sy, h); r.y = mulk(cy - sx, h); }
+    return r;
+  }
+  if (INV) { r.x = mulk2(v.x, c, v.y, -s); r.y = mulk2(v.x, s, v.y, c); }
+  else     { r.x = mulk2(v.x, c, v.y, s);  r.y = mulk2(v.y, c, v.x, -s); }
+  return r;
+}
+
+// 8-point DFT (radix-2 over two 4-point DFTs), constants through twc32.
+template <bool INV, class C> __device__ __forceinline__ void dft8c(C* v) {
+  C a[4], b[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) { a[k] = cadd(v[k], v[k + 4]); b[k] = csub(v[k], v[k + 4]); }
+  b[1] = twc32<INV>(b[1], 4);
+  b[2] = mul_mi<INV>(b[2]);
+  b[3] = twc32<INV>(b[3], 12);
+  dft4<INV>(a[0], a[1], a[2], a[3]);
+  dft4<INV>(b[0], b[1], b[2], b[3]);
+#pragma unroll
+  for (int m = 0; m < 4; ++m) { v[2 * m] = a[m]; v[2 * m + 1] = b[m]; }
+}
+
+// 16-point DFT as 4 x 4 (n = 4 a + b): radix-4 over a, twiddles W_16^{b k1},
+// radix-4 over b.  Natural order in and out.
+template <bool INV, class C> __device__ __forceinline__ void dft16(C* v) {
+  C t[16];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    C a0 = v[b], a1 = v[b + 4], a2 = v[b + 8], a3 = v[b + 12];
+    dft4<INV>(a0, a1, a2, a3);
+    t[b] = a0; t[b + 4] = a1; t[b + 8] = a2; t[b + 12] = a3;   // t[4 k1 + b]
+  }
+#pragma unroll
+  for (int k1 = 1; k1 < 4; ++k1)
+#pragma unroll
+    for (int b = 1; b < 4; ++b) t[4 * k1 + b] = twc32<INV>(t[4 * k1 + b], 2 * b * k1);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    C a0 = t[4 * k1], a1 = t[4 * k1 + 1], a2 = t[4 * k1 + 2], a3 = t[4 * k1 + 3];
+    dft4<INV>(a0, a1, a2, a3);
+    v[k1] = a0; v[k1 + 4] = a1; v[k1 + 8] = a2; v[k1 + 12] = a3;   // X[k1 + 4 k2]
+  }
+}
+
+// 32-point DFT: radix-2 decimation in time over two 16-point DFTs.
+template <bool INV, class C> __device__ __forceinline__ void dft32(C* v) {
+  C e[16], o[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) { e[k] = v[2 * k]; o[k] = v[2 * k + 1]; }
+  dft16<INV>(e);
+  dft16<INV>(o);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const C t = twc32<INV>(o[k], k);
+    v[k] = cadd(e[k], t);
+    v[k + 16] = csub(e[k], t);
+  }
+}
+
+template <int R, bool INV, class C> __device__ __forceinline__ void dft_r(C* v) {
+  if constexpr (R == 32) dft32<INV>(v);
+  else if constexpr (R == 16) dft16<INV>(v);
+  else if constexpr (R == 8) dft8c<INV>(v);
+  else if constexpr (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+  else if constexpr (R == 2) dft2<INV>(v[0], v[1]);
+}
+
 template <int R, bool INV, class C> __device__ __forceinline__ void dft(C* v) {
-  if (R == 2) dft2<INV>(v[0], v[1]);
-  else if (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
-  else dft8<INV>(v);
+  if constexpr (R == 2) dft2<INV>(v[0], v[1]);
+  else if constexpr (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+  else if constexpr (R == 8) dft8<INV>(v);
+  else dft16<INV>(v);
 }
 
 // ---------------------------------------------------------------- layouts
@@ -102,17 +226,20 @@ template <int NB> struct ColMap {
   template <int NBF> __device__ __forceinline__ static void split(int q, int& b, int& j) { b = q % NB; j = q / NB; }
 };
 
-template <int N, int NS> struct Radix {
+// Largest radix <= MAXR that fits the remaining length.  MAXR = 16 takes fewer
+// shared-memory round trips (256 = 16 16, 1024 = 16 16 4) but needs about twice the
+// registers of MAXR = 8, so it is a per-call-site choice.
+template <int N, int NS, int MAXR = 8> struct Radix {
   static constexpr int rem = N / NS;
-  static constexpr int value = rem >= 8 ? 8 : (rem >= 4 ? 4 : 2);
+  static constexpr int value = (MAXR >= 16 && rem >= 16) ? 16 : (rem >= 8 ? 8 : (rem >= 4 ? 4 : 2));
 };
 
 // One Stockham stage over all NB sequences.  Phase 1 reads each butterfly's R
 // inputs from shared memory and its R-1 twiddles from the (L1-resident) table,
 // so the twiddle latency overlaps the barrier; phase 2 computes and writes.
-template <class C, int N, int NS, int NB, int NT, bool INV, class Map>
+template <class C, int N, int NS, int NB, int NT, bool INV, class Map, int MAXR = 8>
 __device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
-  constexpr int R = Radix<N, NS>::value;
+  constexpr int R = Radix<N, NS, MAXR>::value;
   constexpr int NBF = N / R;                 // butterflies per sequence
   constexpr int TOT = NB * NBF;              // butterflies per stage
   constexpr int PER = (TOT + NT - 1) / NT;   // per thread
@@ -156,21 +283,21 @@ __device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
   __syncthreads();
 }
 
-template <class C, int N, int NS, int NB, int NT, bool INV, class Map> struct FftRun {
+template <class C, int N, int NS, int NB, int NT, bool INV, class Map, int MAXR> struct FftRun {
   __device__ __forceinline__ static void run(C* s, const C* __restrict__ tw) {
-    fft_stage<C, N, NS, NB, NT, INV, Map>(s, tw);
-    FftRun<C, N, NS * Radix<N, NS>::value, NB, NT, INV, Map>::run(s, tw);
+    fft_stage<C, N, NS, NB, NT, INV, Map, MAXR>(s, tw);
+    FftRun<C, N, NS * Radix<N, NS, MAXR>::value, NB, NT, INV, Map, MAXR>::run(s, tw);
   }
 };
-template <class C, int N, int NB, int NT, bool INV, class Map> struct FftRun<C, N, N, NB, NT, INV, Map> {
+template <class C, int N, int NB, int NT, bool INV, class Map, int MAXR> struct FftRun<C, N, N, NB, NT, INV, Map, MAXR> {
   __device__ __forceinline__ static void run(C*, const C* __restrict__) {}
 };
 
 // Batched FFT of NB sequences of length N in shared memory (caller has
 // synchronised before; the CTA is synchronised on return).
-template <class C, int N, int NB, int NT, bool INV, class Map>
+template <class C, int N, int NB, int NT, bool INV, class Map, int MAXR = 8>
 __device__ __forceinline__ void cta_fft(C* s, const C* __restrict__ tw) {
-  FftRun<C, N, 1, NB, NT, INV, Map>::run(s, tw);
+  FftRun<C, N, 1, NB, NT, INV, Map, MAXR>::run(s, tw);
 }
 
 }  // namespace wig

@@ -23,6 +23,14 @@
 #pragma once
 #include "wig_fft.cuh"
 
+// largest Stockham radix of the complex128 x-pass / p-pass transforms (the JIT sets them)
+#ifndef WIG_XR
+#define WIG_XR 8
+#endif
+#ifndef WIG_PR
+#define WIG_PR 8
+#endif
+
 namespace wig {
 
 constexpr int NACC = 12;   // sumRe, sumIm, x, x^2, p, p^2, xp, V', pV', xV', H, negative
@@ -202,7 +210,7 @@ __device__ __forceinline__ void xpass_body(const WigArgs& a, const Phys& ph, dou
     sm[M::idx(r, k)] = v;
   }
   __syncthreads();
-  cta_fft<double2, NX, ROWS, NT, false, M>(sm, a.tw_x);
+  cta_fft<double2, NX, ROWS, NT, false, M, WIG_XR>(sm, a.tw_x);
   const double inv_n = 1.0 / (double)NX;
   for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
     const int r = e / NX, k = e - r * NX;
@@ -223,7 +231,7 @@ __device__ __forceinline__ void xpass_body(const WigArgs& a, const Phys& ph, dou
     sm[id] = cmul(sm[id], make_double2(rr * cs, -rr * sn));
   }
   __syncthreads();
-  cta_fft<double2, NX, ROWS, NT, true, M>(sm, a.tw_x);
+  cta_fft<double2, NX, ROWS, NT, true, M, WIG_XR>(sm, a.tw_x);
   for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
     const int r = e / NX, k = e - r * NX;
     Wb[e] = sm[M::idx(r, k)];
@@ -237,10 +245,10 @@ __device__ __forceinline__ void cl_apply_D(const WigArgs& a, double2* B, const d
   typedef ColMap<C> M;
   for (int e = threadIdx.x; e < C * NP; e += NT) B[pad8(e)] = cscale(B[pad8(e)], sfp[e / C]);
   __syncthreads();
-  cta_fft<double2, NP, C, NT, false, M>(B, a.tw_p);
+  cta_fft<double2, NP, C, NT, false, M, WIG_PR>(B, a.tw_p);
   for (int e = threadIdx.x; e < C * NP; e += NT) B[pad8(e)] = cscale(B[pad8(e)], ths[e / C]);
   __syncthreads();
-  cta_fft<double2, NP, C, NT, true, M>(B, a.tw_p);
+  cta_fft<double2, NP, C, NT, true, M, WIG_PR>(B, a.tw_p);
 }
 
 // p-pass: a tile of C columns x NP rows per CTA.  DAMP: 0 none, 1 Caldeira-Leggett.
@@ -283,7 +291,7 @@ __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, dou
     A[pad8(e)] = v;
   }
   __syncthreads();
-  cta_fft<double2, NP, C, NT, false, M>(A, a.tw_p);
+  cta_fft<double2, NP, C, NT, false, M, WIG_PR>(A, a.tw_p);
   for (int e = threadIdx.x; e < C * NP; e += NT) {
     const int k = e / C, c = e - k * C;
     const int col = col0 + c;
@@ -308,7 +316,7 @@ __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, dou
     A[pad8(e)] = v;
   }
   __syncthreads();
-  cta_fft<double2, NP, C, NT, true, M>(A, a.tw_p);
+  cta_fft<double2, NP, C, NT, true, M, WIG_PR>(A, a.tw_p);
   if (!FINAL) {
     for (int e = threadIdx.x; e < C * NP; e += NT) {
       const int k = e / C, c = e - k * C;
