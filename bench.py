@@ -534,6 +534,7 @@ def run_batch(args, world, rank, local):
         'drift_vs_fp64': {'steps': nval, 'norm_max_abs': norm_err, 'energy_max_abs': energy_err,
                           'energy_max_rel_to_H_range': energy_err_h,
                           'reference': 'complex128 drop-in path, exact constants, same instances'},
+        'flops': batch_flops(cases_all, world, ms / K, clk.summary()),
         'roofline': {'bound': 'hbm', 'kernel': dom, 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                      'frac': achieved / peak, 'peak_kind': peak_kind, 'algorithmic_bytes_per_launch': pass_bytes,
                      'avg_launch_us': dom_ms / nl * 1e3, 'x_pass_us': x_ms / nl * 1e3, 'p_pass_us': p_ms / nl * 1e3,
@@ -552,6 +553,26 @@ def run_batch(args, world, rank, local):
                                 'sample': what + ' (%.1f s)' % el}
     if rank == 0:
         print(json.dumps(line))
+
+
+def batch_flops(cases, world, ms_step, clocks):
+    """Algorithmic FP32 flops of one batched step: 5 N log2 N per length-N transform, N transforms
+    per axis pass; 2 in the x-pass, 2 for the potential and 6 for Caldeira-Leggett order 3 (when
+    damped) in the p-pass.  Against the nominal FP32 rate of the SM clock seen under load
+    (148 SMs x 128 lanes x 2 flops per FMA); no measured FP32 peak exists for this pool."""
+    import math
+    total = 0.
+    for c in cases:
+        n = c['n']
+        ffts = 2 + 2 + (6 if c['gamma'] != 0. else 0)
+        total += ffts * 5. * n * n * math.log2(n)
+    per_rank = total / world
+    mhz = (clocks or {}).get('sm_mhz') or 1965.
+    nominal = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    achieved = per_rank / (ms_step / 1e3) / 1e12
+    return {'algorithmic_per_step': total, 'achieved_tflops': achieved, 'fp32_nominal_tflops': nominal,
+            'frac_of_nominal': achieved / nominal, 'counted': '5 N log2 N per transform; 10 transforms per '
+            'point per damped step'}
 
 
 def make_dirac_instance(time_steps):
