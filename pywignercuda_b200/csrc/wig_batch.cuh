@@ -62,7 +62,11 @@ struct BArgs {
 // p-pass tile and its Caldeira-Leggett copy A.  The twiddle and factor tables
 // are read through the read-only data path (a few KB per size, L1-resident).
 __host__ __device__ constexpr int bx_smem(int n, int warps) { return warps * rf_spw(n) * (n + (rf_g(n) == 8 ? 8 : 0)); }
-__host__ __device__ constexpr int bp_smem(int n, int warps) { return 2 * warps * rf_spw(n) * n; }
+// The p-pass packs two real columns into one complex sequence for the
+// Caldeira-Leggett part (see batch_p_item): an item is BP_PACK column groups.
+constexpr int BP_PACK = 2;
+__host__ __device__ constexpr int bp_cols(int n, int warps) { return BP_PACK * warps * rf_spw(n); }
+__host__ __device__ constexpr int bp_smem(int n, int warps) { return BP_PACK * warps * rf_spw(n) * n; }
 
 // p-pass: column of the CT-wide tile owned by group `grp` of warp `warp`.
 // With 8-lane groups two sequences share a half-warp; pairing columns c and
@@ -223,72 +227,99 @@ __device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BIn
 }
 
 // ------------------------------------------------------------------ p-pass
-// Item: a tile of CT = WIGB_WARPS * rf_spw(N) columns x N rows, staged in
-// shared memory (element (k, c) at k CT + (c ^ sw(k))) so that the global
-// loads and stores are row segments; each group then owns one column.
+// Item: a tile of CT2 = BP_PACK * WIGB_WARPS * rf_spw(N) columns x N rows, staged
+// in shared memory (element (k, c) at k CT2 + (c ^ sw(k))) so that the global
+// loads and stores are row segments.  Each lane group owns two columns, c1 and
+// c2 = c1 + CT2 / 2:
+//   it = 0, 1:  w = IFFT[Moyal FFT(w)] for c1, then c2 (the Moyal factor
+//               depends on x, so each column takes its own transform pair);
+//   it = 2..4 (damped): Caldeira-Leggett on the pair packed into one complex
+//               sequence z = Re W(c1) + i Re W(c2).  The dissipator polynomial
+//               z -> A + i c D(z), D(z) = IFFT[theta/N FFT(sign(p) f(p) z)], is
+//               complex-linear and the same for every column, so it acts on the
+//               two real columns at once, and the results are Re z, Im z.
+// A damped step therefore costs 5 transform pairs per 2 columns instead of 8.
+// W is real (the Wigner function); the imaginary rounding noise the Moyal and
+// kinetic steps leave (~1e-8 in FP32) is dropped by the packing, so damped
+// columns leave the pass real.
 template <int N>
 __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BInst& I, int col0, int item,
                                              int sample) {
   typedef RegFft<float2, N> F;
-  constexpr int E = F::E, G = F::G, Q = F::Q, SPW = rf_spw(N), CT = WIGB_WARPS * SPW, NT = WIGB_NT;
+  constexpr int E = F::E, G = F::G, Q = F::Q, SPW = rf_spw(N), CT = WIGB_WARPS * SPW, CT2 = BP_PACK * CT;
+  constexpr int NT = WIGB_NT;
+  static_assert(BP_PACK == 2, "two columns per lane group");
   extern __shared__ float2 smb[];
   const float2* tf = A.tw + I.tw_p;
   const float2* ti = tf + N;
   const float* rth = A.ft + I.ft_p;   // exp(-D_theta theta^2 dt)
   const float* sfp = rth + N;         // sign(p) f(p)
   const float* ths = sfp + N;         // theta / N
-  float2* tile = smb;
-  float2* atile = tile + CT * N;      // A (post-Moyal column), same slot map
+  float2* tile = smb;                 // after packing, c1's slots hold A (the packed post-Moyal pair)
   const int nx = I.n_x;
   float2* Wi = A.W + I.off;
-  // coalesced tile load: all of the thread's loads issued before their
-  // shared-memory stores (one latency per item instead of one per element)
-  constexpr int PER = CT * N / NT, LB = PER;   // every load of the thread in flight
-  static_assert(PER * NT == CT * N && PER % LB == 0, "tile load shape");
+  // coalesced tile load, one register batch per column group (loads in flight
+  // before their shared-memory stores)
+  constexpr int PER = CT2 * N / NT, LB = PER / BP_PACK;
+  static_assert(PER * NT == CT2 * N && PER % LB == 0, "tile load shape");
 #pragma unroll 1
   for (int r0 = 0; r0 < PER; r0 += LB) {
     float2 buf[LB];
 #pragma unroll
     for (int r = 0; r < LB; ++r) {
       const int e = threadIdx.x + (r0 + r) * NT;
-      buf[r] = Wi[(size_t)(e / CT) * nx + col0 + (e & (CT - 1))];
+      buf[r] = Wi[(size_t)(e / CT2) * nx + col0 + (e & (CT2 - 1))];
     }
 #pragma unroll
     for (int r = 0; r < LB; ++r) {
-      const int e = threadIdx.x + (r0 + r) * NT, k = e / CT;
-      tile[k * CT + ((e & (CT - 1)) ^ tile_sw<CT>(k))] = buf[r];
+      const int e = threadIdx.x + (r0 + r) * NT, k = e / CT2;
+      tile[k * CT2 + ((e & (CT2 - 1)) ^ tile_sw<CT2>(k))] = buf[r];
     }
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
-  const int c = rf_col<N>(warp, grp);
-  const TileSlot<CT> sl{c};
+  const int c1 = rf_col<N>(warp, grp), c2 = c1 + CT;
+  const TileSlot<CT2> sl1{c1}, sl2{c2};
   float2 w[E];
 #pragma unroll
-  for (int m = 0; m < E; ++m) w[m] = tile[sl(g + G * m)];
+  for (int m = 0; m < E; ++m) w[m] = tile[sl1(g + G * m)];
   // Moyal factor exp(-i dt [V(x - u) - V(x + u)] / hbar) r_theta mask1 mask2 / N,
   // u = hbar theta / 2 = h j:  V(x - u) - V(x + u) = -2u (a3 + a1 u^2); phase in turns
-  const int col = col0 + c;
-  const double x = I.dx * (double)shifted(col, nx);
   const double h = 0.5 * I.hbar * I.dtheta;
   const double kk = -I.dt * h / (3.141592653589793238 * I.hbar);
-  const double al = kk * ((4. * I.v4 * x * x + 2. * I.v2) * x + I.v1);
-  const double be = kk * h * h * (4. * I.v4 * x);
-  const float mm = __ldg(A.ft + I.ft_x + nx + col);
+  const bool damped = I.damp == 1;
+  const int n_it = damped ? 5 : 2;
   // One transform pair per pass through this loop (kept rolled so the kernel
-  // holds a single copy of each FFT):
-  //   it = 0:  w = IFFT[Moyal FFT(w)]                       -> A = w (kept in atile)
-  //   it = 1..3 (Caldeira-Leggett, Horner form):
-  //            w = A + coef_it D(w),  D(w) = IFFT[theta/N FFT(sign(p) f(p) w)]
-  const int n_it = I.damp == 1 ? 4 : 1;
+  // holds a single copy of each FFT).
 #pragma unroll 1
   for (int it = 0; it < n_it; ++it) {
-    if (it > 0) {
+    const TileSlot<CT2> sl{it == 0 ? c1 : c2};    // exchange slots: the column in flight
+    __syncwarp();   // the previous transform's exchange reads are done before these slots change
+    if (it == 1) {
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        tile[sl1(g + G * m)] = w[m];               // c1 done with its Moyal step
+        w[m] = tile[sl2(g + G * m)];
+      }
+    } else if (it == 2) {
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        w[m] = make_float2(tile[sl1(g + G * m)].x, w[m].x);   // z = Re W(c1) + i Re W(c2)
+        tile[sl1(g + G * m)] = w[m];                          // A, in the slots c1 no longer needs
+      }
+    }
+    if (it >= 2) {
 #pragma unroll
       for (int m = 0; m < E; ++m) w[m] = cscale(w[m], __ldg(sfp + g + G * m));
     }
     F::fwd(w, tile, sl, tf, g);
-    if (it == 0) {
+    if (it < 2) {
+      __syncwarp();   // exchange reads done before the factor writes reuse the slots
+      const int col = col0 + (it == 0 ? c1 : c2);
+      const double x = I.dx * (double)shifted(col, nx);
+      const double al = kk * ((4. * I.v4 * x * x + 2. * I.v2) * x + I.v1);
+      const double be = kk * h * h * (4. * I.v4 * x);
+      const float mm = __ldg(A.ft + I.ft_x + nx + col);
       // Moyal factors through the column's (free) tile slots, as in the x-pass
 #pragma unroll 2
       for (int e = 0; e < E; ++e) {
@@ -306,72 +337,82 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
         for (int b = 0; b < G; ++b) w[i * G + b] = cscale(w[i * G + b], __ldg(ths + g * Q + i + E * b));
     }
     F::inv(w, tile, sl, ti, g);
-    if (it == 0) {
-      if (n_it > 1) {
-#pragma unroll
-        for (int m = 0; m < E; ++m) atile[sl(g + G * m)] = w[m];
-      }
-    } else {
-      const float cf = (float)(it == 1 ? I.cl_k1 : (it == 2 ? I.cl_k12 : I.cl_c3));
+    if (it >= 2) {
+      const float cf = (float)(it == 2 ? I.cl_k1 : (it == 3 ? I.cl_k12 : I.cl_c3));
 #pragma unroll
       for (int m = 0; m < E; ++m) {
-        const float2 a = atile[sl(g + G * m)];
+        const float2 a = tile[sl1(g + G * m)];
         w[m] = make_float2(a.x - cf * w[m].y, a.y + cf * w[m].x);
       }
     }
   }
-  // observables: column moments sum W, sum W p_j, sum W p_j^2 (FP64), Im and
+  // the two columns' values: damped -> (Re z, 0), (Im z, 0); undamped -> tile c1, w
+  __syncwarp();
+  if (damped) {
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      tile[sl1(g + G * m)] = make_float2(w[m].x, 0.f);
+      w[m] = make_float2(w[m].y, 0.f);
+    }
+  }
+  __syncwarp();
+  // observables: per column, moments sum W, sum W p_j, sum W p_j^2 (FP64), Im and
   // the negative part (FP32 per lane), reduced over the group's lanes
-  double s0 = 0., s1 = 0., s2 = 0.;
-  float si = 0.f, sn = 0.f;
-#pragma unroll
-  for (int m = 0; m < E; ++m) {
-    const double wr = (double)w[m].x;
-    const double pj = (double)(g + G * m - (m >= E / 2 ? N : 0));
-    s0 += wr;
-    const double wp = wr * pj;
-    s1 += wp;
-    s2 = fma(wp, pj, s2);
-    si += w[m].y;
-    sn += fminf(w[m].x, 0.f);
-  }
-  double sid = (double)si, snd = (double)sn;
-#pragma unroll
-  for (int o = G / 2; o > 0; o >>= 1) {
-    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    sid += __shfl_xor_sync(0xffffffffu, sid, o);
-    snd += __shfl_xor_sync(0xffffffffu, snd, o);
-  }
   double acc[NACC];
 #pragma unroll
   for (int v = 0; v < NACC; ++v) acc[v] = 0.;
-  if (g == 0) {
-    const double dV = (4. * I.v4 * x * x + 2. * I.v2) * x + I.v1;
-    const double V = ((I.v4 * x * x + I.v2) * x + I.v1) * x + I.v0;
-    const double M1 = s1 * I.dp, M2 = s2 * (I.dp * I.dp);
-    acc[0] = s0;
-    acc[1] = sid;
-    acc[2] = s0 * x;
-    acc[3] = s0 * x * x;
-    acc[4] = M1;
-    acc[5] = M2;
-    acc[6] = M1 * x;
-    acc[7] = s0 * dV;
-    acc[8] = M1 * dV;
-    acc[9] = s0 * x * dV;
-    acc[10] = M2 / (2. * I.mass) + s0 * V;
-    acc[11] = snd;
+#pragma unroll 1
+  for (int q = 0; q < 2; ++q) {
+    double s0 = 0., s1 = 0., s2 = 0.;
+    float si = 0.f, sn = 0.f;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const float2 v = q == 0 ? tile[sl1(g + G * m)] : w[m];
+      const double wr = (double)v.x;
+      const double pj = (double)(g + G * m - (m >= E / 2 ? N : 0));
+      s0 += wr;
+      const double wp = wr * pj;
+      s1 += wp;
+      s2 = fma(wp, pj, s2);
+      si += v.y;
+      sn += fminf(v.x, 0.f);
+    }
+    double sid = (double)si, snd = (double)sn;
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      sid += __shfl_xor_sync(0xffffffffu, sid, o);
+      snd += __shfl_xor_sync(0xffffffffu, snd, o);
+    }
+    if (g == 0) {
+      const double x = I.dx * (double)shifted(col0 + (q == 0 ? c1 : c2), nx);
+      const double dV = (4. * I.v4 * x * x + 2. * I.v2) * x + I.v1;
+      const double V = ((I.v4 * x * x + I.v2) * x + I.v1) * x + I.v0;
+      const double M1 = s1 * I.dp, M2 = s2 * (I.dp * I.dp);
+      acc[0] += s0;
+      acc[1] += sid;
+      acc[2] += s0 * x;
+      acc[3] += s0 * x * x;
+      acc[4] += M1;
+      acc[5] += M2;
+      acc[6] += M1 * x;
+      acc[7] += s0 * dV;
+      acc[8] += M1 * dV;
+      acc[9] += s0 * x * dV;
+      acc[10] += M2 / (2. * I.mass) + s0 * V;
+      acc[11] += snd;
+    }
   }
   __syncwarp();
 #pragma unroll
-  for (int m = 0; m < E; ++m) tile[sl(g + G * m)] = w[m];
+  for (int m = 0; m < E; ++m) tile[sl2(g + G * m)] = w[m];
   __syncthreads();
 #pragma unroll 8
   for (int r = 0; r < PER; ++r) {
-    const int e = threadIdx.x + r * NT, k = e / CT, cc = e & (CT - 1);
-    Wi[(size_t)k * nx + col0 + cc] = tile[k * CT + (cc ^ tile_sw<CT>(k))];
+    const int e = threadIdx.x + r * NT, k = e / CT2, cc = e & (CT2 - 1);
+    Wi[(size_t)k * nx + col0 + cc] = tile[k * CT2 + (cc ^ tile_sw<CT2>(k))];
   }
   batch_item_done<NT>(A, inst, I, item, acc, I.damp ? 1 : 0, sample);
 }
@@ -380,7 +421,7 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
 template <int N>
 __device__ __forceinline__ void batch_reduce_item(const BArgs& A, int inst, const BInst& I, int col0, int item,
                                                   int mode, int sample) {
-  constexpr int CPB = WIGB_WARPS * rf_spw(N);
+  constexpr int CPB = bp_cols(N, WIGB_WARPS);
   constexpr int NT = WIGB_NT;
   const int nx = I.n_x;
   const float2* Wi = A.W + I.off;
@@ -398,7 +439,7 @@ __device__ __forceinline__ void batch_reduce_item(const BArgs& A, int inst, cons
 
 template <int N>
 __device__ __forceinline__ void batch_scale_item(const BArgs& A, int inst, const BInst& I, int col0) {
-  constexpr int CPB = WIGB_WARPS * rf_spw(N);
+  constexpr int CPB = bp_cols(N, WIGB_WARPS);
   constexpr int NT = WIGB_NT;
   const double2 sd = A.scale[inst];
   const float2 sc = make_float2((float)sd.x, (float)sd.y);

@@ -195,7 +195,9 @@ int copy_log(const std::string& log, char* out, int64_t cap) {
 int get_fn(CUmodule mod, const char* name, CUfunction* f, int dyn_smem) {
   CUresult r = g_drv.getf(f, mod, name);
   if (r != CUDA_SUCCESS) return fail(WIG_ERR_CUDA, "cuModuleGetFunction(%s): %s", name, cu_err(r));
-  if (dyn_smem > 48 * 1024) {
+  // always raise the dynamic ceiling to the request: static shared memory counts against the
+  // default 48 KB too, so a request just at 48 KB already needs the attribute
+  if (dyn_smem > 0) {
     r = g_drv.setattr(*f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, dyn_smem);
     if (r != CUDA_SUCCESS) return fail(WIG_ERR_CUDA, "cuFuncSetAttribute(%s): %s", name, cu_err(r));
   }
@@ -1449,7 +1451,7 @@ static int wigb_compile(wigb_handle* h, int warps, BVariant* v) {
 }
 
 // Work lists for a tile of `warps` warps: x-items of warps*rf_spw(n_x) rows,
-// p-items of warps*rf_spw(n_p) columns; p-items of each instance contiguous
+// p-items of bp_cols(n_p, warps) columns; p-items of each instance contiguous
 // (the last-CTA reduction reads them as a range), instances ordered by
 // decreasing per-item cost so the persistent loop ends balanced.
 static int wigb_set_warps(wigb_handle* h, int warps) {
@@ -1468,7 +1470,7 @@ static int wigb_set_warps(wigb_handle* h, int warps) {
   std::vector<int2> xi, pi;
   for (int i : order) {
     wig::BInst& b = h->binst[i];
-    const int rpb = warps * wig::rf_spw(b.n_x), cpb = warps * wig::rf_spw(b.n_p);
+    const int rpb = warps * wig::rf_spw(b.n_x), cpb = wig::bp_cols(b.n_p, warps);
     if (b.n_p % rpb || b.n_x % cpb)
       return fail(WIG_ERR_ARG, "instance %d: grid %d x %d does not tile with %d warps", i, b.n_x, b.n_p, warps);
     b.xitem0 = (int)xi.size();
