@@ -61,7 +61,10 @@ struct BArgs {
 // Shared memory of one item (float2 units): the x-pass exchange regions; the
 // p-pass tile and its Caldeira-Leggett copy A.  The twiddle and factor tables
 // are read through the read-only data path (a few KB per size, L1-resident).
-__host__ __device__ constexpr int bx_smem(int n, int warps) { return warps * rf_spw(n) * (n + (rf_g(n) == 8 ? 8 : 0)); }
+// x-pass: each lane group carries two rows packed into one complex sequence and
+// holds, per row pair, the transform exchange / spectrum region and a factor region.
+__host__ __device__ constexpr int bx_rows(int n, int warps) { return 2 * warps * rf_spw(n); }
+__host__ __device__ constexpr int bx_smem(int n, int warps) { return 2 * warps * rf_spw(n) * (n + (rf_g(n) == 8 ? 8 : 0)); }
 // The p-pass packs two real columns into one complex sequence for the
 // Caldeira-Leggett part (see batch_p_item): an item is BP_PACK column groups.
 constexpr int BP_PACK = 2;
@@ -184,8 +187,15 @@ __device__ __forceinline__ int next_item(unsigned* ticket, int n_items) {
 }
 
 // ------------------------------------------------------------------ x-pass
-// Item: WIGB_WARPS * rf_spw(N) consecutive rows; lane g of group `grp` holds
-// elements g + G m of its row.
+// Item: bx_rows(N) consecutive rows; lane group `pair` carries rows ra = row0 +
+// 2 pair and rb = ra + 1 packed into z = Re W(ra) + i Re W(rb) (W is real), lane
+// g holding elements g + G m.  The kinetic factor differs between the two rows,
+// so the spectrum is split with its mirror: for real rows a, b with z = a + i b,
+//   Z'(k) = [Z(k) (fa + fb) + conj Z(N - k) (fa - fb)] / 2
+// is the spectrum of a' + i b', a' = IFFT[fa FFT a], b' = IFFT[fb FFT b]
+// (fa, fb map Hermitian spectra to Hermitian spectra).  Rows ra, rb differ by
+// one p step, so fb = fa g(lambda) with g = exp(-i dt dp lambda / m), a table.
+// One transform pair per two rows.
 template <int N>
 __device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BInst& I, int row0) {
   typedef RegFft<float2, N> F;
@@ -194,36 +204,54 @@ __device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BIn
   extern __shared__ float2 smb[];
   const float2* tf = A.tw + I.tw_x;
   const float2* ti = tf + N;
-  const float* rtab = A.ft + I.ft_x;   // exp(-D_lambda lambda^2) / N
+  const float* rtab = A.ft + I.ft_x;            // exp(-D_lambda lambda^2) / N
+  const float* gtab = rtab + 2 * N;             // exp(-i dt dp lambda / m): (cos, -sin) pairs
   float2* X = smb;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
-  const int row = row0 + warp * SPW + grp;
+  const int pair = warp * SPW + grp;
+  const int ra = row0 + 2 * pair;
   const double2 sd = A.scale[inst];
   const float2 sc = make_float2((float)sd.x, (float)sd.y);
-  float2* Wr = A.W + I.off + (size_t)row * N;
+  float2* Wa = A.W + I.off + (size_t)ra * N;
+  float2* Wb = Wa + N;
   float2 v[E];
 #pragma unroll
-  for (int m = 0; m < E; ++m) v[m] = cmul(Wr[g + G * m], sc);
-  const PlainSlot sl{(warp * SPW + grp) * XS};
+  for (int m = 0; m < E; ++m) {
+    const float2 a = Wa[g + G * m], b = Wb[g + G * m];
+    v[m] = make_float2(a.x * sc.x - a.y * sc.y, b.x * sc.x - b.y * sc.y);   // Re(W s) of each row
+  }
+  const PlainSlot sl{pair * 2 * XS};            // exchange, then the spectrum in natural order
+  const PlainSlot sf{pair * 2 * XS + XS};       // row a's kinetic factors
   F::fwd(v, X, sl, tf, g);
-  // kinetic factor exp(-i dt lambda p / m) r_lambda(lambda) / N, in turns.  The
-  // factors are evaluated in a rolled loop into the lane's exchange slots (free
-  // between the two transforms) and then applied: one copy of the FP64
-  // reduction + sincospif per kernel instead of E (instruction-cache footprint).
-  const double cq = I.dt * I.dp * I.dlambda * (double)shifted(row, I.n_p) / (I.mass * 6.283185307179586477);
+  __syncwarp();   // the transform's exchange reads are done before the spectrum is staged
+#pragma unroll
+  for (int e = 0; e < E; ++e) X[sl(g * Q + e / G + E * (e % G))] = v[e];
+  // kinetic factor of row a, exp(-i dt lambda p / m), in turns (rolled: one copy of the
+  // FP64 reduction + sincospif per kernel)
+  const double cq = I.dt * I.dp * I.dlambda * (double)shifted(ra, I.n_p) / (I.mass * 6.283185307179586477);
 #pragma unroll 2
   for (int e = 0; e < E; ++e) {
     const int i = e / G, b = e % G;
     const int k = g * Q + i + E * b;
     const int lj = b < G / 2 ? k : k - N;
-    X[sl(e * G + g)] = turn_factor(cq * (double)lj, 1.f);
+    X[sf(e * G + g)] = turn_factor(cq * (double)lj, 1.f);
   }
+  __syncwarp();
 #pragma unroll
-  for (int e = 0; e < E; ++e)
-    v[e] = cscale(cmul(v[e], X[sl(e * G + g)]), __ldg(rtab + g * Q + e / G + E * (e % G)));
+  for (int e = 0; e < E; ++e) {
+    const int k = g * Q + e / G + E * (e % G);
+    const float2 P = X[sl((N - k) & (N - 1))];
+    const float2 fa = X[sf(e * G + g)];
+    const float2 fb = cmul(fa, make_float2(__ldg(gtab + 2 * k), __ldg(gtab + 2 * k + 1)));
+    const float r = 0.5f * __ldg(rtab + k);
+    v[e] = cscale(cadd(cmul(v[e], cadd(fa, fb)), cmul(cconj(P), csub(fa, fb))), r);
+  }
   F::inv(v, X, sl, ti, g);
 #pragma unroll
-  for (int m = 0; m < E; ++m) Wr[g + G * m] = v[m];
+  for (int m = 0; m < E; ++m) {
+    Wa[g + G * m] = make_float2(v[m].x, 0.f);
+    Wb[g + G * m] = make_float2(v[m].y, 0.f);
+  }
 }
 
 // ------------------------------------------------------------------ p-pass

@@ -1450,7 +1450,7 @@ static int wigb_compile(wigb_handle* h, int warps, BVariant* v) {
   return WIG_OK;
 }
 
-// Work lists for a tile of `warps` warps: x-items of warps*rf_spw(n_x) rows,
+// Work lists for a tile of `warps` warps: x-items of bx_rows(n_x, warps) rows,
 // p-items of bp_cols(n_p, warps) columns; p-items of each instance contiguous
 // (the last-CTA reduction reads them as a range), instances ordered by
 // decreasing per-item cost so the persistent loop ends balanced.
@@ -1470,7 +1470,7 @@ static int wigb_set_warps(wigb_handle* h, int warps) {
   std::vector<int2> xi, pi;
   for (int i : order) {
     wig::BInst& b = h->binst[i];
-    const int rpb = warps * wig::rf_spw(b.n_x), cpb = wig::bp_cols(b.n_p, warps);
+    const int rpb = wig::bx_rows(b.n_x, warps), cpb = wig::bp_cols(b.n_p, warps);
     if (b.n_p % rpb || b.n_x % cpb)
       return fail(WIG_ERR_ARG, "instance %d: grid %d x %d does not tile with %d warps", i, b.n_x, b.n_p, warps);
     b.xitem0 = (int)xi.size();
@@ -1586,6 +1586,15 @@ extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t war
       const double w2 = (10. * b.dx) * (10. * b.dx);
       const double m1 = 1. - exp(-(x - x_max) * (x - x_max) / w2), m2 = 1. - exp(-(x + x_max) * (x + x_max) / w2);
       ft.push_back((float)(m1 * m2 / (double)d.n_p));
+    }
+    // exp(-i dt dp lambda / m) per x-frequency: the kinetic factor of row p + dp over that of
+    // row p (the x-pass carries rows 2r and 2r + 1 together), as (cos, -sin) of the turn
+    for (int k = 0; k < d.n_x; ++k) {
+      const int lj = k < d.n_x / 2 ? k : k - d.n_x;
+      double t = b.dt * b.dp * b.dlambda * (double)lj / (b.mass * 2. * M_PI);
+      t -= rint(t);
+      ft.push_back((float)cos(2. * M_PI * t));
+      ft.push_back((float)(-sin(2. * M_PI * t)));
     }
     b.ft_p = (int)ft.size();
     for (int k = 0; k < d.n_p; ++k) {   // r_theta
