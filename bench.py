@@ -572,7 +572,7 @@ def batch_flops(cases, world, ms_step, clocks):
     achieved = per_rank / (ms_step / 1e3) / 1e12
     return {'algorithmic_per_step': total, 'achieved_tflops': achieved, 'fp32_nominal_tflops': nominal,
             'frac_of_nominal': achieved / nominal, 'counted': '5 N log2 N per transform; 10 transforms per '
-            'point per damped step in the complex formulation (the real-storage packing does the step with 6.5, '
+            'point per damped step in the complex formulation (the real-storage packing does the step with 5, '
             'so this is an equivalent rate)'}
 
 

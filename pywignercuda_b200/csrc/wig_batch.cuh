@@ -186,6 +186,16 @@ __device__ __forceinline__ int next_item(unsigned* ticket, int n_items) {
   return s_item;
 }
 
+// ------------------------------------------------------------------ nyquist_real
+// The mirror split below is exact where a factor maps Hermitian spectra to
+// Hermitian spectra.  At the Nyquist bin k = N/2 (its own mirror) the
+// reference's factors are complex, and the split becomes the real-linear map
+// Z -> Z (fa + fb)/2 + conj(Z) (fa - fb)/2, whose gain reaches sqrt(2) when the
+// two factors' phases differ: any Nyquist content would then grow every step.
+// A real sequence's Nyquist coefficient is real, and the reference's result for
+// it, Re IFFT[f A], only sees Re f there, so the split uses Re fa, Re fb at
+// k = N/2: the same real result, and a contraction.
+
 // ------------------------------------------------------------------ x-pass
 // Item: bx_rows(N) consecutive rows; lane group `pair` carries rows ra = row0 +
 // 2 pair and rb = ra + 1 packed into z = Re W(ra) + i Re W(rb) (W is real), lane
@@ -241,8 +251,9 @@ __device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BIn
   for (int e = 0; e < E; ++e) {
     const int k = g * Q + e / G + E * (e % G);
     const float2 P = X[sl((N - k) & (N - 1))];
-    const float2 fa = X[sf(e * G + g)];
-    const float2 fb = cmul(fa, make_float2(__ldg(gtab + 2 * k), __ldg(gtab + 2 * k + 1)));
+    float2 fa = X[sf(e * G + g)];
+    float2 fb = cmul(fa, make_float2(__ldg(gtab + 2 * k), __ldg(gtab + 2 * k + 1)));
+    if (k == N / 2) { fa.y = 0.f; fb.y = 0.f; }     // Nyquist: see nyquist_real
     const float r = 0.5f * __ldg(rtab + k);
     v[e] = cscale(cadd(cmul(v[e], cadd(fa, fb)), cmul(cconj(P), csub(fa, fb))), r);
   }
@@ -258,18 +269,18 @@ __device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BIn
 // Item: a tile of CT2 = BP_PACK * WIGB_WARPS * rf_spw(N) columns x N rows, staged
 // in shared memory (element (k, c) at k CT2 + (c ^ sw(k))) so that the global
 // loads and stores are row segments.  Each lane group owns two columns, c1 and
-// c2 = c1 + CT2 / 2:
-//   it = 0, 1:  w = IFFT[Moyal FFT(w)] for c1, then c2 (the Moyal factor
-//               depends on x, so each column takes its own transform pair);
-//   it = 2..4 (damped): Caldeira-Leggett on the pair packed into one complex
-//               sequence z = Re W(c1) + i Re W(c2).  The dissipator polynomial
+// c2 = c1 + CT2 / 2, packed into one complex sequence z = Re W(c1) + i Re W(c2)
+// (W, the Wigner function, is real):
+//   it = 0:     the Moyal pair.  The factor depends on x, so the packed spectrum
+//               is split with its mirror (as in the x-pass) and each column's
+//               factor applied to its own half;
+//   it = 1..3 (damped): Caldeira-Leggett.  The dissipator polynomial
 //               z -> A + i c D(z), D(z) = IFFT[theta/N FFT(sign(p) f(p) z)], is
 //               complex-linear and the same for every column, so it acts on the
-//               two real columns at once, and the results are Re z, Im z.
-// A damped step therefore costs 5 transform pairs per 2 columns instead of 8.
-// W is real (the Wigner function); the imaginary rounding noise the Moyal and
-// kinetic steps leave (~1e-8 in FP32) is dropped by the packing, so damped
-// columns leave the pass real.
+//               two real columns at once.
+// The results are Re z, Im z: a damped step costs 4 transform pairs per 2
+// columns instead of 8, and the imaginary rounding noise of W (~1e-8 in FP32)
+// is dropped.
 template <int N>
 __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BInst& I, int col0, int item,
                                              int sample) {
@@ -310,63 +321,67 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
   const TileSlot<CT2> sl1{c1}, sl2{c2};
   float2 w[E];
 #pragma unroll
-  for (int m = 0; m < E; ++m) w[m] = tile[sl1(g + G * m)];
+  for (int m = 0; m < E; ++m) {
+    const float2 a = tile[sl1(g + G * m)], b = tile[sl2(g + G * m)];
+    w[m] = make_float2(a.x, b.x);                  // z = Re W(c1) + i Re W(c2)
+  }
   // Moyal factor exp(-i dt [V(x - u) - V(x + u)] / hbar) r_theta mask1 mask2 / N,
   // u = hbar theta / 2 = h j:  V(x - u) - V(x + u) = -2u (a3 + a1 u^2); phase in turns
   const double h = 0.5 * I.hbar * I.dtheta;
   const double kk = -I.dt * h / (3.141592653589793238 * I.hbar);
+  const double xa = I.dx * (double)shifted(col0 + c1, nx), xb = I.dx * (double)shifted(col0 + c2, nx);
+  const double ala = kk * ((4. * I.v4 * xa * xa + 2. * I.v2) * xa + I.v1);
+  const double alb = kk * ((4. * I.v4 * xb * xb + 2. * I.v2) * xb + I.v1);
+  const double bea = kk * h * h * (4. * I.v4 * xa), beb = kk * h * h * (4. * I.v4 * xb);
+  const float mma = __ldg(A.ft + I.ft_x + nx + col0 + c1), mmb = __ldg(A.ft + I.ft_x + nx + col0 + c2);
   const bool damped = I.damp == 1;
-  const int n_it = damped ? 5 : 2;
+  const int n_it = damped ? 4 : 1;
   // One transform pair per pass through this loop (kept rolled so the kernel
-  // holds a single copy of each FFT).
+  // holds a single copy of each FFT); the exchange runs in c2's slots.
 #pragma unroll 1
   for (int it = 0; it < n_it; ++it) {
-    const TileSlot<CT2> sl{it == 0 ? c1 : c2};    // exchange slots: the column in flight
-    __syncwarp();   // the previous transform's exchange reads are done before these slots change
+    __syncwarp();   // the previous transform's exchange reads are done before slots change
     if (it == 1) {
 #pragma unroll
-      for (int m = 0; m < E; ++m) {
-        tile[sl1(g + G * m)] = w[m];               // c1 done with its Moyal step
-        w[m] = tile[sl2(g + G * m)];
-      }
-    } else if (it == 2) {
-#pragma unroll
-      for (int m = 0; m < E; ++m) {
-        w[m] = make_float2(tile[sl1(g + G * m)].x, w[m].x);   // z = Re W(c1) + i Re W(c2)
-        tile[sl1(g + G * m)] = w[m];                          // A, in the slots c1 no longer needs
-      }
+      for (int m = 0; m < E; ++m) tile[sl1(g + G * m)] = w[m];   // A, the packed post-Moyal pair
     }
-    if (it >= 2) {
+    if (it >= 1) {
 #pragma unroll
       for (int m = 0; m < E; ++m) w[m] = cscale(w[m], __ldg(sfp + g + G * m));
     }
-    F::fwd(w, tile, sl, tf, g);
-    if (it < 2) {
-      __syncwarp();   // exchange reads done before the factor writes reuse the slots
-      const int col = col0 + (it == 0 ? c1 : c2);
-      const double x = I.dx * (double)shifted(col, nx);
-      const double al = kk * ((4. * I.v4 * x * x + 2. * I.v2) * x + I.v1);
-      const double be = kk * h * h * (4. * I.v4 * x);
-      const float mm = __ldg(A.ft + I.ft_x + nx + col);
-      // Moyal factors through the column's (free) tile slots, as in the x-pass
+    F::fwd(w, tile, sl2, tf, g);
+    if (it == 0) {
+      // the two columns' Moyal factors differ (x), so the packed spectrum is split
+      // with its mirror:  Z'(k) = [Z(k) (fa + fb) + conj Z(N - k) (fa - fb)] / 2.
+      // The spectrum is staged in natural order in c1's slots, Z' goes through c2's.
+      __syncwarp();
+#pragma unroll
+      for (int e = 0; e < E; ++e) tile[sl1(g * Q + e / G + E * (e % G))] = w[e];
+      __syncwarp();
 #pragma unroll 2
       for (int e = 0; e < E; ++e) {
         const int i = e / G, b = e % G;
         const int k = g * Q + i + E * b;
         const double j = (double)(b < G / 2 ? k : k - N);
-        tile[sl(e * G + g)] = turn_factor(j * fma(be, j * j, al), __ldg(rth + k) * mm);
+        const float r = __ldg(rth + k);
+        float2 fa = turn_factor(j * fma(bea, j * j, ala), r * mma);
+        float2 fb = turn_factor(j * fma(beb, j * j, alb), r * mmb);
+        if (k == N / 2) { fa.y = 0.f; fb.y = 0.f; }   // Nyquist: see nyquist_real
+        const float2 Z = tile[sl1(k)], P = tile[sl1((N - k) & (N - 1))];
+        tile[sl2(e * G + g)] = cscale(cadd(cmul(Z, cadd(fa, fb)), cmul(cconj(P), csub(fa, fb))), 0.5f);
       }
+      __syncwarp();
 #pragma unroll
-      for (int e = 0; e < E; ++e) w[e] = cmul(w[e], tile[sl(e * G + g)]);
+      for (int e = 0; e < E; ++e) w[e] = tile[sl2(e * G + g)];
     } else {
 #pragma unroll
       for (int i = 0; i < Q; ++i)
 #pragma unroll
         for (int b = 0; b < G; ++b) w[i * G + b] = cscale(w[i * G + b], __ldg(ths + g * Q + i + E * b));
     }
-    F::inv(w, tile, sl, ti, g);
-    if (it >= 2) {
-      const float cf = (float)(it == 2 ? I.cl_k1 : (it == 3 ? I.cl_k12 : I.cl_c3));
+    F::inv(w, tile, sl2, ti, g);
+    if (it >= 1) {
+      const float cf = (float)(it == 1 ? I.cl_k1 : (it == 2 ? I.cl_k12 : I.cl_c3));
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const float2 a = tile[sl1(g + G * m)];
@@ -374,14 +389,12 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
       }
     }
   }
-  // the two columns' values: damped -> (Re z, 0), (Im z, 0); undamped -> tile c1, w
+  // unpack the two real columns: (Re z, 0) -> c1, (Im z, 0) -> c2
   __syncwarp();
-  if (damped) {
 #pragma unroll
-    for (int m = 0; m < E; ++m) {
-      tile[sl1(g + G * m)] = make_float2(w[m].x, 0.f);
-      w[m] = make_float2(w[m].y, 0.f);
-    }
+  for (int m = 0; m < E; ++m) {
+    tile[sl1(g + G * m)] = make_float2(w[m].x, 0.f);
+    w[m] = make_float2(w[m].y, 0.f);
   }
   __syncwarp();
   // observables: per column, moments sum W, sum W p_j, sum W p_j^2 (FP64), Im and

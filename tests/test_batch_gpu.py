@@ -50,10 +50,10 @@ def test_graph_and_tile_shapes_agree():
     _, o4, W4 = run_batch(cases, 20, warps=4, graph=True)
     for a, b in zip(W8, W8n):
         assert np.array_equal(a, b)
-    # the tile width decides which two columns share a packed Caldeira-Leggett
-    # sequence (their FP32 roundings mix), so 8 and 4 warps agree to FP32 level
+    # the tile width decides which two columns share a packed sequence (their FP32
+    # roundings mix), so 8 and 4 warps agree to FP32 level (20 steps)
     for a, b in zip(W8, W4):
-        assert np.max(np.abs(a - b)) < 1e-6 * np.max(np.abs(a))
+        assert np.max(np.abs(a - b)) < 1e-5 * np.max(np.abs(a))
     assert np.array_equal(o8, o8n)
     assert np.max(np.abs(o8 - o4)) < 1e-4      # the <x> bound of the FP64 comparison above
 
