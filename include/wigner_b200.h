@@ -265,7 +265,10 @@ int dirac3_jit_check(const dirac3_desc* desc, char* log, int64_t log_cap);
  * (powers of two in [64, 1024]), advanced together in FP32 complex (W,
  * FFTs, pointwise factors) with FP64 phase arguments reduced to one turn
  * before sincospif and FP64 observables (per-column moments, compensated
- * per-instance sums).  Constants are exact (no
+ * per-instance sums).  Real storage: W is a Wigner function, so two real rows
+ * (x-pass) or columns (p-pass) share each complex transform; the state keeps
+ * the complex64 layout but each step leaves W real (imaginary parts, which are
+ * rounding noise for a real initial state, are dropped).  Constants are exact (no
  * '%f' rounding).  No counterpart in the reference, which runs one complex128
  * instance per Run() (GPU_Wigner2D_FFT.py:1843); the step is the same Lie
  * split (:1884-1913). */
