@@ -576,6 +576,10 @@ def batch_flops(cases, world, ms_step, clocks):
             'so this is an equivalent rate)'}
 
 
+# DRAM bytes of one Dirac2D step of one replica at 512^2 (row + column pass); filled from an ncu capture
+NCU_TRAFFIC_DIRAC = None
+
+
 def make_dirac_instance(time_steps):
     from pywignercuda_b200 import GPU_Dirac2D
 
@@ -618,6 +622,17 @@ def run_dirac(args, world, rank, local):
     value = world * R * 512 * 512 * args.steps / (ms / 1e3)
     peak, peak_kind = peaks()
     achieved = 2 * 512 * 512 * 128 / (ms / 1e3 / (R * args.steps)) / 1e9   # 2 passes x 128 B per point
+    # end to end: each replica's host spinor in, host spinor and observables out, through dirac_run_host
+    host_out = np.empty_like(P0)
+    obs_e2e = np.empty((args.steps, _lib.DIRAC_NOBS))
+    P0c = np.ascontiguousarray(P0, dtype=np.complex128)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for i in insts:
+        _lib.check(lib.dirac_run_host(i._handle, P0c.ctypes.data, host_out.ctypes.data, 0, args.steps,
+                                      _lib.dptr(obs_e2e), stream.cuda_stream), 'e2e')
+    e2e_s = barrier_max(world, time.perf_counter() - t0)
     line = {'metric': 'Dirac2D spinor-pt-steps/s', 'value': value, 'unit': 'spinor-pt-steps/s',
             'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms / args.steps,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c128',
@@ -625,10 +640,27 @@ def run_dirac(args, world, rank, local):
             'config': {'workload': 'Dirac2D 512x512 c=137.036 softened Coulomb, p0=(5,0), dt=1e-4',
                        'replicas_per_gpu': R,
                        'l2': 'per-step working set %d MB > 126 MB L2' % (R * 16)},
+            'e2e': {'value': world * R * 512 * 512 * args.steps / e2e_s, 'unit': 'spinor-pt-steps/s',
+                    'h2d_bytes_per_step': R * P0c.nbytes / args.steps,
+                    'd2h_bytes_per_step': R * (P0c.nbytes + obs_e2e.nbytes) / args.steps,
+                    'note': 'one dirac_run_host call per replica, one after the other'},
             'roofline': {'bound': 'hbm', 'kernel': 'dirac_rowpass+dirac_colpass (step average)',
-                         'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
-                         'peak_kind': peak_kind, 'traffic': None},
+                         'algorithmic_bytes_per_point': 256, 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'peak_kind': peak_kind, 'traffic': NCU_TRAFFIC_DIRAC,
+                         'traffic_per': 'step (row + column pass) of one replica, ncu at 512^2'},
             'gpu_launches': R * (2 * args.steps + 3), 'clocks': clk.summary()}
+    if rank == 0 and args.cpu_baseline:
+        from oracle.dirac2d import DiracOracle, DiracParams
+        prm = DiracParams(512, 512, 12., 12., 1e-4, c=137.036, A0='-1./sqrt(x*x+y*y+0.5)')
+        orc = DiracOracle(prm)
+        t0, k = time.perf_counter(), 0
+        while time.perf_counter() - t0 < 10. or k < 1:
+            orc.run(P0c, 1)
+            k += 1
+        dt_cpu = time.perf_counter() - t0
+        line['cpu_baseline'] = {'value': 512 * 512 * k / dt_cpu, 'unit': 'spinor-pt-steps/s',
+                                'cores': os.cpu_count(), 'kind': 'port',
+                                'sample': '%d steps of the oracle (numpy + scipy.fft) at 512^2, same instance' % k}
     if rank == 0:
         print(json.dumps(line))
 
@@ -741,11 +773,13 @@ def main():
                     help='batch workload: only the timed section (for profiler launch lists)')
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.impl == 'reference':
+        # host-only work on rank 0; the other ranks exit 0 without joining a process group
+        run_reference(args, int(os.environ.get('WORLD_SIZE', '1')), int(os.environ.get('RANK', '0')))
+        return
     world, rank, local = dist_setup()
     try:
-        if args.impl == 'reference':
-            run_reference(args, world, rank)
-        elif args.workload == 'dirac':
+        if args.workload == 'dirac':
             run_dirac(args, world, rank, local)
         elif args.workload == 'c128':
             run_c128(args, world, rank, local)

@@ -50,19 +50,23 @@ struct DiracArgs {
 template <class Phys>
 __device__ __forceinline__ void dirac_A(const DiracArgs& a, const Phys& ph, double t, double x, double y,
                                         double2& p1, double2& p2, double2& p3, double2& p4) {
+  // The reference's pow(v, 2.) are squares and its repeated "* sF / F" one
+  // ratio: written as products, the factors differ from it by rounding only.
   const double A0 = ph.A0(t, x, y), A1 = ph.A1(t, x, y), A2 = ph.A2(t, x, y), A3 = ph.A3(t, x, y);
-  const double F = sqrt(pow(a.mass * a.c * a.c, 2.) + a.c * (pow(A1, 2.) + pow(A2, 2.) + pow(A3, 2.)));
+  const double mc2 = a.mass * a.c * a.c;
+  const double F = sqrt(mc2 * mc2 + a.c * (A1 * A1 + A2 * A2 + A3 * A3));
   double sv, cv;
   sincos(a.dt * A0, &sv, &cv);
   const double2 e = make_double2(cv, -sv);               // exp(-i dt A0)
   double sF, cF;
   sincos(a.dt * F, &sF, &cF);
-  const double2 U11 = make_double2(cF, -a.mass * a.c * a.c * sF / F);
-  const double2 U33 = make_double2(cF, a.mass * a.c * a.c * sF / F);
-  const double2 U31 = make_double2(0., A3 * sF / F);
-  const double2 U41 = make_double2(-A2 * sF / F, A1 * sF / F);
-  const double2 U32 = make_double2(A2 * sF / F, A1 * sF / F);
-  const double2 U42 = make_double2(0., -A3 * sF / F);
+  const double r = sF / F;
+  const double2 U11 = make_double2(cF, -mc2 * r);
+  const double2 U33 = make_double2(cF, mc2 * r);
+  const double2 U31 = make_double2(0., A3 * r);
+  const double2 U41 = make_double2(-A2 * r, A1 * r);
+  const double2 U32 = make_double2(A2 * r, A1 * r);
+  const double2 U42 = make_double2(0., -A3 * r);
   const double2 q1 = cmul(e, cadd(cadd(cmul(U11, p1), cmul(U31, p3)), cmul(U32, p4)));
   const double2 q2 = cmul(e, cadd(cadd(cmul(U11, p2), cmul(U41, p3)), cmul(U42, p4)));
   const double2 q3 = cmul(e, cadd(cadd(cmul(U31, p1), cmul(U32, p2)), cmul(U33, p3)));

@@ -3,7 +3,9 @@
 // calls, GPU_Dirac2D.py:369-388).  The host prepends a prelude defining the
 // reference's '%f' constants (mass, c, dt, dX, dY, dPx, dPy; :358-367),
 // struct UserPhys { A0..A3(t, x, y) } from Potential_{0..3}_String, and the
-// macros DIR_NX, DIR_NY, DIR_ROWS, DIR_RNT, DIR_C, DIR_CNT, DIR_SNT.
+// macros DIR_NX, DIR_NY, DIR_ROWS, DIR_RNT, DIR_RMB, DIR_C, DIR_CNT, DIR_CMB,
+// DIR_SNT (DIR_RMB / DIR_CMB: resident CTAs per SM the register allocation of
+// the row / column pass targets).
 #pragma once
 #include "wig_dirac.cuh"
 
@@ -14,14 +16,14 @@ __device__ __forceinline__ UserPhys user_phys(const wig::DiracArgs& a) {
   return ph;
 }
 
-extern "C" __global__ void __launch_bounds__(DIR_RNT)
+extern "C" __global__ void __launch_bounds__(DIR_RNT, DIR_RMB)
 dirac_rowpass(wig::DiracArgs a, double2* psi, int mode, int parity, double t_step, double t_obs,
               double* obs_row) {
   wig::dirac_row_body<UserPhys, DIR_NX, DIR_NY, DIR_ROWS, DIR_RNT>(
       a, user_phys(a), psi, mode, parity, t_step, t_obs, obs_row);
 }
 
-extern "C" __global__ void __launch_bounds__(DIR_CNT)
+extern "C" __global__ void __launch_bounds__(DIR_CNT, DIR_CMB)
 dirac_colpass(wig::DiracArgs a, double2* psi) {
   wig::dirac_col_body<DIR_NX, DIR_NY, DIR_C, DIR_CNT>(a, psi);
 }

@@ -1,0 +1,44 @@
+"""bench.py's reference arm on the host: the JSON line it prints and its
+behaviour on ranks other than 0.  The GPU arm is exercised by the round of
+GPU tests and the bench itself."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _run(extra_env=None, timeout=300):
+    env = dict(os.environ)
+    env.update(extra_env or {})
+    return subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference',
+                           '--steps', '1', '--warmup', '3'],
+                          capture_output=True, text=True, timeout=timeout, env=env, cwd=ROOT)
+
+
+def test_reference_arm_line():
+    p = _run()
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [ln for ln in p.stdout.splitlines() if ln.startswith('{')]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ('metric', 'value', 'unit', 'n_gpus', 'steps', 'warmup', 'ms_per_step', 'higher_is_better',
+              'scaling', 'vs_baseline', 'dtype', 'data', 'config', 'cpu_baseline', 'e2e'):
+        assert k in d, k
+    assert d['impl'] == 'reference'
+    assert d['metric'] == 'Wigner2D grid-pt-steps/s: FP32 batched vs plain complex128 at stated error'
+    assert d['unit'] == 'grid-pt-steps/s' and d['higher_is_better'] is True
+    assert d['value'] > 0 and d['steps'] >= 2 and d['warmup'] >= 3
+    assert d['cpu_baseline']['kind'] == 'port' and d['cpu_baseline']['cores'] >= 1
+    assert d['cpu_baseline']['value'] == d['value']
+    assert d['e2e'] == {'value': d['value'], 'unit': d['unit'], 'h2d_bytes_per_step': 0,
+                        'd2h_bytes_per_step': 0}
+
+
+def test_reference_arm_other_ranks_exit_quietly():
+    p = _run({'WORLD_SIZE': '2', 'RANK': '1', 'LOCAL_RANK': '1'}, timeout=120)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert not [ln for ln in p.stdout.splitlines() if ln.startswith('{')]
