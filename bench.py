@@ -576,8 +576,10 @@ def batch_flops(cases, world, ms_step, clocks):
             'so this is an equivalent rate)'}
 
 
-# DRAM bytes of one Dirac2D step of one replica at 512^2 (row + column pass); filled from an ncu capture
-NCU_TRAFFIC_DIRAC = None
+# DRAM bytes of one Dirac2D step of one replica at 512^2 (row + column pass, read + write), from
+# the ncu capture summarised in profiles/dirac_passes_512.md (the replica fits in L2: one read of
+# it per pass, the writes still in L2 when each kernel ends)
+NCU_TRAFFIC_DIRAC = 16.917e6 + 0.002e6 + 16.822e6 + 0.0003e6
 
 
 def make_dirac_instance(time_steps):
