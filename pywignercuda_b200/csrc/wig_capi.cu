@@ -399,6 +399,13 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
   P->xrows = clampi(2048 / NX, 1, NP);
   P->xnt = round_warp(clampi(P->xrows * NX / 8, 32, 256));
   P->xminb = 3;
+  if (NX == 1024 && d->splitting == WIG_SPLIT_LIE) {
+    // one 1024-point row per CTA of 128 threads, 8 CTAs per SM (64 registers, no spill): the
+    // rows of a 1024^2 grid fill one wave (2.446 -> 2.293 ms per 16-replica Caldeira-Leggett step)
+    P->xrows = 1;
+    P->xnt = 128;
+    P->xminb = 8;
+  }
   P->pc = clampi(2048 / NP, 1, NX);
   P->pnt = round_warp(clampi(P->pc * NP / 8, 32, 256));
   P->pminb = P->damp ? 2 : 3;
