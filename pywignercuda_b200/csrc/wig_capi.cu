@@ -399,6 +399,9 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
   P->xrows = clampi(2048 / NX, 1, NP);
   P->xnt = round_warp(clampi(P->xrows * NX / 8, 32, 256));
   P->xminb = 3;
+  // beyond 2048-point rows a thread holds two radix-8 butterflies per stage: 3 CTAs per SM
+  // (80 registers) would spill ~1.4 KB per thread, 2 (128) spill a few bytes
+  if ((P->xrows * NX / 8 + P->xnt - 1) / P->xnt > 1) P->xminb = 2;
   if (NX == 1024 && d->splitting == WIG_SPLIT_LIE) {
     // one 1024-point row per CTA of 128 threads, 8 CTAs per SM (64 registers, no spill): the
     // rows of a 1024^2 grid fill one wave (2.446 -> 2.293 ms per 16-replica Caldeira-Leggett step)
@@ -409,6 +412,7 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
   P->pc = clampi(2048 / NP, 1, NX);
   P->pnt = round_warp(clampi(P->pc * NP / 8, 32, 256));
   P->pminb = P->damp ? 2 : 3;
+  if ((P->pc * NP / 8 + P->pnt - 1) / P->pnt > 1) P->pminb = 2;   // as for the x-pass, beyond 2048 points
   if (const char* tv = getenv("WIG_TILING")) {
     int v[6];
     if (sscanf(tv, "%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]) == 6) {

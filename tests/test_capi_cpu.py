@@ -56,6 +56,28 @@ def test_wigner_jit_compiles(n):
     assert rc == 0, log
     assert 'wig_xpass' in log and 'wig_ppass' in log
     assert '0 bytes spill stores' in log
+    # the x-pass's register target follows the butterflies a thread holds per stage, so it
+    # spills at most a few bytes at every size (the exact count depends on the NVRTC loaded)
+    lines = log.splitlines()
+    at = [i for i, l in enumerate(lines) if "Compiling entry function 'wig_xpass'" in l]
+    props = ' '.join(lines[at[0] + 1:at[0] + 3])
+    assert int(props.split(' bytes spill stores')[0].split()[-1]) <= 16, props
+
+
+def test_dirac_tiling_override_validated(monkeypatch):
+    """WIG_DIRAC_TILING replaces the planner's tiles; a tile that does not divide
+    the grid is refused on the host, before any compile."""
+    d = DiracDesc()
+    d.abi_version = _lib.ABI_VERSION
+    d.n_x = d.n_y = 64
+    d.x_amplitude = d.y_amplitude = 12.
+    d.mass, d.c, d.hbar, d.dt = 1., 137.036, 1., 1e-4
+    monkeypatch.setenv('WIG_DIRAC_TILING', '3,0,0,0,0,0')
+    rc, log = jit(d, 'dirac_jit_check')
+    assert rc == 1 and 'must divide the grid' in log      # WIG_ERR_ARG
+    monkeypatch.setenv('WIG_DIRAC_TILING', '2,64,2,2,64,2')
+    rc, log = jit(d, 'dirac_jit_check')
+    assert rc == 0, log
 
 
 @pytest.mark.parametrize('nx,ny', [(512, 512), (64, 32), (1024, 1024), (16, 2048)])
