@@ -1,0 +1,88 @@
+// Host execution of this package's CUDA device code, for checking the kernels'
+// index arithmetic, tiling and synchronisation on a machine without a GPU.
+// Test infrastructure only: nothing in the package includes it.
+//
+// One std::thread per CUDA thread; the blocks of a launch run one after another
+// (the kernels checked this way never wait on another block).  __syncthreads
+// is a std::barrier over the block, __syncwarp and the shuffles a barrier over
+// the warp.  Block-scope `__shared__` arrays become function statics (one copy,
+// seen by every thread of the running block); `extern __shared__` arrays are
+// rewritten by the test harness to point into emu_smem.  Math functions are
+// the host C library's.
+#pragma once
+#include <math.h>
+
+#include <barrier>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <thread>
+#include <vector>
+
+struct double2 { double x, y; };
+struct float2 { float x, y; };
+struct int2 { int x, y; };
+inline double2 make_double2(double a, double b) { return {a, b}; }
+inline float2 make_float2(float a, float b) { return {a, b}; }
+inline int2 make_int2(int a, int b) { return {a, b}; }
+
+struct emu_dim3 { unsigned x = 0, y = 1, z = 1; };
+inline thread_local emu_dim3 threadIdx, blockIdx;
+inline emu_dim3 blockDim, gridDim;
+
+#define __device__
+#define __host__
+#define __global__
+#define __forceinline__ inline
+#define __restrict__
+#define __launch_bounds__(...)
+#define __shared__ static
+
+alignas(256) inline unsigned char emu_smem[1 << 22];
+
+inline std::barrier<>* emu_block_barrier = nullptr;
+inline std::vector<std::unique_ptr<std::barrier<>>> emu_warp_barriers;
+inline double emu_shfl[1024];
+
+inline void __syncthreads() { emu_block_barrier->arrive_and_wait(); }
+inline void __syncwarp(unsigned = 0xffffffffu) { emu_warp_barriers[threadIdx.x / 32]->arrive_and_wait(); }
+
+// every lane of the warp takes part (the kernels shuffle with full masks only)
+inline double __shfl_xor_sync(unsigned, double v, int lane_mask) {
+  const unsigned t = threadIdx.x;
+  std::barrier<>& wb = *emu_warp_barriers[t / 32];
+  emu_shfl[t] = v;
+  wb.arrive_and_wait();
+  const double r = emu_shfl[(t & ~31u) | ((t & 31u) ^ (unsigned)lane_mask)];
+  wb.arrive_and_wait();
+  return r;
+}
+
+template <class T> inline T __ldg(const T* p) { return *p; }
+
+// grid x block threads; block b's threads run concurrently, blocks in turn
+inline void emu_launch(unsigned grid, unsigned block, const std::function<void()>& body) {
+  if (block == 0 || block > 1024 || (block % 32) != 0) {
+    std::fprintf(stderr, "emu_launch: block of %u threads\n", block);
+    std::exit(3);
+  }
+  gridDim = {grid, 1, 1};
+  blockDim = {block, 1, 1};
+  for (unsigned b = 0; b < grid; ++b) {
+    std::barrier<> bar((std::ptrdiff_t)block);
+    emu_block_barrier = &bar;
+    emu_warp_barriers.clear();
+    for (unsigned w = 0; w < block / 32; ++w) emu_warp_barriers.emplace_back(new std::barrier<>(32));
+    std::vector<std::thread> threads;
+    threads.reserve(block);
+    for (unsigned t = 0; t < block; ++t)
+      threads.emplace_back([&body, t, b] {
+        threadIdx = {t, 0, 0};
+        blockIdx = {b, 0, 0};
+        body();
+      });
+    for (auto& th : threads) th.join();
+  }
+}

@@ -1,0 +1,80 @@
+"""The Dirac2D kernels' device code, executed on the host (tests/emu/shim.h:
+one thread per CUDA thread, real barriers and shuffles), against the oracle.
+
+It checks the passes' tiling, index arithmetic, partial-sum reductions and the
+launch sequence of dirac_run, for tile shapes the planner picks at 512^2 and
+others, without a GPU.  The same device sources are what NVRTC compiles for
+sm_100a; only `extern __shared__` arrays are pointed at a host buffer."""
+import os
+import re
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle.common import rel_l2
+from oracle.dirac2d import DiracOracle, DiracParams, spinor_particle_spin_up
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CSRC = os.path.join(ROOT, 'pywignercuda_b200', 'csrc')
+EMU = os.path.join(ROOT, 'tests', 'emu')
+HEADERS = ('wig_fft.cuh', 'wig_wigner.cuh', 'wig_dirac.cuh', 'wig_jit_dirac.cuh')
+EXTERN_SHARED = re.compile(r'extern\s+__shared__\s+(\w+)\s+(\w+)\s*\[\s*\]\s*;')
+
+NX, NY = 32, 16
+XA, YA, DT, MASS, C = 12., 8., 1e-3, 1., 137.036
+A = ('-1./sqrt(x*x+y*y+0.5) + 0.3*t*x', '-0.5*y', '0.5*x', '0.')   # as in tests/emu/dirac2d_emu.cpp
+
+
+def stage(dst):
+    for h in HEADERS:
+        src = open(os.path.join(CSRC, h)).read()
+        src = EXTERN_SHARED.sub(lambda m: '%s* %s = reinterpret_cast<%s*>(emu_smem);'
+                                % (m.group(1), m.group(2), m.group(1)), src)
+        open(os.path.join(dst, h), 'w').write(src)
+    for f in ('shim.h', 'dirac2d_emu.cpp'):
+        shutil.copy(os.path.join(EMU, f), dst)
+
+
+def build(dst, rows, rnt, cc, cnt):
+    exe = os.path.join(dst, 'dirac2d_emu_%d_%d_%d_%d' % (rows, rnt, cc, cnt))
+    macros = dict(DIR_NX=NX, DIR_NY=NY, DIR_ROWS=rows, DIR_RNT=rnt, DIR_RMB=1, DIR_C=cc, DIR_CNT=cnt,
+                  DIR_CMB=1, DIR_SNT=256)
+    cmd = (['g++', '-std=c++20', '-O1', '-pthread', '-w', '-I', dst] +
+           ['-D%s=%d' % kv for kv in macros.items()] + [os.path.join(dst, 'dirac2d_emu.cpp'), '-o', exe])
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return exe
+
+
+@pytest.fixture(scope='module')
+def staged(tmp_path_factory):
+    if shutil.which('g++') is None:
+        pytest.skip('no host C++ compiler')
+    d = str(tmp_path_factory.mktemp('emu'))
+    stage(d)
+    return d
+
+
+# (rows, row threads, columns, column threads) per CTA: the planner's rule at 32 x 16 (one CTA per
+# pass), several CTAs per pass, and one row / one column per CTA as at 512^2
+@pytest.mark.parametrize('rows,rnt,cc,cnt', [(16, 256, 32, 256), (4, 64, 8, 64), (1, 32, 1, 32)])
+def test_dirac2d_device_code_matches_oracle(staged, rows, rnt, cc, cnt):
+    exe = build(staged, rows, rnt, cc, cnt)
+    prm = DiracParams(NX, NY, XA, YA, DT, mass=MASS, c=C, A0=A[0], A1=A[1], A2=A[2], A3=A[3],
+                      constants='exact')
+    psi0 = spinor_particle_spin_up(prm, (2., 1.), lambda x, y: np.exp(-(x * x + y * y) / 4.))
+    psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
+    steps = 3
+    fin, fout, fobs = (os.path.join(staged, n) for n in ('psi_in.bin', 'psi_out.bin', 'obs.bin'))
+    psi0.tofile(fin)
+    r = subprocess.run([exe, fin, fout, fobs, str(steps), repr(XA), repr(YA), repr(DT), repr(MASS), repr(C)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.fromfile(fout, dtype=np.complex128).reshape(4, NY, NX)
+    obs = np.fromfile(fobs).reshape(steps, 10)
+    ref_obs, ref = DiracOracle(prm).run(psi0, steps)
+    assert rel_l2(got, ref) < 1e-12
+    scale = np.maximum(np.abs(ref_obs).max(axis=0), 1e-3)
+    assert np.all(np.abs(obs - ref_obs) / scale < 1e-10), (obs - ref_obs) / scale
