@@ -1,0 +1,161 @@
+// Host execution of the complex128 Wigner2D kernels (csrc/wig_jit_wigner.cuh)
+// in the launch sequence of wig_run for a Lie-split Caldeira-Leggett plan
+// (csrc/wig_capi.cu: wig_run_begin / wig_run_step / wig_run_end), with the tile
+// macros WIG_* given on the command line.  Test infrastructure:
+// tests/test_emu_cpu.py builds it and compares the result with the oracle.
+//
+//   wigner2d_emu W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda
+//
+// W_in / W_out: (WIG_NP, WIG_NX) complex128; obs_out: (n_prop + 1) x 11
+// doubles.  hbar = mass = 1, constants used exactly.  The expressions are
+// fixed here and restated by the test for the oracle.
+#include "shim.h"
+
+#define __constant__
+double dt, dx, dp, dtheta, dlambda, mass, hBar, D_Theta, D_Lambda;
+
+struct UserPhys {
+  double cf[8];
+  double Potential(double t, double x) const { return 0.05 * pow(x, 4) - pow(x, 2) + 0.2 * x * sin(3. * t); }
+  double KineticEnergy(double p) const { return 0.5 * p * p; }
+  double f(double p) const { return fabs(p); }
+  double DPotential(double t, double x) const { return 0.2 * pow(x, 3) - 2. * x + 0.2 * sin(3. * t); }
+};
+
+#include "wig_jit_wigner.cuh"
+
+namespace {
+
+std::vector<double> shifted_range(double amp, int n) {
+  const double d = 2. * amp / (double)n;
+  const double start = -amp, stop = amp - d;
+  const double step = (stop - start) / (double)(n - 1);
+  std::vector<double> y(n), out(n);
+  for (int i = 0; i < n; ++i) y[i] = (double)i * step + start;
+  y[n - 1] = stop;
+  for (int k = 0; k < n; ++k) out[k] = y[(k + n / 2) % n];
+  return out;
+}
+
+std::vector<double2> twiddles(int n) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  std::vector<double2> t(n);
+  for (int m = 0; m < n; ++m) {
+    const long double a = 2.0L * pi * (long double)m / (long double)n;
+    double c = (double)cosl(a), s = (double)(-sinl(a));
+    if (fabs(c) < 1e-18) c = 0.;
+    if (fabs(s) < 1e-18) s = 0.;
+    t[m] = make_double2(c, s);
+  }
+  return t;
+}
+
+bool read_all(const char* path, void* p, size_t bytes) {
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return false;
+  const bool ok = std::fread(p, 1, bytes, f) == bytes;
+  std::fclose(f);
+  return ok;
+}
+
+bool write_all(const char* path, const void* p, size_t bytes) {
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return false;
+  const bool ok = std::fwrite(p, 1, bytes, f) == bytes;
+  std::fclose(f);
+  return ok;
+}
+
+int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc != 11) {
+    std::fprintf(stderr, "usage: %s W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda\n", argv[0]);
+    return 2;
+  }
+  constexpr int NX = WIG_NX, NP = WIG_NP, NOBS = 11;
+  const long n_prop = std::atol(argv[4]);
+  const double xa = std::atof(argv[5]), pa = std::atof(argv[6]);
+  const double gamma = std::atof(argv[8]);
+  if (n_prop < 1 || NP % WIG_XROWS != 0 || NX % WIG_PC != 0) return 2;
+  dt = std::atof(argv[7]);
+  D_Theta = std::atof(argv[9]);
+  D_Lambda = std::atof(argv[10]);
+  mass = hBar = 1.;
+  const size_t npts = (size_t)NX * NP;
+  std::vector<double2> W(npts);
+  if (!read_all(argv[1], W.data(), npts * sizeof(double2))) return 4;
+
+  // wig_plan / wig_create
+  dx = 2. * xa / NX;
+  dp = 2. * pa / NP;
+  dtheta = 2. * M_PI / (2. * pa);
+  dlambda = 2. * M_PI / (2. * xa);
+  const int n_cta_x = NP / WIG_XROWS, n_cta_p = NX / WIG_PC;
+  const int n_cta_r = clampi(NX * NP / (4 * WIG_RNT), 1, 296);
+
+  wig::WigArgs a{};
+  a.dt = dt; a.dx = dx; a.dp = dp; a.dtheta = dtheta; a.dlambda = dlambda; a.mass = mass; a.hbar = hBar;
+  a.D_theta = D_Theta; a.D_lambda = D_Lambda;
+  a.dX = dx; a.dP = dp; a.mass_exact = mass;
+  {
+    const double g = dt * gamma;
+    const double c1 = 2. / 3. * g, c2 = 2. / 2. * g, c3 = 2. * g;
+    const double k1 = (c1 + c2) != 0. ? c1 * c2 / (c1 + c2) : 0.;
+    a.cl_k1 = make_double2(0., k1);
+    a.cl_k12 = make_double2(0., c1 + c2);
+    a.cl_c3 = make_double2(0., c3);
+  }
+  std::vector<double> xt = shifted_range(xa, NX), pt = shifted_range(pa, NP);
+  std::vector<double> tht = shifted_range(dtheta * NP / 2., NP), ths(NP);
+  for (int i = 0; i < NP; ++i) ths[i] = tht[i] * (1.0 / (double)NP);
+  std::vector<double> lt = shifted_range(dlambda * NX / 2., NX);
+  const UserPhys ph{};
+  std::vector<double> dv(NX), v0(NX);
+  for (int k = 0; k < NX; ++k) {
+    dv[k] = ph.DPotential(0., xt[k]);
+    v0[k] = ph.Potential(0., xt[k]);
+  }
+  std::vector<double2> twx = twiddles(NX), twp = twiddles(NP);
+  std::vector<double> rl(NX), rt(NP), m1(NX), m2(NX), sfp(NP), rth(NP);
+  const int nparts = n_cta_x > n_cta_p ? (n_cta_x > n_cta_r ? n_cta_x : n_cta_r) : (n_cta_p > n_cta_r ? n_cta_p : n_cta_r);
+  std::vector<double> partials((size_t)nparts * wig::NACC, 0.);
+  std::vector<double> obs((size_t)(n_prop + 1) * NOBS, 0.);
+  double2 scale{1., 0.};
+  a.x_tab = xt.data(); a.p_tab = pt.data(); a.dV_tab = dv.data(); a.V0_tab = v0.data(); a.theta_s = ths.data();
+  a.r_lambda = rl.data(); a.r_theta = rt.data(); a.mask1 = m1.data(); a.mask2s = m2.data(); a.sfp = sfp.data();
+  a.tw_x = twx.data(); a.tw_p = twp.data(); a.partials = partials.data(); a.n_partials = 0;
+  a.lambda_tab = lt.data(); a.hbar_exact = hBar; a.L_material = 1.;
+  a.r_theta_half = rth.data();
+  emu_launch(1, 64, [&] { wig_setup(a, rl.data(), rt.data(), m1.data(), m2.data(), sfp.data(), rth.data()); });
+
+  double2* Wp = W.data();
+  // wig_run_begin: partial sums of W for the initial normalisation and sample 0
+  emu_launch(n_cta_r, WIG_RNT, [&] { wig_reduce(a, Wp); });
+  a.n_partials = n_cta_r;
+  // wig_run_step (first call of a run: normalise on load; damped steps renormalise)
+  const bool damped = gamma != 0.;
+  for (long n = 0; n < n_prop; ++n) {
+    const int mode = (n == 0) ? 1 : (damped ? 2 : 0);
+    double* orow = obs.data() + (size_t)n * NOBS;
+    emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, mode, orow); });
+    const double t = (double)n * dt;
+    emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass(a, Wp, t); });
+    a.n_partials = n_cta_p;
+  }
+  // wig_run_end
+  {
+    const int fmode = damped ? 2 : 0;
+    double* last = obs.data() + (size_t)n_prop * NOBS;
+    emu_launch(1, WIG_RNT, [&] { wig_finalize(a, fmode, last, &scale); });
+    if (fmode != 0) {
+      const long n = (long)npts;
+      emu_launch(2, WIG_RNT, [&] { wig_scale(Wp, n, &scale); });
+    }
+  }
+  if (!write_all(argv[2], W.data(), npts * sizeof(double2))) return 4;
+  if (!write_all(argv[3], obs.data(), obs.size() * sizeof(double))) return 4;
+  return 0;
+}

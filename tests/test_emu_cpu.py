@@ -1,10 +1,12 @@
-"""The Dirac2D kernels' device code, executed on the host (tests/emu/shim.h:
-one thread per CUDA thread, real barriers and shuffles), against the oracle.
+"""The complex128 Wigner2D and Dirac2D kernels' device code, executed on the
+host (tests/emu/shim.h: one thread per CUDA thread, real barriers and
+shuffles), against the oracle.
 
 It checks the passes' tiling, index arithmetic, partial-sum reductions and the
-launch sequence of dirac_run, for tile shapes the planner picks at 512^2 and
-others, without a GPU.  The same device sources are what NVRTC compiles for
-sm_100a; only `extern __shared__` arrays are pointed at a host buffer."""
+launch sequences of wig_run and dirac_run, for the tile shapes the planners
+pick at large grids and others, without a GPU.  The device sources are the
+ones NVRTC compiles for sm_100a; only `extern __shared__` arrays are pointed
+at a host buffer."""
 import os
 import re
 import shutil
@@ -15,11 +17,12 @@ import pytest
 
 from oracle.common import rel_l2
 from oracle.dirac2d import DiracOracle, DiracParams, spinor_particle_spin_up
+from oracle.wigner2d import WignerOracle, WignerParams
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, 'pywignercuda_b200', 'csrc')
 EMU = os.path.join(ROOT, 'tests', 'emu')
-HEADERS = ('wig_fft.cuh', 'wig_wigner.cuh', 'wig_dirac.cuh', 'wig_jit_dirac.cuh')
+HEADERS = ('wig_fft.cuh', 'wig_wigner.cuh', 'wig_dirac.cuh', 'wig_jit_dirac.cuh', 'wig_jit_wigner.cuh')
 EXTERN_SHARED = re.compile(r'extern\s+__shared__\s+(\w+)\s+(\w+)\s*\[\s*\]\s*;')
 
 NX, NY = 32, 16
@@ -33,16 +36,14 @@ def stage(dst):
         src = EXTERN_SHARED.sub(lambda m: '%s* %s = reinterpret_cast<%s*>(emu_smem);'
                                 % (m.group(1), m.group(2), m.group(1)), src)
         open(os.path.join(dst, h), 'w').write(src)
-    for f in ('shim.h', 'dirac2d_emu.cpp'):
+    for f in ('shim.h', 'dirac2d_emu.cpp', 'wigner2d_emu.cpp'):
         shutil.copy(os.path.join(EMU, f), dst)
 
 
-def build(dst, rows, rnt, cc, cnt):
-    exe = os.path.join(dst, 'dirac2d_emu_%d_%d_%d_%d' % (rows, rnt, cc, cnt))
-    macros = dict(DIR_NX=NX, DIR_NY=NY, DIR_ROWS=rows, DIR_RNT=rnt, DIR_RMB=1, DIR_C=cc, DIR_CNT=cnt,
-                  DIR_CMB=1, DIR_SNT=256)
+def build(dst, source, macros):
+    exe = os.path.join(dst, source.split('.')[0] + ''.join('_%d' % v for v in macros.values()))
     cmd = (['g++', '-std=c++20', '-O1', '-pthread', '-w', '-I', dst] +
-           ['-D%s=%d' % kv for kv in macros.items()] + [os.path.join(dst, 'dirac2d_emu.cpp'), '-o', exe])
+           ['-D%s=%d' % kv for kv in macros.items()] + [os.path.join(dst, source), '-o', exe])
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
     return exe
@@ -61,7 +62,8 @@ def staged(tmp_path_factory):
 # pass), several CTAs per pass, and one row / one column per CTA as at 512^2
 @pytest.mark.parametrize('rows,rnt,cc,cnt', [(16, 256, 32, 256), (4, 64, 8, 64), (1, 32, 1, 32)])
 def test_dirac2d_device_code_matches_oracle(staged, rows, rnt, cc, cnt):
-    exe = build(staged, rows, rnt, cc, cnt)
+    exe = build(staged, 'dirac2d_emu.cpp', dict(DIR_NX=NX, DIR_NY=NY, DIR_ROWS=rows, DIR_RNT=rnt, DIR_RMB=1,
+                                                DIR_C=cc, DIR_CNT=cnt, DIR_CMB=1, DIR_SNT=256))
     prm = DiracParams(NX, NY, XA, YA, DT, mass=MASS, c=C, A0=A[0], A1=A[1], A2=A[2], A3=A[3],
                       constants='exact')
     psi0 = spinor_particle_spin_up(prm, (2., 1.), lambda x, y: np.exp(-(x * x + y * y) / 4.))
@@ -78,3 +80,38 @@ def test_dirac2d_device_code_matches_oracle(staged, rows, rnt, cc, cnt):
     assert rel_l2(got, ref) < 1e-12
     scale = np.maximum(np.abs(ref_obs).max(axis=0), 1e-3)
     assert np.all(np.abs(obs - ref_obs) / scale < 1e-10), (obs - ref_obs) / scale
+
+
+WNX, WNP = 64, 32
+WXA, WPA, WDT, WGAMMA, WDTH, WDLA = 10., 8., 0.01, 0.1, 0.1, 0.05
+# as in tests/emu/wigner2d_emu.cpp
+WPOT, WDPOT = '0.05*pow(x,4) - pow(x,2) + 0.2*x*sin(3.*t)', '0.2*pow(x,3) - 2.*x + 0.2*sin(3.*t)'
+
+
+# (rows, x threads, columns, p threads) per CTA: the planner's rule at 64 x 32 (one CTA per pass),
+# one row per 128-thread CTA as for 1024-point rows, and several small CTAs per pass
+@pytest.mark.parametrize('xrows,xnt,pc,pnt', [(32, 256, 64, 256), (1, 128, 2, 32), (4, 32, 8, 32)])
+def test_wigner2d_device_code_matches_oracle(staged, xrows, xnt, pc, pnt):
+    exe = build(staged, 'wigner2d_emu.cpp', dict(WIG_NX=WNX, WIG_NP=WNP, WIG_XROWS=xrows, WIG_XNT=xnt,
+                                                 WIG_KIN_STRING=0, WIG_PC=pc, WIG_PNT=pnt, WIG_DAMP=1,
+                                                 WIG_RNT=256, WIG_XMINB=1, WIG_PMINB=1))
+    prm = WignerParams(WNX, WNP, WXA, WPA, WDT, d_theta=WDTH, d_lambda=WDLA, gamma=WGAMMA, potential=WPOT,
+                       dpotential=WDPOT, fp_damping='fabs(p)', constants='exact')
+    X = np.fft.fftshift(np.linspace(-WXA, WXA - 2 * WXA / WNX, WNX))[np.newaxis, :]
+    P = np.fft.fftshift(np.linspace(-WPA, WPA - 2 * WPA / WNP, WNP))[:, np.newaxis]
+    W0 = np.ascontiguousarray(np.exp(-(X - 1.5) ** 2 - (P + 0.5) ** 2 * 1.3) + 0. * 1j)
+    steps = 3
+    fin, fout, fobs = (os.path.join(staged, n) for n in ('w_in.bin', 'w_out.bin', 'w_obs.bin'))
+    W0.tofile(fin)
+    r = subprocess.run([exe, fin, fout, fobs, str(steps)] + [repr(v) for v in (WXA, WPA, WDT, WGAMMA, WDTH, WDLA)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.fromfile(fout, dtype=np.complex128).reshape(WNP, WNX)
+    obs = np.fromfile(fobs).reshape(steps + 1, 11)
+    ref_obs, ref = WignerOracle(prm).run(W0, steps)
+    assert rel_l2(got, ref) < 1e-12
+    scale = np.maximum(np.abs(ref_obs[:, :10]).max(axis=0), 1e-3)
+    assert np.all(np.abs(obs[:, :10] - ref_obs[:, :10]) / scale < 1e-10), (obs - ref_obs) / scale
+    # the negative area (here ~ -4e-5) sums the points below zero: points within rounding of zero
+    # enter one sum and not the other, so it is held to an absolute 1e-12
+    assert np.all(np.abs(obs[:, 10] - ref_obs[:, 10]) < 1e-12), obs[:, 10] - ref_obs[:, 10]
