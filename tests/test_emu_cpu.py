@@ -1,12 +1,12 @@
-"""The complex128 Wigner2D and Dirac2D kernels' device code, executed on the
-host (tests/emu/shim.h: one thread per CUDA thread, real barriers and
+"""The complex128 Wigner2D, Dirac2D and Dirac3D kernels' device code, executed
+on the host (tests/emu/shim.h: one thread per CUDA thread, real barriers and
 shuffles), against the oracle.
 
 It checks the passes' tiling, index arithmetic, partial-sum reductions and the
-launch sequences of wig_run and dirac_run, for the tile shapes the planners
-pick at large grids and others, without a GPU.  The device sources are the
-ones NVRTC compiles for sm_100a; only `extern __shared__` arrays are pointed
-at a host buffer."""
+launch sequences of wig_run, dirac_run and dirac3_run, for the tile shapes the
+planners pick at large grids and others, without a GPU.  The device sources
+are the ones NVRTC compiles for sm_100a; only `extern __shared__` arrays are
+pointed at a host buffer."""
 import os
 import re
 import shutil
@@ -17,12 +17,14 @@ import pytest
 
 from oracle.common import rel_l2
 from oracle.dirac2d import DiracOracle, DiracParams, spinor_particle_spin_up
+from oracle.dirac3d import Dirac3DOracle, Dirac3DParams, spinor_particle_spin_up_3d
 from oracle.wigner2d import WignerOracle, WignerParams
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, 'pywignercuda_b200', 'csrc')
 EMU = os.path.join(ROOT, 'tests', 'emu')
-HEADERS = ('wig_fft.cuh', 'wig_wigner.cuh', 'wig_dirac.cuh', 'wig_jit_dirac.cuh', 'wig_jit_wigner.cuh')
+HEADERS = ('wig_fft.cuh', 'wig_wigner.cuh', 'wig_dirac.cuh', 'wig_jit_dirac.cuh', 'wig_jit_wigner.cuh',
+           'wig_dirac3.cuh', 'wig_jit_dirac3.cuh')
 EXTERN_SHARED = re.compile(r'extern\s+__shared__\s+(\w+)\s+(\w+)\s*\[\s*\]\s*;')
 
 NX, NY = 32, 16
@@ -36,7 +38,7 @@ def stage(dst):
         src = EXTERN_SHARED.sub(lambda m: '%s* %s = reinterpret_cast<%s*>(emu_smem);'
                                 % (m.group(1), m.group(2), m.group(1)), src)
         open(os.path.join(dst, h), 'w').write(src)
-    for f in ('shim.h', 'dirac2d_emu.cpp', 'wigner2d_emu.cpp'):
+    for f in ('shim.h', 'dirac2d_emu.cpp', 'wigner2d_emu.cpp', 'dirac3d_emu.cpp'):
         shutil.copy(os.path.join(EMU, f), dst)
 
 
@@ -115,3 +117,42 @@ def test_wigner2d_device_code_matches_oracle(staged, xrows, xnt, pc, pnt):
     # the negative area (here ~ -4e-5) sums the points below zero: points within rounding of zero
     # enter one sum and not the other, so it is held to an absolute 1e-12
     assert np.all(np.abs(obs[:, 10] - ref_obs[:, 10]) < 1e-12), obs[:, 10] - ref_obs[:, 10]
+
+
+D3 = (32, 16, 16)
+D3A, D3DT = (10., 8., 8.), 1e-3
+# as in tests/emu/dirac3d_emu.cpp
+D3POT = ('-1./sqrt(x*x+y*y+z*z+0.5) + 0.2*t*z', '-0.5*y', '0.5*x', '0.1*z')
+
+
+def d3_threads(n):
+    return max(32, min(256, n)) // 32 * 32
+
+
+# (rows, yc, zc, radix x / y / z, CTA cap): the planner's tiles at 32 x 16 x 16 (radix 16 on z),
+# small tiles with every pass grid-striding over 5 CTAs, and radix 16 on every axis over 3 CTAs
+@pytest.mark.parametrize('rows,yc,zc,xr,yr,zr,cap', [(16, 32, 32, 8, 8, 16, 2368), (2, 4, 2, 8, 8, 16, 5),
+                                                     (16, 32, 32, 16, 16, 16, 3)])
+def test_dirac3d_device_code_matches_oracle(staged, rows, yc, zc, xr, yr, zr, cap):
+    nx, ny, nz = D3
+    exe = build(staged, 'dirac3d_emu.cpp', dict(D3_NX=nx, D3_NY=ny, D3_NZ=nz, D3_ROWS=rows,
+                                                D3_XNT=d3_threads(4 * rows * nx // 8), D3_YC=yc,
+                                                D3_YNT=d3_threads(ny * yc // 8), D3_ZC=zc,
+                                                D3_ZNT=d3_threads(4 * zc * nz // 8), D3_SNT=256, D3_XR=xr,
+                                                D3_YR=yr, D3_ZR=zr, D3_XMB=1, D3_YMB=1, D3_ZMB=1))
+    prm = Dirac3DParams(nx, ny, nz, *D3A, D3DT, mass=1., c=137.036, A0=D3POT[0], A1=D3POT[1], A2=D3POT[2],
+                        A3=D3POT[3], constants='exact')
+    psi0 = spinor_particle_spin_up_3d(prm, (2., 0.5, 1.), lambda x, y, z: np.exp(-(x * x + y * y + z * z) / 4.))
+    psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
+    steps = 3
+    fin, fout, fobs = (os.path.join(staged, n) for n in ('p3_in.bin', 'p3_out.bin', 'p3_obs.bin'))
+    psi0.tofile(fin)
+    r = subprocess.run([exe, fin, fout, fobs, str(steps)] + [repr(v) for v in D3A + (D3DT, 1., 137.036)] +
+                       [str(cap)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.fromfile(fout, dtype=np.complex128).reshape(4, nz, ny, nx)
+    obs = np.fromfile(fobs).reshape(steps, 12)
+    ref_obs, ref = Dirac3DOracle(prm).run(psi0, steps)
+    assert rel_l2(got, ref) < 1e-12
+    scale = np.maximum(np.abs(ref_obs).max(axis=0), 1e-3)
+    assert np.all(np.abs(obs - ref_obs) / scale < 1e-10), (obs - ref_obs) / scale
