@@ -8,10 +8,13 @@
 // the warp.  Block-scope `__shared__` arrays become function statics (one copy,
 // seen by every thread of the running block); `extern __shared__` arrays are
 // rewritten by the test harness to point into emu_smem.  Math functions are
-// the host C library's.
+// the host C library's.  Blocks running one after another, a persistent
+// kernel's first block drains its work list and the others draw only the
+// overflowing tickets.
 #pragma once
 #include <math.h>
 
+#include <atomic>
 #include <barrier>
 #include <cstdio>
 #include <cstdlib>
@@ -61,6 +64,17 @@ inline double __shfl_xor_sync(unsigned, double v, int lane_mask) {
 }
 
 template <class T> inline T __ldg(const T* p) { return *p; }
+template <class T> inline T __ldcg(const T* p) { return *p; }
+
+inline unsigned atomicAdd(unsigned* p, unsigned v) { return std::atomic_ref<unsigned>(*p).fetch_add(v); }
+inline void __threadfence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
+
+// sin / cos of pi x, evaluated in double and rounded once
+inline void sincospif(float x, float* s, float* c) {
+  const double a = 3.141592653589793238462643383279502884 * (double)x;
+  *s = (float)::sin(a);
+  *c = (float)::cos(a);
+}
 
 // grid x block threads; block b's threads run concurrently, blocks in turn
 inline void emu_launch(unsigned grid, unsigned block, const std::function<void()>& body) {

@@ -19,12 +19,13 @@ from oracle.common import rel_l2
 from oracle.dirac2d import DiracOracle, DiracParams, spinor_particle_spin_up
 from oracle.dirac3d import Dirac3DOracle, Dirac3DParams, spinor_particle_spin_up_3d
 from oracle.wigner2d import WignerOracle, WignerParams
+from batch_cases import random_batch, to_params, initial_state
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, 'pywignercuda_b200', 'csrc')
 EMU = os.path.join(ROOT, 'tests', 'emu')
 HEADERS = ('wig_fft.cuh', 'wig_wigner.cuh', 'wig_dirac.cuh', 'wig_jit_dirac.cuh', 'wig_jit_wigner.cuh',
-           'wig_dirac3.cuh', 'wig_jit_dirac3.cuh')
+           'wig_dirac3.cuh', 'wig_jit_dirac3.cuh', 'wig_rfft.cuh', 'wig_batch.cuh', 'wig_jit_batch.cuh')
 EXTERN_SHARED = re.compile(r'extern\s+__shared__\s+(\w+)\s+(\w+)\s*\[\s*\]\s*;')
 
 NX, NY = 32, 16
@@ -38,14 +39,15 @@ def stage(dst):
         src = EXTERN_SHARED.sub(lambda m: '%s* %s = reinterpret_cast<%s*>(emu_smem);'
                                 % (m.group(1), m.group(2), m.group(1)), src)
         open(os.path.join(dst, h), 'w').write(src)
-    for f in ('shim.h', 'dirac2d_emu.cpp', 'wigner2d_emu.cpp', 'dirac3d_emu.cpp'):
+    for f in ('shim.h', 'dirac2d_emu.cpp', 'wigner2d_emu.cpp', 'dirac3d_emu.cpp', 'batch_emu.cpp'):
         shutil.copy(os.path.join(EMU, f), dst)
 
 
 def build(dst, source, macros):
-    exe = os.path.join(dst, source.split('.')[0] + ''.join('_%d' % v for v in macros.values()))
+    tag = ''.join('_%s' % re.sub(r'\W', '', str(v)) for v in macros.values())
+    exe = os.path.join(dst, source.split('.')[0] + tag)
     cmd = (['g++', '-std=c++20', '-O1', '-pthread', '-w', '-I', dst] +
-           ['-D%s=%d' % kv for kv in macros.items()] + [os.path.join(dst, source), '-o', exe])
+           ['-D%s=%s' % kv for kv in macros.items()] + [os.path.join(dst, source), '-o', exe])
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
     return exe
@@ -156,3 +158,40 @@ def test_dirac3d_device_code_matches_oracle(staged, rows, yc, zc, xr, yr, zr, ca
     assert rel_l2(got, ref) < 1e-12
     scale = np.maximum(np.abs(ref_obs).max(axis=0), 1e-3)
     assert np.all(np.abs(obs - ref_obs) / scale < 1e-10), (obs - ref_obs) / scale
+
+
+# instances of the batched FP32 form: mixed square grids, one undamped
+BSIZES = (64, 128, 128, 64)
+
+
+@pytest.mark.parametrize('warps,grid', [(4, 3), (2, 5)])
+def test_batch_device_code_matches_oracle(staged, warps, grid):
+    """The FP32 real-storage passes (two rows / columns per complex transform, the
+    Nyquist split), the persistent work lists and the last-CTA normalisation,
+    against the FP64 oracle at FP32 accuracy, 6 steps (each emulated step costs
+    seconds of barrier traffic)."""
+    exe = build(staged, 'batch_emu.cpp', {'WIGB_WARPS': warps, 'WIGB_XMINB': 1, 'WIGB_PMINB': 1,
+                                          'WIGB_CASES(F)': 'F(64) F(128)'})
+    cases = random_batch(list(BSIZES), seed=11)
+    cases[2]['gamma'] = 0.
+    steps, dt = 6, 0.005
+    prm = np.array([[c['n'], c['a'], c['b'], c['gamma'], c['gamma'], dt, 10.] for c in cases], dtype=np.float64)
+    W0 = [initial_state(c) for c in cases]
+    packed = np.concatenate([w.real.astype(np.float32).ravel() for w in W0]).astype(np.complex64)
+    fprm, fin, fout, fobs = (os.path.join(staged, n) for n in ('b_prm.bin', 'b_in.bin', 'b_out.bin', 'b_obs.bin'))
+    prm.tofile(fprm)
+    packed.tofile(fin)
+    r = subprocess.run([exe, fprm, fin, fout, fobs, str(steps), str(grid)], capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = np.fromfile(fout, dtype=np.complex64)
+    obs = np.fromfile(fobs).reshape(len(cases), steps + 1, 11)
+    off = 0
+    for i, c in enumerate(cases):
+        n = c['n']
+        W = out[off:off + n * n].reshape(n, n)
+        off += n * n
+        ref_obs, ref = WignerOracle(to_params(c)).run(W0[i], steps)
+        assert rel_l2(W, ref) < 2e-6, (i, rel_l2(W, ref))
+        assert np.max(np.abs(obs[i, :, 0] - ref_obs[:, 0])) < (1e-6 if c['gamma'] else 2e-8 * steps), i
+        assert np.max(np.abs(obs[i, :, 1:10] - ref_obs[:, 1:10])) < 1e-4, i
