@@ -584,6 +584,9 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   double* lam_d = nullptr;
   if (!rc) rc = B.alloc(&lam_d, NX, lt.data());
   if (!rc && h->odm) rc = B.alloc(&h->odm_T, 5 * (size_t)NX * NP);
+  // ODM steps do not keep sum W real: the samples need the imaginary moment sums too
+  double* part_im_d = nullptr;
+  if (!rc && h->odm) rc = B.alloc(&part_im_d, (size_t)nparts * wig::NIM);
   double* rth_d = nullptr;
   if (!rc) rc = B.alloc(&rth_d, NP);
   if (!rc && h->gp) rc = B.alloc(&h->gp_chunks, (size_t)h->n_chunks * NX);
@@ -604,7 +607,7 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   h->odm_coef[1] = d->dt * 2 * d->gamma * d->weight2 / 1. * (1.0 / (double)NP);
   a.x_tab = x_d; a.p_tab = p_d; a.dV_tab = dv_d; a.V0_tab = v0_d; a.theta_s = ths_d;
   a.r_lambda = rl_d; a.r_theta = rt_d; a.mask1 = m1_d; a.mask2s = m2_d; a.sfp = sfp_d;
-  a.tw_x = twx_d; a.tw_p = twp_d; a.partials = part_d; a.n_partials = 0;
+  a.tw_x = twx_d; a.tw_p = twp_d; a.partials = part_d; a.partials_im = part_im_d; a.n_partials = 0;
   {
     void* args[] = {&a, &rl_d, &rt_d, &m1_d, &m2_d, &sfp_d, &rth_d};
     rc = launch(f_setup, 8, 256, 0, 0, args);

@@ -35,6 +35,7 @@ namespace wig {
 
 constexpr int NACC = 12;   // sumRe, sumIm, x, x^2, p, p^2, xp, V', pV', xV', H, negative
 constexpr int NOBS = 11;   // norm, x, x^2, p, p^2, xp, V', pV', xV', H, negative area
+constexpr int NIM = 10;    // imaginary parts of the sums of observables 1..10
 
 struct WigArgs {
   // kernel constants exactly as the reference's kernels see them
@@ -59,6 +60,9 @@ struct WigArgs {
   const double2* tw_x;     // [n_x] exp(-2 pi i m / n_x)
   const double2* tw_p;     // [n_p]
   double* partials;        // [n_cta][NACC]
+  // [n_cta][NIM] imaginary parts of the moment sums, written with `partials` by the passes of
+  // plans whose steps do not keep sum W real (ODM damping); null otherwise
+  double* partials_im;
   int n_partials;          // CTAs that wrote `partials`
   // ODM Lindblad damping (SetA_ODM :1206-1244, _Lindbladian_ODM :1516-1634), exact host values
   const double* lambda_tab; // [n_x] exact shifted Lambda
@@ -129,13 +133,26 @@ __device__ __forceinline__ double2 consume_partials(const WigArgs& a, int mode, 
   double2 s = make_double2(1., 0.);
   if (mode == 1) s = crecip(make_double2(S.x * a.dX * a.dP, S.y * a.dX * a.dP));
   else if (mode == 2) { const double d = a.dX * a.dP; s = crecip(make_double2(S.x * d, S.y * d)); }
-  if (obs_row && threadIdx.x < NOBS) {
-    const double dXdP = a.dX * a.dP;
-    double val;
-    if (threadIdx.x == 0) val = (s.x * S.x - s.y * S.y) * dXdP;
-    else val = s.x * (dXdP * red[0][threadIdx.x + 1]);
-    obs_row[threadIdx.x] = val;
+  const double dXdP = a.dX * a.dP;
+  double val = 0.;
+  if (obs_row && threadIdx.x < NOBS)
+    val = threadIdx.x == 0 ? (s.x * S.x - s.y * S.y) * dXdP : s.x * (dXdP * red[0][threadIdx.x + 1]);
+  if (obs_row && a.partials_im) {
+    // the reference takes the observables of the normalised complex W: Re(s Z) = s.x Re Z - s.y Im Z
+    // for each moment sum Z (the s.y term matters where the step does not keep sum W real)
+    __syncthreads();   // every thread has read red[0][] before block_sum rewrites it
+    double im[NACC];
+#pragma unroll
+    for (int v = 0; v < NACC; ++v) im[v] = 0.;
+    for (int i = threadIdx.x; i < a.n_partials; i += NT) {
+      const double* q = a.partials_im + (size_t)i * NIM;
+#pragma unroll
+      for (int v = 0; v < NIM; ++v) im[v] += q[v];
+    }
+    block_sum<NT, NACC>(im, red);
+    if (threadIdx.x >= 1 && threadIdx.x < NOBS) val -= s.y * (dXdP * red[0][threadIdx.x - 1]);
   }
+  if (obs_row && threadIdx.x < NOBS) obs_row[threadIdx.x] = val;
   __syncthreads();   // red[] is reused by the caller
   return s;
 }
@@ -157,21 +174,48 @@ __device__ __forceinline__ void accumulate_obs(double (&acc)[NACC], double2 v, d
   acc[11] += (w < 0.) ? w : 0.;
 }
 
+// Imaginary parts of the moment sums of accumulate_obs (slots 2..11 there, 0..9 here).
+__device__ __forceinline__ void accumulate_obs_im(double (&im)[NACC], double2 v, double x, double p,
+                                                  double dV, double V0, double mass_exact) {
+  const double u = v.y;
+  im[0] += u * x;
+  im[1] += u * (x * x);
+  im[2] += u * p;
+  im[3] += u * (p * p);
+  im[4] += u * (p * x);
+  im[5] += u * dV;
+  im[6] += u * (p * dV);
+  im[7] += u * (dV * x);
+  im[8] += u * ((p * p) / (2. * mass_exact) + V0);
+  im[9] += (v.x < 0.) ? u : 0.;
+}
+
+// The CTA's imaginary moment sums into a.partials_im (after the real ones have been stored).
+template <int NT>
+__device__ __forceinline__ void store_partials_im(const WigArgs& a, double (&im)[NACC], double (*red)[NACC]) {
+  __syncthreads();   // the real sums have been read out of red[0][]
+  block_sum<NT, NACC>(im, red);
+  if (threadIdx.x < NIM) a.partials_im[(size_t)blockIdx.x * NIM + threadIdx.x] = red[0][threadIdx.x];
+}
+
 // ------------------------------------------------------------------ kernels
 // Partial sums over the whole grid (initial state, or any state): grid-stride.
 template <int NX, int NP, int NT>
 __device__ __forceinline__ void reduce_body(const WigArgs& a, const double2* __restrict__ W,
                                             double* __restrict__ partials) {
   __shared__ double red[NT / 32][NACC];
-  double acc[NACC];
+  double acc[NACC], im[NACC];
 #pragma unroll
-  for (int v = 0; v < NACC; ++v) acc[v] = 0.;
+  for (int v = 0; v < NACC; ++v) acc[v] = im[v] = 0.;
+  const bool with_im = a.partials_im != nullptr;
   for (int e = blockIdx.x * NT + threadIdx.x; e < NX * NP; e += gridDim.x * NT) {
     const int i = e / NX, j = e - i * NX;
     accumulate_obs(acc, W[e], a.x_tab[j], a.p_tab[i], a.dV_tab[j], a.V0_tab[j], a.mass_exact);
+    if (with_im) accumulate_obs_im(im, W[e], a.x_tab[j], a.p_tab[i], a.dV_tab[j], a.V0_tab[j], a.mass_exact);
   }
   block_sum<NT, NACC>(acc, red);
   if (threadIdx.x < NACC) partials[(size_t)blockIdx.x * NACC + threadIdx.x] = red[0][threadIdx.x];
+  if (with_im) store_partials_im<NT>(a, im, red);
 }
 
 // One CTA: the last sample's observables and the final scale.
@@ -675,9 +719,10 @@ __device__ __forceinline__ void odm_ppass_body(const WigArgs& a, double2* __rest
     __syncthreads();
   }
   cta_fft<double2, NP, C, NT, true, M>(Acc, a.tw_p);
-  double acc[NACC];
+  double acc[NACC], im[NACC];
 #pragma unroll
-  for (int v = 0; v < NACC; ++v) acc[v] = 0.;
+  for (int v = 0; v < NACC; ++v) acc[v] = im[v] = 0.;
+  const bool with_im = a.partials_im != nullptr;
   for (int e = threadIdx.x; e < C * NP; e += NT) {
     const int k = e / C, c = e - k * C;
     const int col = col0 + c;
@@ -685,9 +730,11 @@ __device__ __forceinline__ void odm_ppass_body(const WigArgs& a, double2* __rest
     const double2 v = cadd(W[g], cscale(Acc[pad8(e)], coef));
     W[g] = v;
     accumulate_obs(acc, v, a.x_tab[col], a.p_tab[k], a.dV_tab[col], a.V0_tab[col], a.mass_exact);
+    if (with_im) accumulate_obs_im(im, v, a.x_tab[col], a.p_tab[k], a.dV_tab[col], a.V0_tab[col], a.mass_exact);
   }
   block_sum<NT, NACC>(acc, red);
   if (threadIdx.x < NACC) a.partials[(size_t)blockIdx.x * NACC + threadIdx.x] = red[0][threadIdx.x];
+  if (with_im) store_partials_im<NT>(a, im, red);
 }
 
 }  // namespace wig

@@ -1,10 +1,11 @@
 // Host execution of the complex128 Wigner2D kernels (csrc/wig_jit_wigner.cuh)
-// in the launch sequence of wig_run for a Lie-split Caldeira-Leggett plan
+// in the launch sequence of wig_run for a Lie-split plan with Caldeira-Leggett
+// (WIG_DAMP 1) or first-order ODM Lindblad damping (WIG_DAMP 0, odm 1)
 // (csrc/wig_capi.cu: wig_run_begin / wig_run_step / wig_run_end), with the tile
 // macros WIG_* given on the command line.  Test infrastructure:
 // tests/test_emu_cpu.py builds it and compares the result with the oracle.
 //
-//   wigner2d_emu W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda
+//   wigner2d_emu W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda odm
 //
 // W_in / W_out: (WIG_NP, WIG_NX) complex128; obs_out: (n_prop + 1) x 11
 // doubles.  hbar = mass = 1, constants used exactly.  The expressions are
@@ -71,15 +72,16 @@ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 11) {
-    std::fprintf(stderr, "usage: %s W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda\n", argv[0]);
+  if (argc != 12) {
+    std::fprintf(stderr, "usage: %s W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda odm\n", argv[0]);
     return 2;
   }
   constexpr int NX = WIG_NX, NP = WIG_NP, NOBS = 11;
   const long n_prop = std::atol(argv[4]);
   const double xa = std::atof(argv[5]), pa = std::atof(argv[6]);
   const double gamma = std::atof(argv[8]);
-  if (n_prop < 1 || NP % WIG_XROWS != 0 || NX % WIG_PC != 0) return 2;
+  const int odm = std::atoi(argv[11]);
+  if (n_prop < 1 || NP % WIG_XROWS != 0 || NX % WIG_PC != 0 || (odm != 0) != (WIG_DAMP == 0)) return 2;
   dt = std::atof(argv[7]);
   D_Theta = std::atof(argv[9]);
   D_Lambda = std::atof(argv[10]);
@@ -121,15 +123,19 @@ int main(int argc, char** argv) {
   std::vector<double2> twx = twiddles(NX), twp = twiddles(NP);
   std::vector<double> rl(NX), rt(NP), m1(NX), m2(NX), sfp(NP), rth(NP);
   const int nparts = n_cta_x > n_cta_p ? (n_cta_x > n_cta_r ? n_cta_x : n_cta_r) : (n_cta_p > n_cta_r ? n_cta_p : n_cta_r);
-  std::vector<double> partials((size_t)nparts * wig::NACC, 0.);
+  std::vector<double> partials((size_t)nparts * wig::NACC, 0.), partials_im(odm ? (size_t)nparts * wig::NIM : 0, 0.);
   std::vector<double> obs((size_t)(n_prop + 1) * NOBS, 0.);
   double2 scale{1., 0.};
   a.x_tab = xt.data(); a.p_tab = pt.data(); a.dV_tab = dv.data(); a.V0_tab = v0.data(); a.theta_s = ths.data();
   a.r_lambda = rl.data(); a.r_theta = rt.data(); a.mask1 = m1.data(); a.mask2s = m2.data(); a.sfp = sfp.data();
   a.tw_x = twx.data(); a.tw_p = twp.data(); a.partials = partials.data(); a.n_partials = 0;
+  a.partials_im = odm ? partials_im.data() : nullptr;   // as wig_create: ODM plans only
   a.lambda_tab = lt.data(); a.hbar_exact = hBar; a.L_material = 1.;
   a.r_theta_half = rth.data();
   emu_launch(1, 64, [&] { wig_setup(a, rl.data(), rt.data(), m1.data(), m2.data(), sfp.data(), rth.data()); });
+  // Lindbladian_ODM_Order1 (weight 1, sign 1): scale dt 2 gamma / n_p, five intermediate planes
+  const double odm_coef = dt * 2 * gamma * 1. / 1. * (1.0 / (double)NP);
+  std::vector<double2> T(odm ? 5 * npts : 0);
 
   double2* Wp = W.data();
   // wig_run_begin: partial sums of W for the initial normalisation and sample 0
@@ -143,6 +149,10 @@ int main(int argc, char** argv) {
     emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, mode, orow); });
     const double t = (double)n * dt;
     emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass(a, Wp, t); });
+    if (odm) {
+      emu_launch(n_cta_x, WIG_XNT, [&] { wig_odm_xpass(a, Wp, T.data()); });
+      emu_launch(n_cta_p, WIG_PNT, [&] { wig_odm_ppass(a, Wp, T.data(), odm_coef, 1.); });
+    }
     a.n_partials = n_cta_p;
   }
   // wig_run_end

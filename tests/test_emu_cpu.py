@@ -93,29 +93,32 @@ WPOT, WDPOT = '0.05*pow(x,4) - pow(x,2) + 0.2*x*sin(3.*t)', '0.2*pow(x,3) - 2.*x
 
 
 # (rows, x threads, columns, p threads) per CTA: the planner's rule at 64 x 32 (one CTA per pass),
-# one row per 128-thread CTA as for 1024-point rows, and several small CTAs per pass
-@pytest.mark.parametrize('xrows,xnt,pc,pnt', [(32, 256, 64, 256), (1, 128, 2, 32), (4, 32, 8, 32)])
-def test_wigner2d_device_code_matches_oracle(staged, xrows, xnt, pc, pnt):
+# one row per 128-thread CTA as for 1024-point rows, and several small CTAs per pass; Caldeira-Leggett,
+# and ODM Lindblad damping (first order) on two of the shapes
+@pytest.mark.parametrize('xrows,xnt,pc,pnt,odm', [(32, 256, 64, 256, 0), (1, 128, 2, 32, 0), (4, 32, 8, 32, 0),
+                                                  (32, 256, 64, 256, 1), (4, 32, 8, 32, 1)])
+def test_wigner2d_device_code_matches_oracle(staged, xrows, xnt, pc, pnt, odm):
     exe = build(staged, 'wigner2d_emu.cpp', dict(WIG_NX=WNX, WIG_NP=WNP, WIG_XROWS=xrows, WIG_XNT=xnt,
-                                                 WIG_KIN_STRING=0, WIG_PC=pc, WIG_PNT=pnt, WIG_DAMP=1,
+                                                 WIG_KIN_STRING=0, WIG_PC=pc, WIG_PNT=pnt, WIG_DAMP=1 - odm,
                                                  WIG_RNT=256, WIG_XMINB=1, WIG_PMINB=1))
     prm = WignerParams(WNX, WNP, WXA, WPA, WDT, d_theta=WDTH, d_lambda=WDLA, gamma=WGAMMA, potential=WPOT,
-                       dpotential=WDPOT, fp_damping='fabs(p)', constants='exact')
+                       dpotential=WDPOT, damping='ODM' if odm else 'CaldeiraLeggett', fp_damping='fabs(p)',
+                       L_material=1., constants='exact')
     X = np.fft.fftshift(np.linspace(-WXA, WXA - 2 * WXA / WNX, WNX))[np.newaxis, :]
     P = np.fft.fftshift(np.linspace(-WPA, WPA - 2 * WPA / WNP, WNP))[:, np.newaxis]
     W0 = np.ascontiguousarray(np.exp(-(X - 1.5) ** 2 - (P + 0.5) ** 2 * 1.3) + 0. * 1j)
     steps = 3
     fin, fout, fobs = (os.path.join(staged, n) for n in ('w_in.bin', 'w_out.bin', 'w_obs.bin'))
     W0.tofile(fin)
-    r = subprocess.run([exe, fin, fout, fobs, str(steps)] + [repr(v) for v in (WXA, WPA, WDT, WGAMMA, WDTH, WDLA)],
-                       capture_output=True, text=True, timeout=600)
+    r = subprocess.run([exe, fin, fout, fobs, str(steps)] + [repr(v) for v in (WXA, WPA, WDT, WGAMMA, WDTH, WDLA)] +
+                       [str(odm)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     got = np.fromfile(fout, dtype=np.complex128).reshape(WNP, WNX)
     obs = np.fromfile(fobs).reshape(steps + 1, 11)
     ref_obs, ref = WignerOracle(prm).run(W0, steps)
     assert rel_l2(got, ref) < 1e-12
     scale = np.maximum(np.abs(ref_obs[:, :10]).max(axis=0), 1e-3)
-    assert np.all(np.abs(obs[:, :10] - ref_obs[:, :10]) / scale < 1e-10), (obs - ref_obs) / scale
+    assert np.all(np.abs(obs[:, :10] - ref_obs[:, :10]) / scale < 1e-10), (obs[:, :10] - ref_obs[:, :10]) / scale
     # the negative area (here ~ -4e-5) sums the points below zero: points within rounding of zero
     # enter one sum and not the other, so it is held to an absolute 1e-12
     assert np.all(np.abs(obs[:, 10] - ref_obs[:, 10]) < 1e-12), obs[:, 10] - ref_obs[:, 10]
