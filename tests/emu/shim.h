@@ -76,27 +76,32 @@ inline void sincospif(float x, float* s, float* c) {
   *c = (float)::cos(a);
 }
 
-// grid x block threads; block b's threads run concurrently, blocks in turn
-inline void emu_launch(unsigned grid, unsigned block, const std::function<void()>& body) {
+// (grid_x, grid_y) x block threads; a block's threads run concurrently, blocks in turn
+inline void emu_launch2d(unsigned grid_x, unsigned grid_y, unsigned block, const std::function<void()>& body) {
   if (block == 0 || block > 1024 || (block % 32) != 0) {
     std::fprintf(stderr, "emu_launch: block of %u threads\n", block);
     std::exit(3);
   }
-  gridDim = {grid, 1, 1};
+  gridDim = {grid_x, grid_y, 1};
   blockDim = {block, 1, 1};
-  for (unsigned b = 0; b < grid; ++b) {
-    std::barrier<> bar((std::ptrdiff_t)block);
-    emu_block_barrier = &bar;
-    emu_warp_barriers.clear();
-    for (unsigned w = 0; w < block / 32; ++w) emu_warp_barriers.emplace_back(new std::barrier<>(32));
-    std::vector<std::thread> threads;
-    threads.reserve(block);
-    for (unsigned t = 0; t < block; ++t)
-      threads.emplace_back([&body, t, b] {
-        threadIdx = {t, 0, 0};
-        blockIdx = {b, 0, 0};
-        body();
-      });
-    for (auto& th : threads) th.join();
-  }
+  for (unsigned by = 0; by < grid_y; ++by)
+    for (unsigned bx = 0; bx < grid_x; ++bx) {
+      std::barrier<> bar((std::ptrdiff_t)block);
+      emu_block_barrier = &bar;
+      emu_warp_barriers.clear();
+      for (unsigned w = 0; w < block / 32; ++w) emu_warp_barriers.emplace_back(new std::barrier<>(32));
+      std::vector<std::thread> threads;
+      threads.reserve(block);
+      for (unsigned t = 0; t < block; ++t)
+        threads.emplace_back([&body, t, bx, by] {
+          threadIdx = {t, 0, 0};
+          blockIdx = {bx, by, 0};
+          body();
+        });
+      for (auto& th : threads) th.join();
+    }
+}
+
+inline void emu_launch(unsigned grid, unsigned block, const std::function<void()>& body) {
+  emu_launch2d(grid, 1, block, body);
 }

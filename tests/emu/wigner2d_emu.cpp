@@ -1,15 +1,17 @@
 // Host execution of the complex128 Wigner2D kernels (csrc/wig_jit_wigner.cuh)
-// in the launch sequence of wig_run for a Lie-split plan with Caldeira-Leggett
-// (WIG_DAMP 1) or first-order ODM Lindblad damping (WIG_DAMP 0, odm 1)
-// (csrc/wig_capi.cu: wig_run_begin / wig_run_step / wig_run_end), with the tile
-// macros WIG_* given on the command line.  Test infrastructure:
+// in the launch sequence of wig_run for a plan with Caldeira-Leggett (WIG_DAMP 1)
+// or first-order ODM Lindblad damping (WIG_DAMP 0, odm 1), Lie-split or, with
+// WIG_STRANG 1, the Strang / Gross-Pitaevskii step (csrc/wig_capi.cu:
+// wig_run_begin / wig_run_step / wig_run_step_strang / wig_run_end), with the
+// tile macros WIG_* given on the command line.  Test infrastructure:
 // tests/test_emu_cpu.py builds it and compares the result with the oracle.
 //
-//   wigner2d_emu W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda odm
+//   wigner2d_emu W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda odm a_gp
 //
 // W_in / W_out: (WIG_NP, WIG_NX) complex128; obs_out: (n_prop + 1) x 11
-// doubles.  hbar = mass = 1, constants used exactly.  The expressions are
-// fixed here and restated by the test for the oracle.
+// doubles, then (Strang) n_prop values of sum P(x)^2 dx.  hbar = mass = 1,
+// constants used exactly.  The expressions are fixed here and restated by the
+// test for the oracle.
 #include "shim.h"
 
 #define __constant__
@@ -72,8 +74,9 @@ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 12) {
-    std::fprintf(stderr, "usage: %s W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda odm\n", argv[0]);
+  if (argc != 13) {
+    std::fprintf(stderr, "usage: %s W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda odm a_gp\n",
+                 argv[0]);
     return 2;
   }
   constexpr int NX = WIG_NX, NP = WIG_NP, NOBS = 11;
@@ -81,6 +84,7 @@ int main(int argc, char** argv) {
   const double xa = std::atof(argv[5]), pa = std::atof(argv[6]);
   const double gamma = std::atof(argv[8]);
   const int odm = std::atoi(argv[11]);
+  const double a_gp = std::atof(argv[12]);
   if (n_prop < 1 || NP % WIG_XROWS != 0 || NX % WIG_PC != 0 || (odm != 0) != (WIG_DAMP == 0)) return 2;
   dt = std::atof(argv[7]);
   D_Theta = std::atof(argv[9]);
@@ -132,6 +136,7 @@ int main(int argc, char** argv) {
   a.partials_im = odm ? partials_im.data() : nullptr;   // as wig_create: ODM plans only
   a.lambda_tab = lt.data(); a.hbar_exact = hBar; a.L_material = 1.;
   a.r_theta_half = rth.data();
+  a.gp_coef = a_gp;
   emu_launch(1, 64, [&] { wig_setup(a, rl.data(), rt.data(), m1.data(), m2.data(), sfp.data(), rth.data()); });
   // Lindbladian_ODM_Order1 (weight 1, sign 1): scale dt 2 gamma / n_p, five intermediate planes
   const double odm_coef = dt * 2 * gamma * 1. / 1. * (1.0 / (double)NP);
@@ -143,12 +148,33 @@ int main(int argc, char** argv) {
   a.n_partials = n_cta_r;
   // wig_run_step (first call of a run: normalise on load; damped steps renormalise)
   const bool damped = gamma != 0.;
+#if WIG_STRANG
+  // wig_gp_terms: column sums over 16-row chunks, the marginal, the per-row phase
+  const int gp = a_gp != 0.;
+  const int gcnt = NX < 256 ? NX : 256, n_chunks = NP / 16;
+  std::vector<double2> chunks((size_t)n_chunks * NX);
+  std::vector<double> Px(NX), phase(npts), psq(n_prop, 0.);
+  auto gp_terms = [&](int scale_mode, double* psq_out) {
+    emu_launch2d(NX / gcnt, NP / 16, gcnt, [&] { wig_gp_colsum(Wp, chunks.data()); });
+    emu_launch(1, 256, [&] { wig_gp_marginal(a, chunks.data(), n_chunks, scale_mode, Px.data(), psq_out); });
+    emu_launch(n_cta_x, WIG_XNT, [&] { wig_gp_phase(a, Px.data(), phase.data()); });
+  };
+  const double* gph = gp ? phase.data() : nullptr;
+#endif
   for (long n = 0; n < n_prop; ++n) {
     const int mode = (n == 0) ? 1 : (damped ? 2 : 0);
     double* orow = obs.data() + (size_t)n * NOBS;
-    emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, mode, orow); });
     const double t = (double)n * dt;
+#if WIG_STRANG
+    if (gp) gp_terms(mode, nullptr);
+    emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass_half(a, Wp, t, mode, orow, gph); });
+    emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, 0, nullptr); });
+    if (gp) gp_terms(0, psq.data() + n);
+    emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass_half_final(a, Wp, t, gph); });
+#else
+    emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, mode, orow); });
     emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass(a, Wp, t); });
+#endif
     if (odm) {
       emu_launch(n_cta_x, WIG_XNT, [&] { wig_odm_xpass(a, Wp, T.data()); });
       emu_launch(n_cta_p, WIG_PNT, [&] { wig_odm_ppass(a, Wp, T.data(), odm_coef, 1.); });
@@ -166,6 +192,9 @@ int main(int argc, char** argv) {
     }
   }
   if (!write_all(argv[2], W.data(), npts * sizeof(double2))) return 4;
+#if WIG_STRANG
+  obs.insert(obs.end(), psq.begin(), psq.end());
+#endif
   if (!write_all(argv[3], obs.data(), obs.size() * sizeof(double))) return 4;
   return 0;
 }

@@ -111,7 +111,7 @@ def test_wigner2d_device_code_matches_oracle(staged, xrows, xnt, pc, pnt, odm):
     fin, fout, fobs = (os.path.join(staged, n) for n in ('w_in.bin', 'w_out.bin', 'w_obs.bin'))
     W0.tofile(fin)
     r = subprocess.run([exe, fin, fout, fobs, str(steps)] + [repr(v) for v in (WXA, WPA, WDT, WGAMMA, WDTH, WDLA)] +
-                       [str(odm)], capture_output=True, text=True, timeout=600)
+                       [str(odm), '0.'], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     got = np.fromfile(fout, dtype=np.complex128).reshape(WNP, WNX)
     obs = np.fromfile(fobs).reshape(steps + 1, 11)
@@ -122,6 +122,39 @@ def test_wigner2d_device_code_matches_oracle(staged, xrows, xnt, pc, pnt, odm):
     # the negative area (here ~ -4e-5) sums the points below zero: points within rounding of zero
     # enter one sum and not the other, so it is held to an absolute 1e-12
     assert np.all(np.abs(obs[:, 10] - ref_obs[:, 10]) < 1e-12), obs[:, 10] - ref_obs[:, 10]
+
+
+# Strang splitting with the Gross-Pitaevskii mean-field term (GPU_Wigner2D_GPitaevskii): with
+# Caldeira-Leggett, and with ODM damping on the planner's tile and on small CTAs
+@pytest.mark.parametrize('xrows,xnt,pc,pnt,odm,a_gp', [(32, 256, 64, 256, 0, 0.5), (32, 256, 64, 256, 1, -0.3),
+                                                       (4, 32, 8, 32, 1, -0.3)])
+def test_strang_gp_device_code_matches_oracle(staged, xrows, xnt, pc, pnt, odm, a_gp):
+    from oracle.gpitaevskii import GPitaevskiiOracle
+    exe = build(staged, 'wigner2d_emu.cpp', dict(WIG_NX=WNX, WIG_NP=WNP, WIG_XROWS=xrows, WIG_XNT=xnt,
+                                                 WIG_KIN_STRING=1, WIG_PC=pc, WIG_PNT=pnt, WIG_DAMP=1 - odm,
+                                                 WIG_RNT=256, WIG_XMINB=1, WIG_PMINB=1, WIG_STRANG=1))
+    prm = WignerParams(WNX, WNP, WXA, WPA, WDT, d_theta=WDTH, d_lambda=WDLA, gamma=WGAMMA, potential=WPOT,
+                       dpotential=WDPOT, kinetic='0.5*p*p', damping='ODM' if odm else 'CaldeiraLeggett',
+                       fp_damping='fabs(p)', L_material=1., constants='exact')
+    X = np.fft.fftshift(np.linspace(-WXA, WXA - 2 * WXA / WNX, WNX))[np.newaxis, :]
+    P = np.fft.fftshift(np.linspace(-WPA, WPA - 2 * WPA / WNP, WNP))[:, np.newaxis]
+    W0 = np.ascontiguousarray(np.exp(-(X - 1.5) ** 2 - (P + 0.5) ** 2 * 1.3) + 0. * 1j)
+    steps = 3
+    fin, fout, fobs = (os.path.join(staged, n) for n in ('g_in.bin', 'g_out.bin', 'g_obs.bin'))
+    W0.tofile(fin)
+    r = subprocess.run([exe, fin, fout, fobs, str(steps)] + [repr(v) for v in (WXA, WPA, WDT, WGAMMA, WDTH, WDLA)] +
+                       [str(odm), repr(a_gp)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.fromfile(fout, dtype=np.complex128).reshape(WNP, WNX)
+    raw = np.fromfile(fobs)
+    obs, psq = raw[:(steps + 1) * 11].reshape(steps + 1, 11), raw[(steps + 1) * 11:]
+    ref_obs, ref, ref_psq = GPitaevskiiOracle(prm, a_gp).run(W0, steps)
+    assert rel_l2(got, ref) < 1e-12
+    # row 0 is the initial state's sample, row n + 1 the state after step n (the oracle's row n)
+    scale = np.maximum(np.abs(ref_obs[:, :10]).max(axis=0), 1e-3)
+    assert np.all(np.abs(obs[1:, :10] - ref_obs[:, :10]) / scale < 1e-10), (obs[1:, :10] - ref_obs[:, :10]) / scale
+    assert np.all(np.abs(obs[1:, 10] - ref_obs[:, 10]) < 1e-12)
+    assert np.max(np.abs(psq - ref_psq) / np.abs(ref_psq)) < 1e-10
 
 
 D3 = (32, 16, 16)
