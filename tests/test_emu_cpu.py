@@ -25,7 +25,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, 'pywignercuda_b200', 'csrc')
 EMU = os.path.join(ROOT, 'tests', 'emu')
 HEADERS = ('wig_fft.cuh', 'wig_wigner.cuh', 'wig_dirac.cuh', 'wig_jit_dirac.cuh', 'wig_jit_wigner.cuh',
-           'wig_dirac3.cuh', 'wig_jit_dirac3.cuh', 'wig_rfft.cuh', 'wig_batch.cuh', 'wig_jit_batch.cuh')
+           'wig_dirac3.cuh', 'wig_jit_dirac3.cuh', 'wig_rfft.cuh', 'wig_batch.cuh', 'wig_jit_batch.cuh',
+           'wig_adjoint.cuh', 'wig_jit_adjoint.cuh')
 EXTERN_SHARED = re.compile(r'extern\s+__shared__\s+(\w+)\s+(\w+)\s*\[\s*\]\s*;')
 
 NX, NY = 32, 16
@@ -39,7 +40,7 @@ def stage(dst):
         src = EXTERN_SHARED.sub(lambda m: '%s* %s = reinterpret_cast<%s*>(emu_smem);'
                                 % (m.group(1), m.group(2), m.group(1)), src)
         open(os.path.join(dst, h), 'w').write(src)
-    for f in ('shim.h', 'dirac2d_emu.cpp', 'wigner2d_emu.cpp', 'dirac3d_emu.cpp', 'batch_emu.cpp'):
+    for f in ('shim.h', 'dirac2d_emu.cpp', 'wigner2d_emu.cpp', 'dirac3d_emu.cpp', 'batch_emu.cpp', 'adjoint_emu.cpp'):
         shutil.copy(os.path.join(EMU, f), dst)
 
 
@@ -232,3 +233,51 @@ def test_batch_device_code_matches_oracle(staged, warps, grid):
         assert rel_l2(W, ref) < 2e-6, (i, rel_l2(W, ref))
         assert np.max(np.abs(obs[i, :, 0] - ref_obs[:, 0])) < (1e-6 if c['gamma'] else 2e-8 * steps), i
         assert np.max(np.abs(obs[i, :, 1:10] - ref_obs[:, 1:10])) < 1e-4, i
+
+
+def test_adjoint_device_code_matches_twin(staged):
+    """The adjoint form on a 128 x 64 grid, 4 steps with controls eps_n: the forward against the
+    complex128 torch twin, the adjoint sweep as the transpose of the forward
+    (<L, M X> = <M^H L, X> in the real inner product) and dL/deps_n of L = Re <L, W_N> against
+    central differences of the twin."""
+    import torch
+    from adjoint_twin import Twin
+    nx, npp, steps, amp, dt, dth, dla, v4, v2, v0 = 128, 64, 4, 10., 0.005, 0.02, 0.001, 0.05, -1., 0.
+    exe = build(staged, 'adjoint_emu.cpp', dict(WIGA_NX=nx, WIGA_NP=npp, WIGA_PW=1))
+    rng = np.random.default_rng(4)
+    eps = rng.normal(0., 0.3, steps)
+    dx, dp = 2 * amp / nx, 2 * amp / npp
+    xg = (dx * np.fft.fftshift(np.arange(nx) - nx // 2))[None, :]
+    pg = (dp * np.fft.fftshift(np.arange(npp) - npp // 2))[:, None]
+    X = np.exp(-((xg + 1.5) ** 2 + (pg - 0.4) ** 2)).astype(np.complex64)
+    L = (rng.normal(size=(npp, nx)) + 1j * rng.normal(size=(npp, nx))).astype(np.complex64)
+    names = ('a_x.bin', 'a_l.bin', 'a_eps.bin', 'a_w.bin', 'a_lam.bin', 'a_grad.bin')
+    fx, fl, fe, fw, flam, fg = (os.path.join(staged, n) for n in names)
+    X.tofile(fx)
+    L.tofile(fl)
+    eps.tofile(fe)
+    r = subprocess.run([exe, fx, fl, fe, fw, flam, fg, str(steps)] + [repr(v) for v in (amp, dt, dth, dla, v4, v2, v0)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    W = np.fromfile(fw, dtype=np.complex64).reshape(npp, nx).astype(np.complex128)
+    lam = np.fromfile(flam, dtype=np.complex64).reshape(npp, nx).astype(np.complex128)
+    grad = np.fromfile(fg)
+    tw = Twin(nx, npp, amp, dt, d_theta=dth, d_lambda=dla, v4=v4, v2=v2, v0=v0)
+    X128, L128 = torch.from_numpy(X.astype(np.complex128)), torch.from_numpy(L.astype(np.complex128))
+    ref = tw.propagate(X128, torch.tensor(eps)).numpy()
+    assert rel_l2(W, ref) < 1e-5, rel_l2(W, ref)
+    lhs = np.real(np.vdot(L.astype(np.complex128), W))
+    rhs = np.real(np.vdot(lam, X.astype(np.complex128)))
+    scale = np.linalg.norm(L) * np.linalg.norm(X)
+    assert abs(lhs - rhs) < 1e-6 * scale, (lhs, rhs, scale)
+
+    def loss(e):
+        return float(torch.real(torch.vdot(L128.flatten(), tw.propagate(X128, torch.tensor(e)).flatten())))
+    for n in range(steps):
+        h = 1e-5
+        ep, em = eps.copy(), eps.copy()
+        ep[n] += h
+        em[n] -= h
+        fd = (loss(ep) - loss(em)) / (2 * h)
+        # FP32 forward and adjoint: measured 1.5e-7 .. 5e-7 relative
+        assert abs(grad[n] - fd) < 1e-5 * abs(fd) + 1e-9 * scale, (n, grad[n], fd)
