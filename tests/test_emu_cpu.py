@@ -73,7 +73,7 @@ def test_dirac2d_device_code_matches_oracle(staged, rows, rnt, cc, cnt):
                       constants='exact')
     psi0 = spinor_particle_spin_up(prm, (2., 1.), lambda x, y: np.exp(-(x * x + y * y) / 4.))
     psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
-    steps = 3
+    steps = 2      # the first, a continuing and the last launch of each kind
     fin, fout, fobs = (os.path.join(staged, n) for n in ('psi_in.bin', 'psi_out.bin', 'obs.bin'))
     psi0.tofile(fin)
     r = subprocess.run([exe, fin, fout, fobs, str(steps), repr(XA), repr(YA), repr(DT), repr(MASS), repr(C)],
@@ -109,7 +109,7 @@ def test_wigner2d_device_code_matches_oracle(staged, xrows, xnt, pc, pnt, odm, k
     X = np.fft.fftshift(np.linspace(-WXA, WXA - 2 * WXA / WNX, WNX))[np.newaxis, :]
     P = np.fft.fftshift(np.linspace(-WPA, WPA - 2 * WPA / WNP, WNP))[:, np.newaxis]
     W0 = np.ascontiguousarray(np.exp(-(X - 1.5) ** 2 - (P + 0.5) ** 2 * 1.3) + 0. * 1j)
-    steps = 3
+    steps = 2      # the first, a continuing and the last launch of each kind
     fin, fout, fobs = (os.path.join(staged, n) for n in ('w_in.bin', 'w_out.bin', 'w_obs.bin'))
     W0.tofile(fin)
     r = subprocess.run([exe, fin, fout, fobs, str(steps)] + [repr(v) for v in (WXA, WPA, WDT, WGAMMA, WDTH, WDLA)] +
@@ -141,7 +141,7 @@ def test_strang_gp_device_code_matches_oracle(staged, xrows, xnt, pc, pnt, odm, 
     X = np.fft.fftshift(np.linspace(-WXA, WXA - 2 * WXA / WNX, WNX))[np.newaxis, :]
     P = np.fft.fftshift(np.linspace(-WPA, WPA - 2 * WPA / WNP, WNP))[:, np.newaxis]
     W0 = np.ascontiguousarray(np.exp(-(X - 1.5) ** 2 - (P + 0.5) ** 2 * 1.3) + 0. * 1j)
-    steps = 3
+    steps = 2      # the first, a continuing and the last launch of each kind
     fin, fout, fobs = (os.path.join(staged, n) for n in ('g_in.bin', 'g_out.bin', 'g_obs.bin'))
     W0.tofile(fin)
     r = subprocess.run([exe, fin, fout, fobs, str(steps)] + [repr(v) for v in (WXA, WPA, WDT, WGAMMA, WDTH, WDLA)] +
@@ -184,7 +184,7 @@ def test_dirac3d_device_code_matches_oracle(staged, rows, yc, zc, xr, yr, zr, ca
                         A3=D3POT[3], constants='exact')
     psi0 = spinor_particle_spin_up_3d(prm, (2., 0.5, 1.), lambda x, y, z: np.exp(-(x * x + y * y + z * z) / 4.))
     psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
-    steps = 3
+    steps = 2      # the first, a continuing and the last launch of each kind
     fin, fout, fobs = (os.path.join(staged, n) for n in ('p3_in.bin', 'p3_out.bin', 'p3_obs.bin'))
     psi0.tofile(fin)
     r = subprocess.run([exe, fin, fout, fobs, str(steps)] + [repr(v) for v in D3A + (D3DT, 1., 137.036)] +
@@ -206,13 +206,13 @@ BSIZES = (64, 128, 128, 64)
 def test_batch_device_code_matches_oracle(staged, warps, grid):
     """The FP32 real-storage passes (two rows / columns per complex transform, the
     Nyquist split), the persistent work lists and the last-CTA normalisation,
-    against the FP64 oracle at FP32 accuracy, 6 steps (each emulated step costs
+    against the FP64 oracle at FP32 accuracy, 4 steps (each emulated step costs
     seconds of barrier traffic)."""
     exe = build(staged, 'batch_emu.cpp', {'WIGB_WARPS': warps, 'WIGB_XMINB': 1, 'WIGB_PMINB': 1,
                                           'WIGB_CASES(F)': 'F(64) F(128)'})
     cases = random_batch(list(BSIZES), seed=11)
     cases[2]['gamma'] = 0.
-    steps, dt = 6, 0.005
+    steps, dt = 4, 0.005
     prm = np.array([[c['n'], c['a'], c['b'], c['gamma'], c['gamma'], dt, 10.] for c in cases], dtype=np.float64)
     W0 = [initial_state(c) for c in cases]
     packed = np.concatenate([w.real.astype(np.float32).ravel() for w in W0]).astype(np.complex64)
