@@ -6,9 +6,9 @@
 //
 //   batch_emu params W_in W_out obs_out n_prop grid
 //
-// params: count x 7 doubles (n, v4, v2, gamma, d_theta, dt, amplitude) per
-// instance, square grids, hbar = mass = 1, f(p) = |p|.  W_in / W_out: the
-// instances' (n, n) states one after another, complex64.  obs_out: count x
+// params: count x 9 doubles (n_x, n_p, v4, v2, gamma, d_theta, dt, x_amplitude,
+// p_amplitude) per instance, hbar = mass = 1, f(p) = |p|.  W_in / W_out: the
+// instances' (n_p, n_x) states one after another, complex64.  obs_out: count x
 // (n_prop + 1) x 11 doubles.  grid: CTAs of every launch.
 #include "shim.h"
 #include "wig_jit_batch.cuh"
@@ -120,13 +120,16 @@ int main(int argc, char** argv) {
   double v;
   while (std::fread(&v, sizeof v, 1, pf) == 1) prm.push_back(v);
   std::fclose(pf);
-  const int count = (int)(prm.size() / 7);
+  const int count = (int)(prm.size() / 9);
   if (count < 1 || n_prop < 1 || grid < 1) return 2;
 
   // wigb_create
   std::vector<wig::BInst> inst(count);
   std::vector<int> cls;
-  for (int i = 0; i < count; ++i) cls.push_back((int)prm[7 * i]);
+  for (int i = 0; i < count; ++i) {
+    cls.push_back((int)prm[9 * i]);
+    cls.push_back((int)prm[9 * i + 1]);
+  }
   std::sort(cls.begin(), cls.end());
   cls.erase(std::unique(cls.begin(), cls.end()), cls.end());
   std::vector<float2> tw;
@@ -138,22 +141,22 @@ int main(int argc, char** argv) {
   std::vector<float> ft;
   long long off = 0;
   for (int i = 0; i < count; ++i) {
-    const double* q = &prm[7 * i];
+    const double* q = &prm[9 * i];
     wig::BInst& b = inst[i];
     std::memset(&b, 0, sizeof(b));
-    const int n = (int)q[0];
-    const double amp = q[6], gamma = q[3];
-    b.n_x = b.n_p = n;
+    const int nx = (int)q[0], np = (int)q[1];
+    const double xa = q[7], pa = q[8], gamma = q[4];
+    b.n_x = nx; b.n_p = np;
     b.damp = gamma != 0. ? 1 : 0;
     b.ff = 0;
     b.off = off;
-    off += (long long)n * n;
-    b.tw_x = b.tw_p = tw_off[n];
-    b.dt = q[5]; b.hbar = 1.; b.mass = 1.;
-    b.dx = b.dp = 2. * amp / n;
-    b.dtheta = b.dlambda = 2. * M_PI / (2. * amp);
-    b.D_theta = q[4]; b.D_lambda = 0.;
-    b.v4 = q[1]; b.v2 = q[2]; b.v1 = 0.; b.v0 = 0.;
+    off += (long long)nx * np;
+    b.tw_x = tw_off[nx]; b.tw_p = tw_off[np];
+    b.dt = q[6]; b.hbar = 1.; b.mass = 1.;
+    b.dx = 2. * xa / nx; b.dp = 2. * pa / np;
+    b.dtheta = 2. * M_PI / (2. * pa); b.dlambda = 2. * M_PI / (2. * xa);
+    b.D_theta = q[5]; b.D_lambda = 0.;
+    b.v4 = q[2]; b.v2 = q[3]; b.v1 = 0.; b.v0 = 0.;
     const double g = b.dt * gamma, c1 = 2. / 3. * g, c2 = g, c3 = 2. * g;
     b.cl_k1 = (c1 + c2) != 0. ? c1 * c2 / (c1 + c2) : 0.;
     b.cl_k12 = c1 + c2;

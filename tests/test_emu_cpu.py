@@ -19,7 +19,8 @@ from oracle.common import rel_l2
 from oracle.dirac2d import DiracOracle, DiracParams, spinor_particle_spin_up
 from oracle.dirac3d import Dirac3DOracle, Dirac3DParams, spinor_particle_spin_up_3d
 from oracle.wigner2d import WignerOracle, WignerParams
-from batch_cases import random_batch, to_params, initial_state
+from batch_cases import random_batch
+from oracle.wigner2d import wigner_harmonic_oscillator
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, 'pywignercuda_b200', 'csrc')
@@ -198,8 +199,10 @@ def test_dirac3d_device_code_matches_oracle(staged, rows, yc, zc, xr, yr, zr, ca
     assert np.all(np.abs(obs - ref_obs) / scale < 1e-10), (obs - ref_obs) / scale
 
 
-# instances of the batched FP32 form: mixed square grids, one undamped
+# instances of the batched FP32 form: mixed grids, two of them non-square with unequal amplitudes,
+# one undamped
 BSIZES = (64, 128, 128, 64)
+BSHAPES = ((64, 128, 10., 8.), (128, 64, 8., 10.))
 
 
 @pytest.mark.parametrize('warps,grid', [(4, 3), (2, 5)])
@@ -210,11 +213,22 @@ def test_batch_device_code_matches_oracle(staged, warps, grid):
     seconds of barrier traffic)."""
     exe = build(staged, 'batch_emu.cpp', {'WIGB_WARPS': warps, 'WIGB_XMINB': 1, 'WIGB_PMINB': 1,
                                           'WIGB_CASES(F)': 'F(64) F(128)'})
-    cases = random_batch(list(BSIZES), seed=11)
+    cases = random_batch(list(BSIZES) + [s[0] for s in BSHAPES], seed=11)
     cases[2]['gamma'] = 0.
+    for c, (nx, npp, xa, pa) in zip(cases[len(BSIZES):], BSHAPES):
+        c.update(n_x=nx, n_p=npp, xa=xa, pa=pa)
     steps, dt = 4, 0.005
-    prm = np.array([[c['n'], c['a'], c['b'], c['gamma'], c['gamma'], dt, 10.] for c in cases], dtype=np.float64)
-    W0 = [initial_state(c) for c in cases]
+    shape = lambda c: (c.get('n_x', c['n']), c.get('n_p', c['n']), c.get('xa', 10.), c.get('pa', 10.))
+    prm = np.array([[shape(c)[0], shape(c)[1], c['a'], c['b'], c['gamma'], c['gamma'], dt, shape(c)[2],
+                     shape(c)[3]] for c in cases], dtype=np.float64)
+
+    def params(c):
+        nx, npp, xa, pa = shape(c)
+        return WignerParams(nx, npp, xa, pa, dt, potential='%r*pow(x,4) + %r*pow(x,2)' % (c['a'], c['b']),
+                            dpotential='4*%r*pow(x,3) + 2*%r*x' % (c['a'], c['b']), gamma=c['gamma'],
+                            d_theta=c['gamma'], damping='CaldeiraLeggett', fp_damping='fabs(p)',
+                            constants='exact')
+    W0 = [np.ascontiguousarray(wigner_harmonic_oscillator(params(c), 0, 1., c['x0'], c['p0'])) for c in cases]
     packed = np.concatenate([w.real.astype(np.float32).ravel() for w in W0]).astype(np.complex64)
     fprm, fin, fout, fobs = (os.path.join(staged, n) for n in ('b_prm.bin', 'b_in.bin', 'b_out.bin', 'b_obs.bin'))
     prm.tofile(fprm)
@@ -226,10 +240,10 @@ def test_batch_device_code_matches_oracle(staged, warps, grid):
     obs = np.fromfile(fobs).reshape(len(cases), steps + 1, 11)
     off = 0
     for i, c in enumerate(cases):
-        n = c['n']
-        W = out[off:off + n * n].reshape(n, n)
-        off += n * n
-        ref_obs, ref = WignerOracle(to_params(c)).run(W0[i], steps)
+        nx, npp = shape(c)[:2]
+        W = out[off:off + nx * npp].reshape(npp, nx)
+        off += nx * npp
+        ref_obs, ref = WignerOracle(params(c)).run(W0[i], steps)
         assert rel_l2(W, ref) < 2e-6, (i, rel_l2(W, ref))
         assert np.max(np.abs(obs[i, :, 0] - ref_obs[:, 0])) < (1e-6 if c['gamma'] else 2e-8 * steps), i
         assert np.max(np.abs(obs[i, :, 1:10] - ref_obs[:, 1:10])) < 1e-4, i
