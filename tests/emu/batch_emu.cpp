@@ -6,8 +6,9 @@
 //
 //   batch_emu params W_in W_out obs_out n_prop grid
 //
-// params: count x 9 doubles (n_x, n_p, v4, v2, gamma, d_theta, dt, x_amplitude,
-// p_amplitude) per instance, hbar = mass = 1, f(p) = |p|.  W_in / W_out: the
+// params: count x 14 doubles per instance: n_x, n_p, v4, v2, v1, v0, gamma,
+// d_theta, d_lambda, dt, x_amplitude, p_amplitude, damping_f (0: |p|, 1:
+// p^2 / sqrt(p^2 + f_eps)), f_eps; hbar = mass = 1.  W_in / W_out: the
 // instances' (n_p, n_x) states one after another, complex64.  obs_out: count x
 // (n_prop + 1) x 11 doubles.  grid: CTAs of every launch.
 #include "shim.h"
@@ -78,7 +79,7 @@ void instance_tables(wig::BInst& b, std::vector<float>* ft) {
   }
   for (int k = 0; k < np; ++k) {
     const double p = b.dp * (((k + np / 2) % np) - 0.5 * np);
-    const double f = fabs(p);
+    const double f = b.ff == 0 ? fabs(p) : p * p / sqrt(p * p + b.f_eps);
     ft->push_back((float)(p >= 0. ? f : -f));
   }
   for (int k = 0; k < np; ++k) {
@@ -120,15 +121,16 @@ int main(int argc, char** argv) {
   double v;
   while (std::fread(&v, sizeof v, 1, pf) == 1) prm.push_back(v);
   std::fclose(pf);
-  const int count = (int)(prm.size() / 9);
+  constexpr int NPRM = 14;
+  const int count = (int)(prm.size() / NPRM);
   if (count < 1 || n_prop < 1 || grid < 1) return 2;
 
   // wigb_create
   std::vector<wig::BInst> inst(count);
   std::vector<int> cls;
   for (int i = 0; i < count; ++i) {
-    cls.push_back((int)prm[9 * i]);
-    cls.push_back((int)prm[9 * i + 1]);
+    cls.push_back((int)prm[NPRM * i]);
+    cls.push_back((int)prm[NPRM * i + 1]);
   }
   std::sort(cls.begin(), cls.end());
   cls.erase(std::unique(cls.begin(), cls.end()), cls.end());
@@ -141,22 +143,23 @@ int main(int argc, char** argv) {
   std::vector<float> ft;
   long long off = 0;
   for (int i = 0; i < count; ++i) {
-    const double* q = &prm[9 * i];
+    const double* q = &prm[NPRM * i];
     wig::BInst& b = inst[i];
     std::memset(&b, 0, sizeof(b));
     const int nx = (int)q[0], np = (int)q[1];
-    const double xa = q[7], pa = q[8], gamma = q[4];
+    const double gamma = q[6], xa = q[10], pa = q[11];
     b.n_x = nx; b.n_p = np;
     b.damp = gamma != 0. ? 1 : 0;
-    b.ff = 0;
+    b.ff = (int)q[12];
+    b.f_eps = q[13];
     b.off = off;
     off += (long long)nx * np;
     b.tw_x = tw_off[nx]; b.tw_p = tw_off[np];
-    b.dt = q[6]; b.hbar = 1.; b.mass = 1.;
+    b.dt = q[9]; b.hbar = 1.; b.mass = 1.;
     b.dx = 2. * xa / nx; b.dp = 2. * pa / np;
     b.dtheta = 2. * M_PI / (2. * pa); b.dlambda = 2. * M_PI / (2. * xa);
-    b.D_theta = q[5]; b.D_lambda = 0.;
-    b.v4 = q[2]; b.v2 = q[3]; b.v1 = 0.; b.v0 = 0.;
+    b.D_theta = q[7]; b.D_lambda = q[8];
+    b.v4 = q[2]; b.v2 = q[3]; b.v1 = q[4]; b.v0 = q[5];
     const double g = b.dt * gamma, c1 = 2. / 3. * g, c2 = g, c3 = 2. * g;
     b.cl_k1 = (c1 + c2) != 0. ? c1 * c2 / (c1 + c2) : 0.;
     b.cl_k12 = c1 + c2;

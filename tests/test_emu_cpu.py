@@ -200,9 +200,11 @@ def test_dirac3d_device_code_matches_oracle(staged, rows, yc, zc, xr, yr, zr, ca
 
 
 # instances of the batched FP32 form: mixed grids, two of them non-square with unequal amplitudes,
-# one undamped
+# one undamped; one with the p^2 / sqrt(p^2 + eps) damping function, a lambda diffusion and linear and
+# constant potential terms, another with a linear term
 BSIZES = (64, 128, 128, 64)
 BSHAPES = ((64, 128, 10., 8.), (128, 64, 8., 10.))
+BEXTRA = {1: dict(ff=1, f_eps=0.5, d_lambda=0.01, v1=0.3, v0=0.2), 4: dict(v1=-0.2)}
 
 
 @pytest.mark.parametrize('warps,grid', [(4, 3), (2, 5)])
@@ -217,17 +219,27 @@ def test_batch_device_code_matches_oracle(staged, warps, grid):
     cases[2]['gamma'] = 0.
     for c, (nx, npp, xa, pa) in zip(cases[len(BSIZES):], BSHAPES):
         c.update(n_x=nx, n_p=npp, xa=xa, pa=pa)
+    for i, extra in BEXTRA.items():
+        cases[i].update(extra)
     steps, dt = 4, 0.005
-    shape = lambda c: (c.get('n_x', c['n']), c.get('n_p', c['n']), c.get('xa', 10.), c.get('pa', 10.))
-    prm = np.array([[shape(c)[0], shape(c)[1], c['a'], c['b'], c['gamma'], c['gamma'], dt, shape(c)[2],
-                     shape(c)[3]] for c in cases], dtype=np.float64)
+
+    def g(c, k, d=0.):
+        return c.get(k, d)
+
+    def shape(c):
+        return g(c, 'n_x', c['n']), g(c, 'n_p', c['n']), g(c, 'xa', 10.), g(c, 'pa', 10.)
+    prm = np.array([[shape(c)[0], shape(c)[1], c['a'], c['b'], g(c, 'v1'), g(c, 'v0'), c['gamma'], c['gamma'],
+                     g(c, 'd_lambda'), dt, shape(c)[2], shape(c)[3], g(c, 'ff'), g(c, 'f_eps', 0.5)]
+                    for c in cases], dtype=np.float64)
 
     def params(c):
         nx, npp, xa, pa = shape(c)
-        return WignerParams(nx, npp, xa, pa, dt, potential='%r*pow(x,4) + %r*pow(x,2)' % (c['a'], c['b']),
-                            dpotential='4*%r*pow(x,3) + 2*%r*x' % (c['a'], c['b']), gamma=c['gamma'],
-                            d_theta=c['gamma'], damping='CaldeiraLeggett', fp_damping='fabs(p)',
-                            constants='exact')
+        pot = '%r*pow(x,4) + %r*pow(x,2) + %r*x + %r' % (c['a'], c['b'], g(c, 'v1'), g(c, 'v0'))
+        dpot = '4*%r*pow(x,3) + 2*%r*x + %r' % (c['a'], c['b'], g(c, 'v1'))
+        f = 'fabs(p)' if not g(c, 'ff') else 'p*p/sqrt(p*p + %r)' % g(c, 'f_eps', 0.5)
+        return WignerParams(nx, npp, xa, pa, dt, potential=pot, dpotential=dpot, gamma=c['gamma'],
+                            d_theta=c['gamma'], d_lambda=g(c, 'd_lambda'), damping='CaldeiraLeggett',
+                            fp_damping=f, constants='exact')
     W0 = [np.ascontiguousarray(wigner_harmonic_oscillator(params(c), 0, 1., c['x0'], c['p0'])) for c in cases]
     packed = np.concatenate([w.real.astype(np.float32).ravel() for w in W0]).astype(np.complex64)
     fprm, fin, fout, fobs = (os.path.join(staged, n) for n in ('b_prm.bin', 'b_in.bin', 'b_out.bin', 'b_obs.bin'))
