@@ -7,11 +7,14 @@
 // tests/test_emu_cpu.py builds it and compares the result with the oracle.
 //
 //   wigner2d_emu W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda odm a_gp
+//                [bloch_steps dtb W0_in|-]
 //
 // W_in / W_out: (WIG_NP, WIG_NX) complex128; obs_out: (n_prop + 1) x 11
-// doubles, then (Strang) n_prop values of sum P(x)^2 dx.  hbar = mass = 1,
-// constants used exactly.  The expressions are fixed here and restated by the
-// test for the oracle.
+// doubles, then (Strang) n_prop values of sum P(x)^2 dx.  With bloch_steps > 0
+// (WIG_STRANG 1) it makes that many imaginary-time steps of dtb instead, as
+// wig_bloch_step (t_index = step, W0 optional), and obs_out holds their
+// WIG_BLOCH_NSTATS = 10 numbers each.  hbar = mass = 1, constants used exactly.
+// The expressions are fixed here and restated by the test for the oracle.
 #include "shim.h"
 
 #define __constant__
@@ -74,11 +77,12 @@ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 13) {
-    std::fprintf(stderr, "usage: %s W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda odm a_gp\n",
-                 argv[0]);
+  if (argc != 13 && argc != 16) {
+    std::fprintf(stderr, "usage: %s W_in W_out obs_out n_prop x_amp p_amp dt gamma d_theta d_lambda odm a_gp "
+                 "[bloch_steps dtb W0_in|-]\n", argv[0]);
     return 2;
   }
+  const long bloch_steps = argc == 16 ? std::atol(argv[13]) : 0;
   constexpr int NX = WIG_NX, NP = WIG_NP, NOBS = 11;
   const long n_prop = std::atol(argv[4]);
   const double xa = std::atof(argv[5]), pa = std::atof(argv[6]);
@@ -143,6 +147,78 @@ int main(int argc, char** argv) {
   std::vector<double2> T(odm ? 5 * npts : 0);
 
   double2* Wp = W.data();
+#if WIG_STRANG
+  if (bloch_steps > 0) {
+    // wig_bloch_step: mean-field exponent, half potential, kinetic, mean-field exponent, half
+    // potential, [W -= c W0], normalisation by the complex sum, then the step statistics
+    const double dtb = std::atof(argv[14]);
+    std::vector<double2> W0;
+    if (std::strcmp(argv[15], "-") != 0) {
+      W0.resize(npts);
+      if (!read_all(argv[15], W0.data(), npts * sizeof(double2))) return 4;
+    }
+    const double2* W0p = W0.empty() ? nullptr : W0.data();
+    const int gp = a_gp != 0., gcnt = NX < 256 ? NX : 256, n_chunks = NP / 16;
+    std::vector<double2> chunks((size_t)n_chunks * NX), rows(NP);
+    std::vector<double> Px(NX), gexp(npts), bpart((size_t)n_cta_r * wig::NBL), psq(1);
+    const long n = (long)npts;
+    const int gaxpy = clampi((int)(n / (4 * WIG_RNT)), 1, 592);
+    const double dXdP = a.dX * a.dP, pf = 2. * M_PI * hBar * dXdP;
+    auto sums = [&](const double2* w0, double* out) {
+      emu_launch(n_cta_r, WIG_RNT, [&] { wig_bloch_reduce(a, Wp, w0, bpart.data()); });
+      for (int v = 0; v < wig::NBL; ++v) out[v] = 0.;
+      for (int c = 0; c < n_cta_r; ++c)
+        for (int v = 0; v < wig::NBL; ++v) out[v] += bpart[(size_t)c * wig::NBL + v];
+    };
+    auto marginal = [&](double* psq_out) {
+      emu_launch2d(NX / gcnt, NP / 16, gcnt, [&] { wig_gp_colsum(Wp, chunks.data()); });
+      emu_launch(1, 256, [&] { wig_gp_marginal(a, chunks.data(), n_chunks, 0, Px.data(), psq_out); });
+    };
+    auto exponent = [&]() -> const double* {
+      if (!gp) return nullptr;
+      marginal(nullptr);
+      emu_launch(n_cta_x, WIG_XNT, [&] { wig_gp_bloch(a, Px.data(), dtb, gexp.data()); });
+      return gexp.data();
+    };
+    std::vector<double> stats((size_t)bloch_steps * 10, 0.);
+    for (long k = 0; k < bloch_steps; ++k) {
+      const double t = (double)k * dt;
+      const double* ge = exponent();
+      emu_launch(n_cta_p, WIG_PNT, [&] { wig_bloch_ppass(a, Wp, t, dtb, ge); });
+      emu_launch(n_cta_x, WIG_XNT, [&] { wig_bloch_xpass(a, Wp, dtb); });
+      ge = exponent();
+      emu_launch(n_cta_p, WIG_PNT, [&] { wig_bloch_ppass(a, Wp, t, dtb, ge); });
+      double sm[wig::NBL];
+      if (W0p) {
+        sums(W0p, sm);
+        const double2 c = make_double2(pf * sm[9], pf * sm[10]), one = make_double2(1., 0.);
+        emu_launch(gaxpy, WIG_RNT, [&] { wig_bloch_axpy(Wp, W0p, n, c, one); });
+      }
+      sums(nullptr, sm);
+      const double2 nrm = make_double2(sm[0] * dXdP, sm[1] * dXdP);
+      const double2 inv = wig::crecip(nrm), zero = make_double2(0., 0.);
+      emu_launch(gaxpy, WIG_RNT, [&] { wig_bloch_axpy(Wp, nullptr, n, zero, inv); });
+      double* st = stats.data() + (size_t)k * 10;
+      sums(nullptr, sm);
+      for (int q = 0; q < 5; ++q) st[q] = dXdP * sm[2 + q];
+      st[5] = pf * sm[7];
+      st[6] = pf * sm[8];
+      if (gp) {
+        marginal(psq.data());
+        st[7] = 0.5 * a_gp * psq[0];
+      }
+      if (W0p) {
+        emu_launch(NP, 256, [&] { wig_rowsum(Wp, rows.data()); });
+        for (const double2& r : rows)
+          if (r.x * a.dX < 0.) { st[8] = 1.; break; }
+      }
+      st[9] = nrm.x;
+    }
+    if (!write_all(argv[2], W.data(), npts * sizeof(double2))) return 4;
+    if (!write_all(argv[3], stats.data(), stats.size() * sizeof(double))) return 4;
+    return 0;
+  }
+#endif
   // wig_run_begin: partial sums of W for the initial normalisation and sample 0
   emu_launch(n_cta_r, WIG_RNT, [&] { wig_reduce(a, Wp); });
   a.n_partials = n_cta_r;

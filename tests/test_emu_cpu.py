@@ -307,3 +307,40 @@ def test_adjoint_device_code_matches_twin(staged):
         fd = (loss(ep) - loss(em)) / (2 * h)
         # FP32 forward and adjoint: measured 1.5e-7 .. 5e-7 relative
         assert abs(grad[n] - fd) < 1e-5 * abs(fd) + 1e-9 * scale, (n, grad[n], fd)
+
+
+# imaginary-time (Bloch) steps, GPU_Wigner2D_GPitaevskii_Bloch: the ground-state iteration with the
+# mean-field term, and the excited-state one (projection on W0) without it
+@pytest.mark.parametrize('a_gp,with_w0', [(0.5, False), (0., True)])
+def test_bloch_device_code_matches_oracle(staged, a_gp, with_w0):
+    from oracle.gpitaevskii import BlochOracle
+    exe = build(staged, 'wigner2d_emu.cpp', dict(WIG_NX=WNX, WIG_NP=WNP, WIG_XROWS=4, WIG_XNT=32,
+                                                 WIG_KIN_STRING=1, WIG_PC=8, WIG_PNT=32, WIG_DAMP=1,
+                                                 WIG_RNT=256, WIG_XMINB=1, WIG_PMINB=1, WIG_STRANG=1))
+    prm = WignerParams(WNX, WNP, WXA, WPA, WDT, potential=WPOT, dpotential=WDPOT, kinetic='0.5*p*p',
+                       constants='exact')
+    orc = BlochOracle(prm, a_gp)
+    X = np.fft.fftshift(np.linspace(-WXA, WXA - 2 * WXA / WNX, WNX))[np.newaxis, :]
+    P = np.fft.fftshift(np.linspace(-WPA, WPA - 2 * WPA / WNP, WNP))[:, np.newaxis]
+    W = orc.initial_normalise(np.exp(-(X - 1.5) ** 2 - (P + 0.5) ** 2 * 1.3) + 0. * 1j)
+    W0 = orc.initial_normalise(np.exp(-(X + 0.5) ** 2 - P ** 2) + 0. * 1j) if with_w0 else None
+    steps, dtb = 2, WDT
+    fin, fout, fst, fw0 = (os.path.join(staged, n) for n in ('bl_in.bin', 'bl_out.bin', 'bl_st.bin', 'bl_w0.bin'))
+    W.tofile(fin)
+    if with_w0:
+        W0.tofile(fw0)
+    r = subprocess.run([exe, fin, fout, fst, '1'] + [repr(v) for v in (WXA, WPA, WDT, 0., 0., 0.)] +
+                       ['0', repr(a_gp), str(steps), repr(dtb), fw0 if with_w0 else '-'],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.fromfile(fout, dtype=np.complex128).reshape(WNP, WNX)
+    st = np.fromfile(fst).reshape(steps, 10)
+    for k in range(steps):
+        W = orc.step_bloch(W, k * WDT, dtb, W0)
+        out, purity, nle = orc.stats(W)
+        ref = np.array([v.real for v in out] + [purity.real, purity.imag, np.real(nle)])
+        got_k = np.concatenate([st[k, :7], st[k, 7:8]])
+        assert np.all(np.abs(got_k - ref) <= 1e-10 * np.maximum(np.abs(ref), 1e-3)), (k, got_k - ref)
+        if with_w0:
+            assert st[k, 8] == float(np.any(W.sum(axis=1).real * prm.dX < 0.))
+    assert rel_l2(got, W) < 1e-12
