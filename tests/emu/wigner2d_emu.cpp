@@ -1,6 +1,7 @@
 // Host execution of the complex128 Wigner2D kernels (csrc/wig_jit_wigner.cuh)
 // in the launch sequence of wig_run for a plan with Caldeira-Leggett (WIG_DAMP 1)
-// or first-order ODM Lindblad damping (WIG_DAMP 0, odm 1), Lie-split or, with
+// or first-order ODM Lindblad damping (WIG_DAMP 0; odm 1: one term, 2: the two
+// terms of GPU_Wigner2D_ODM2), Lie-split or, with
 // WIG_STRANG 1, the Strang / Gross-Pitaevskii step (csrc/wig_capi.cu:
 // wig_run_begin / wig_run_step / wig_run_step_strang / wig_run_end), with the
 // tile macros WIG_* given on the command line.  Test infrastructure:
@@ -142,8 +143,10 @@ int main(int argc, char** argv) {
   a.r_theta_half = rth.data();
   a.gp_coef = a_gp;
   emu_launch(1, 64, [&] { wig_setup(a, rl.data(), rt.data(), m1.data(), m2.data(), sfp.data(), rth.data()); });
-  // Lindbladian_ODM_Order1 (weight 1, sign 1): scale dt 2 gamma / n_p, five intermediate planes
-  const double odm_coef = dt * 2 * gamma * 1. / 1. * (1.0 / (double)NP);
+  // Lindbladian_ODM_Order1: scale dt 2 gamma weight / n_p, five intermediate planes; odm 1: one term
+  // (weight 1, sign 1), odm 2: GPU_Wigner2D_ODM2's damping (weight 1, sign 1) then pumping (weight 0.5,
+  // sign -1)
+  const double odm_w[2] = {1., 0.5}, odm_sign[2] = {1., -1.};
   std::vector<double2> T(odm ? 5 * npts : 0);
 
   double2* Wp = W.data();
@@ -251,9 +254,10 @@ int main(int argc, char** argv) {
     emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, mode, orow); });
     emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass(a, Wp, t); });
 #endif
-    if (odm) {
+    for (int j = 0; j < odm; ++j) {
+      const double coef = dt * 2 * gamma * odm_w[j] / 1. * (1.0 / (double)NP), sign = odm_sign[j];
       emu_launch(n_cta_x, WIG_XNT, [&] { wig_odm_xpass(a, Wp, T.data()); });
-      emu_launch(n_cta_p, WIG_PNT, [&] { wig_odm_ppass(a, Wp, T.data(), odm_coef, 1.); });
+      emu_launch(n_cta_p, WIG_PNT, [&] { wig_odm_ppass(a, Wp, T.data(), coef, sign); });
     }
     a.n_partials = n_cta_p;
   }

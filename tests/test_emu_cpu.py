@@ -96,17 +96,21 @@ WPOT, WDPOT = '0.05*pow(x,4) - pow(x,2) + 0.2*x*sin(3.*t)', '0.2*pow(x,3) - 2.*x
 
 # (rows, x threads, columns, p threads) per CTA: the planner's rule at 64 x 32 (one CTA per pass),
 # one row per 128-thread CTA as for 1024-point rows, and several small CTAs per pass; Caldeira-Leggett,
-# ODM Lindblad damping (first order) on two of the shapes, and the Fokker-Planck (KvN) potential factor
+# ODM Lindblad damping (first order) on two of the shapes, GPU_Wigner2D_ODM2 (damping and pumping terms,
+# kinetic factor from the kinetic string), and the Fokker-Planck (KvN) potential factor
 @pytest.mark.parametrize('xrows,xnt,pc,pnt,odm,kvn', [(32, 256, 64, 256, 0, 0), (1, 128, 2, 32, 0, 0),
                                                       (4, 32, 8, 32, 0, 0), (32, 256, 64, 256, 1, 0),
-                                                      (4, 32, 8, 32, 1, 0), (4, 32, 8, 32, 0, 1)])
+                                                      (4, 32, 8, 32, 1, 0), (4, 32, 8, 32, 2, 0),
+                                                      (4, 32, 8, 32, 0, 1)])
 def test_wigner2d_device_code_matches_oracle(staged, xrows, xnt, pc, pnt, odm, kvn):
     exe = build(staged, 'wigner2d_emu.cpp', dict(WIG_NX=WNX, WIG_NP=WNP, WIG_XROWS=xrows, WIG_XNT=xnt,
-                                                 WIG_KIN_STRING=0, WIG_PC=pc, WIG_PNT=pnt, WIG_DAMP=1 - odm,
-                                                 WIG_RNT=256, WIG_XMINB=1, WIG_PMINB=1, WIG_KVN=kvn))
+                                                 WIG_KIN_STRING=int(odm == 2), WIG_PC=pc, WIG_PNT=pnt,
+                                                 WIG_DAMP=int(odm == 0), WIG_RNT=256, WIG_XMINB=1, WIG_PMINB=1,
+                                                 WIG_KVN=kvn))
     prm = WignerParams(WNX, WNP, WXA, WPA, WDT, d_theta=WDTH, d_lambda=WDLA, gamma=WGAMMA, potential=WPOT,
-                       dpotential=WDPOT, damping='ODM' if odm else 'CaldeiraLeggett', fp_damping='fabs(p)',
-                       L_material=1., kvn=bool(kvn), constants='exact')
+                       dpotential=WDPOT, kinetic='0.5*p*p', damping='ODM' if odm else 'CaldeiraLeggett',
+                       fp_damping='fabs(p)', L_material=1., kvn=bool(kvn), odm2=odm == 2, weight1=1.,
+                       weight2=0.5 if odm == 2 else 0., constants='exact')
     X = np.fft.fftshift(np.linspace(-WXA, WXA - 2 * WXA / WNX, WNX))[np.newaxis, :]
     P = np.fft.fftshift(np.linspace(-WPA, WPA - 2 * WPA / WNP, WNP))[:, np.newaxis]
     W0 = np.ascontiguousarray(np.exp(-(X - 1.5) ** 2 - (P + 0.5) ** 2 * 1.3) + 0. * 1j)
