@@ -1,12 +1,10 @@
 """bench.py's reference arm on the host: the JSON line it prints and its
-behaviour on ranks other than 0.  The GPU arm is exercised by the round of
-GPU tests and the bench itself."""
+behaviour on ranks other than 0.  The GPU arm is exercised by the GPU tests
+and the bench itself."""
 import json
 import os
 import subprocess
 import sys
-
-import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 

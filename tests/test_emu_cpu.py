@@ -18,9 +18,8 @@ import pytest
 from oracle.common import rel_l2
 from oracle.dirac2d import DiracOracle, DiracParams, spinor_particle_spin_up
 from oracle.dirac3d import Dirac3DOracle, Dirac3DParams, spinor_particle_spin_up_3d
-from oracle.wigner2d import WignerOracle, WignerParams
+from oracle.wigner2d import WignerOracle, WignerParams, wigner_harmonic_oscillator
 from batch_cases import random_batch
-from oracle.wigner2d import wigner_harmonic_oscillator
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, 'pywignercuda_b200', 'csrc')
