@@ -60,7 +60,7 @@ PASS_BYTES = NX * NP * 16 * 2      # one fused pass reads and writes the c128 gr
 # L2: the capture shows one read of it) and profiles/wigb_passes_batch64.md (the 64-instance
 # batch, 187 MB of state)
 NCU_TRAFFIC_PPASS = 16.94e6 + 0.04e6
-NCU_TRAFFIC_BATCH = 188.0e6 + 129.2e6
+NCU_TRAFFIC_BATCH = None
 
 
 def peaks():
@@ -321,14 +321,19 @@ def run_c128(args, world, rank, local, steps=None, emit=True):
     torch.cuda.synchronize()
     barrier(world)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    flags = _lib.WIG_RUN_CONTINUE | _lib.WIG_RUN_PROFILE
     with ClockSampler(local) as clk:
         e0.record(stream)
-        _lib.check(lib.wig_run_many(hs, ws, R, args.warmup, steps, flags, obs_p, stream.cuda_stream), 'timed')
+        _lib.check(lib.wig_run_many(hs, ws, R, args.warmup, steps, _lib.WIG_RUN_CONTINUE, obs_p,
+                                    stream.cuda_stream), 'timed')
         e1.record(stream)
         torch.cuda.synchronize()
     ms = barrier_max(world, e0.elapsed_time(e1))
     value = world * R * NX * NP * steps / (ms / 1e3)
+    # per-pass device times from a separate profiled run (events around every launch)
+    nprof = min(steps, 20)
+    _lib.check(lib.wig_run_many(hs, ws, R, args.warmup + steps, nprof, _lib.WIG_RUN_CONTINUE | _lib.WIG_RUN_PROFILE,
+                                None, stream.cuda_stream), 'profiled')
+    torch.cuda.synchronize()
     x_ms = p_ms = 0.
     launches = 0
     for i in insts:
@@ -436,24 +441,16 @@ def run_gp(args, world, rank, local):
         print(json.dumps(line))
 
 
-def run_batch(args, world, rank, local):
-    """Headline: the FP32 batched form on the 64-instance mixed-grid batch.  With
-    N ranks the batch has 64 N instances (the same generator; N = 1 is the
-    configuration itself) partitioned by cost across the ranks (weak scaling);
-    each rank runs its share, the observables are gathered to rank 0."""
+def batch_leg(cases, states, precision, args, world, dev):
+    """One precision of the batched form on `cases`: autotune, warm-up, then K
+    steps each timed on the device (CUDA events around its x-pass and p-pass
+    launches) with the L2 flushed before every step (the real FP32 state, 93 MB
+    for the 64-instance batch, would otherwise stay in the 126 MB L2), and the
+    same K steps replayed as one CUDA graph without flushing."""
     import torch
     from pywignercuda_b200.batch import WignerBatch, instance
-    from pywignercuda_b200.shard import gather_observables, partition
-    dev = torch.device('cuda', local)
-    torch.cuda.set_device(dev)
-    cases_all = batch_config(count=64 * world)
-    parts = partition([dict(n_x=c['n'], n_p=c['n'], gamma=c['gamma']) for c in cases_all], world)
-    cases = [cases_all[i] for i in parts[rank]]
-    grand_total = sum(c['n'] * c['n'] for c in cases_all)
     batch = WignerBatch([instance(c['n'], x_amplitude=10., dt=DT, gamma=c['gamma'], d_theta=c['d_theta'],
-                                  v4=c['a'], v2=c['b']) for c in cases])
-    states = [coherent_state(c['n'], c['x0'], c['p0']) for c in cases]
-    total = batch.total
+                                  v4=c['a'], v2=c['b']) for c in cases], precision=precision)
     stream = torch.cuda.current_stream(dev)
     scratch = batch.pack(states)
     warps, tune_ms = batch.autotune(scratch, probe_steps=3)
@@ -461,46 +458,139 @@ def run_batch(args, world, rank, local):
     K = args.steps
     W = batch.pack(states)
     batch.run(W, args.warmup)                                           # normalises
-    batch.run(W, K, continue_run=True, observables=False)               # captures the K-step graph
     torch.cuda.synchronize()
     barrier(world)
+    batch.run(W, K, continue_run=True, graph=False, observables=False, profile=True, flush_l2=True)
+    torch.cuda.synchronize()
+    x_ms, p_ms, nl = batch.profile()
+    ms = barrier_max(world, (x_ms + p_ms) / nl * K)
+    # the K-step graph replay, no flushing (the state may stay in L2 between steps)
+    batch.run(W, K, continue_run=True, observables=False)               # captures the K-step graph
+    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.run(W, K, continue_run=True, observables=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_graph = barrier_max(world, e0.elapsed_time(e1))
+    return dict(batch=batch, W=W, warps=warps, tune_ms=tune_ms, ms=ms, ms_graph=ms_graph,
+                x_us=x_ms / nl * 1e3, p_us=p_ms / nl * 1e3)
+
+
+def drift(obs, ref, W=None, W_ref=None):
+    """FP32-storage run against the complex128 drop-in path (pinned to the oracle):
+    max |d norm|, energy error as max_t |dE| / max_t |E| and at the last sample as
+    |dE| / |E|, and the final state's relative L2 (worst instance)."""
+    de = np.max(np.abs(obs[:, :, 9] - ref[:, :, 9]), axis=1) / np.max(np.abs(ref[:, :, 9]), axis=1)
+    dfin = np.abs(obs[:, -1, 9] - ref[:, -1, 9]) / np.abs(ref[:, -1, 9])
+    out = {'steps': int(obs.shape[1] - 1), 'norm_max_abs': float(np.max(np.abs(obs[:, :, 0] - ref[:, :, 0]))),
+           'energy_rel_max': float(np.max(de)), 'energy_rel_final': float(np.max(dfin))}
+    if W is not None:
+        out['state_rel_l2_final'] = float(max(np.linalg.norm(a - b.real) / np.linalg.norm(b.real)
+                                               for a, b in zip(W, W_ref)))
+    return out
+
+
+def c128_runs(cases, states, steps, dev, amp=10., f='fabs(p)'):
+    """complex128 drop-in runs (exact constants; coefficient slots, one module per
+    grid size): (obs[count, steps+1, 11], final states)."""
+    import torch
+    from pywignercuda_b200 import GPU_Wigner2D_FFT, _lib
+
+    class Poly(GPU_Wigner2D_FFT):
+        constants_mode = _lib.CONST_EXACT
+
+        def __init__(self, c):
+            self.dampingFunction, self.grossPitaevskiiCoefficient = 'CaldeiraLeggett', 0.
+            self.fp_Damping_String = f
+            self.coefficients = [c['a'], c['b']]
+            self.SetTimeTrack(DT, steps, 10 ** 9, fileName='')
+            GPU_Wigner2D_FFT.__init__(self, c['n'], c['n'], amp, amp, 1., 1., c['d_theta'], 0., c['gamma'],
+                                      'cf[0]*pow(x,4) + cf[1]*pow(x,2)', '4.*cf[0]*pow(x,3) + 2.*cf[1]*x',
+                                      '0.5*p*p')
+    obs, Ws = [], []
+    for c, s in zip(cases, states):
+        inst = Poly(c)
+        W = torch.from_numpy(np.ascontiguousarray(s, dtype=np.complex128)).to(dev)
+        obs.append(inst.propagate(W, steps))
+        Ws.append(W.cpu().numpy())
+        del inst
+    return np.array(obs), Ws
+
+
+def validation(cases, states, dev):
+    """Norm / energy / state error of both precisions at the configurations' full
+    step counts, against the complex128 drop-in path: the 64-instance batch for
+    2000 steps, and the 1024^2 double well (amplitude 12, cat state, CL gamma 0.1,
+    D_theta 0.1, f = |p|) for 4000 steps."""
+    from pywignercuda_b200.batch import WignerBatch, instance
+    out = {}
+    ref3, Wr3 = c128_runs(cases, states, 2000, dev)
+    c2 = dict(n=NX, a=0.05, b=-1., gamma=GAMMA, d_theta=D_THETA)
+    s2 = cat_state(make_instance(1))
+    ref2, Wr2 = c128_runs([c2], [s2], 4000, dev, amp=AMP)
+    for prec in ('mixed', 'f32'):
+        b3 = WignerBatch([instance(c['n'], x_amplitude=10., dt=DT, gamma=c['gamma'], d_theta=c['d_theta'],
+                                   v4=c['a'], v2=c['b']) for c in cases], precision=prec)
+        W = b3.pack(states)
+        o3 = b3.run(W, 2000)
+        W3 = b3.unpack(W)
+        del b3, W
+        b2 = WignerBatch([instance(NX, x_amplitude=AMP, dt=DT, gamma=GAMMA, d_theta=D_THETA, v4=0.05, v2=-1.)],
+                         precision=prec)
+        W = b2.pack([s2])
+        o2 = b2.run(W, 4000)
+        W2 = b2.unpack(W)
+        del b2, W
+        out[prec] = {'batch_2000': drift(o3, ref3, W3, Wr3), 'double_well_1024_4000': drift(o2, ref2, W2, Wr2)}
+    out['reference'] = ('complex128 drop-in path (parity-pinned to the oracle), exact constants, same inputs; '
+                        'energy_rel_max = max_t |dE| / max_t |E|, energy_rel_final = |dE| / |E| at the last sample')
+    return out
+
+
+def run_batch(args, world, rank, local):
+    """Headline: the batched form on the 64-instance mixed-grid batch.  With N
+    ranks the batch has 64 N instances (the same generator; N = 1 is the
+    configuration itself) partitioned by cost across the ranks (weak scaling);
+    each rank runs its share, the observables are gathered to rank 0.  Both
+    precisions are timed; the headline is the one whose measured norm and energy
+    errors at 2000 / 4000 steps are within 1e-6 (the mixed form), the other is
+    reported beside it with its errors."""
+    import torch
+    from pywignercuda_b200.shard import gather_observables, partition
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    cases_all = batch_config(count=64 * world)
+    parts = partition([dict(n_x=c['n'], n_p=c['n'], gamma=c['gamma']) for c in cases_all], world)
+    cases = [cases_all[i] for i in parts[rank]]
+    grand_total = sum(c['n'] * c['n'] for c in cases_all)
+    states = [coherent_state(c['n'], c['x0'], c['p0']) for c in cases]
+    K = args.steps
     with ClockSampler(local) as clk:
-        e0.record(stream)
-        batch.run(W, K, continue_run=True)                              # graph replay; obs D2H included
-        e1.record(stream)
-        torch.cuda.synchronize()
-    ms = barrier_max(world, e0.elapsed_time(e1))
-    value = grand_total * K / (ms / 1e3)
+        legs = {p: batch_leg(cases, states, p, args, world, dev) for p in ('mixed', 'f32')}
+    val = validation(cases, states, dev) if rank == 0 and not args.profile_only else None
+    head_p = 'mixed'
+    if val is not None:
+        ok = all(v['norm_max_abs'] <= 1e-6 and v['energy_rel_max'] <= 1e-6 for v in val['mixed'].values()
+                 if isinstance(v, dict))
+        head_p = 'mixed' if ok else 'f32'
+    head = legs[head_p]
+    value = grand_total * K / (head['ms'] / 1e3)
     if args.profile_only:
         if rank == 0:
-            print(json.dumps({'metric': METRIC, 'value': value, 'unit': UNIT, 'steps': K, 'warps': warps,
+            print(json.dumps({'metric': METRIC, 'value': value, 'unit': UNIT, 'steps': K,
                               'note': 'profile-only run (timed section only)'}))
         return
-    # per-pass device time (a short non-graph run with events around every launch)
-    nprof = min(K, 20)
-    batch.run(W, nprof, continue_run=True, graph=False, observables=False, profile=True)
-    x_ms, p_ms, nl = batch.profile()
+    batch, total = head['batch'], head['batch'].total
     peak, peak_kind = peaks()
-    pass_bytes = total * 8 * 2                                        # complex64 read + write per pass
-    dom, dom_ms = ('wigb_ppass', p_ms) if p_ms >= x_ms else ('wigb_xpass', x_ms)
-    achieved = pass_bytes / (dom_ms / nl / 1e3) / 1e9
-    # FP32 drift against complex128 on every instance (fresh run, same steps)
-    nval = min(K, 200)
-    Wv = batch.pack(states)
-    obs32 = batch.run(Wv, nval, graph=False)
-    obs64 = c128_reference_obs(cases, nval, dev)
-    norm_err = float(np.max(np.abs(obs32[:, :, 0] - obs64[:, :, 0])))
-    energy_abs = np.max(np.abs(obs32[:, :, 9] - obs64[:, :, 9]), axis=1)
-    # scale of H(x, p) over each instance's grid: the FP32 FFT noise is weighted by it
-    hrange = np.array([10. ** 2 / 2. + abs(c['a']) * 10. ** 4 + abs(c['b']) * 10. ** 2 for c in cases])
-    energy_err = float(np.max(energy_abs))
-    energy_err_h = float(np.max(energy_abs / hrange))
-    del Wv
-    # e2e: pinned host state in, run, host state and observables out, all timed
-    hin = torch.from_numpy(np.concatenate([s.astype(np.complex64).ravel() for s in states])).pin_memory()
+    pass_bytes = total * 4 * 2                                        # real FP32 state read + write per pass
+    dom, dom_us = ('wigb_ppass', head['p_us']) if head['p_us'] >= head['x_us'] else ('wigb_xpass', head['x_us'])
+    achieved = pass_bytes / (dom_us / 1e6) / 1e9
+    # e2e: pinned host state in, run (one call, graph), host state and observables out, all timed
+    hin = torch.from_numpy(np.concatenate([s.astype(np.float32).ravel() for s in states])).pin_memory()
     hout = torch.empty_like(hin).pin_memory()
-    Wd = torch.empty(total, dtype=torch.complex64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    Wd = torch.empty(total, dtype=torch.float32, device=dev)
     Wd.copy_(hin)
     batch.run(Wd, K, observables=False)                                 # captures this run's graph
     torch.cuda.synchronize()
@@ -515,34 +605,45 @@ def run_batch(args, world, rank, local):
     torch.cuda.synchronize()
     gather_observables(obs_run, parts, rank)                            # the only cross-rank exchange
     e2e_ms = barrier_max(world, max(f0.elapsed_time(f1), 1e3 * (time.perf_counter() - t0)))
+    for leg in legs.values():
+        leg.pop('batch')
+        leg.pop('W')
+    del batch
     c128 = run_c128(args, world, rank, local, steps=min(K, 100), emit=False)
+    forms = {p: {'value': grand_total * K / (legs[p]['ms'] / 1e3), 'ms_per_step': legs[p]['ms'] / K,
+                 'ms_per_step_graph_no_flush': legs[p]['ms_graph'] / K, 'warps_per_cta': legs[p]['warps'],
+                 'autotune_ms': legs[p]['tune_ms'], 'x_pass_us': legs[p]['x_us'], 'p_pass_us': legs[p]['p_us'],
+                 'ratio_vs_c128': grand_total * K / (legs[p]['ms'] / 1e3) / c128['value'],
+                 'drift_vs_fp64': val[p] if val else None} for p in legs}
     line = {
         'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': K, 'warmup': args.warmup,
-        'ms_per_step': ms / K, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
-        'dtype': 'f32 (FP64 phase arguments and observables)', 'data': 'synthetic',
+        'ms_per_step': head['ms'] / K, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f32 storage; ' + ('FP64 kinetic/Moyal transforms, FP32 dissipator transforms' if head_p == 'mixed'
+                                    else 'FP32 transforms') + '; FP64 phase arguments and observables',
+        'data': 'synthetic',
         'config': {'workload': '64 Wigner2D instances, square grids from {128,256,512,1024} (default_rng(0)), '
                                'V=a x^4+b x^2, Caldeira-Leggett, coherent states, dt=0.005',
-                   'form': 'FP32 batched, one x-pass + one p-pass launch per step, CUDA graph',
+                   'form': 'batched, precision %s, real FP32 state, one x-pass + one p-pass launch per step' % head_p,
                    'instances': len(cases_all), 'instances_per_rank': [len(p) for p in parts],
-                   'grid_points': grand_total, 'warps_per_cta': warps,
-                   'autotune_ms': tune_ms,
+                   'grid_points': grand_total, 'warps_per_cta': head['warps'],
                    'parallelism': 'instances partitioned by cost across ranks, one process per GPU, '
                                   'observables gathered to rank 0 (no data-path collective)',
-                   'l2': 'state %d MB > 126 MB L2' % (total * 8 >> 20)},
+                   'l2': 'state %d MB < 126 MB L2: L2 flushed (a %d MB write) before every timed step, outside '
+                         'the per-launch CUDA events' % (total * 4 >> 20, 2 * 126)},
         'plain_c128': c128,
-        'ratio_fp32_batched_vs_c128': value / c128['value'],
-        'drift_vs_fp64': {'steps': nval, 'norm_max_abs': norm_err, 'energy_max_abs': energy_err,
-                          'energy_max_rel_to_H_range': energy_err_h,
-                          'reference': 'complex128 drop-in path, exact constants, same instances'},
-        'flops': batch_flops(cases_all, world, ms / K, clk.summary()),
+        'ratio_vs_c128': value / c128['value'],
+        'forms': forms,
+        'drift_vs_fp64': val[head_p] if val else None,
+        'flops': batch_flops(cases_all, world, head['ms'] / K, clk.summary()),
         'roofline': {'bound': 'hbm', 'kernel': dom, 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                      'frac': achieved / peak, 'peak_kind': peak_kind, 'algorithmic_bytes_per_launch': pass_bytes,
-                     'avg_launch_us': dom_ms / nl * 1e3, 'x_pass_us': x_ms / nl * 1e3, 'p_pass_us': p_ms / nl * 1e3,
+                     'algorithmic_bytes_complex64_storage': total * 8 * 2,
+                     'avg_launch_us': dom_us, 'x_pass_us': head['x_us'], 'p_pass_us': head['p_us'],
                      'traffic': NCU_TRAFFIC_BATCH},
         'e2e': {'value': grand_total * K / (e2e_ms / 1e3), 'unit': UNIT,
-                'h2d_bytes_per_step': grand_total * 8 / K,
-                'd2h_bytes_per_step': (grand_total * 8 + len(cases_all) * (K + 1) * 11 * 8) / K,
-                'note': 'one run call: upload the packed states, K propagations, download states and '
+                'h2d_bytes_per_step': grand_total * 4 / K,
+                'd2h_bytes_per_step': (grand_total * 4 + len(cases_all) * (K + 1) * 11 * 8) / K,
+                'note': 'one run call (graph): upload the packed states, K propagations, download states and '
                         'observables; bytes per propagation step'},
         'gpu_launches': 2 * K + 2,
         'clocks': clk.summary(),

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define WIG_ABI_VERSION 3
+#define WIG_ABI_VERSION 4
 
 enum wig_status {
   WIG_OK = 0,
@@ -80,6 +80,9 @@ enum wig_potential_phase {
 #define WIG_RUN_CONTINUE 1u /* W continues an earlier call: skip the entry normalisation */
 #define WIG_RUN_PROFILE 2u  /* time every x-pass / p-pass launch with CUDA events (wig_profile) */
 #define WIG_RUN_GRAPH 4u    /* wigb_run: capture the launch sequence in a CUDA graph once, replay it */
+#define WIG_RUN_FLUSH_L2 8u /* wigb_run with WIG_RUN_PROFILE (no graph): before every step, write a
+                               buffer twice the L2 size, outside the timed launches, so each step
+                               starts from a cold L2 */
 
 #define WIG_NOBS 11   /* norm, <x>, <x^2>, <p>, <p^2>, <xp>, <V'>, <pV'>, <xV'>, <H>, negative area */
 #define DIRAC_NOBS 10 /* <x>, <y>, <alpha1>, <alpha2>, <beta>, <K>, <A0>, <px>, <py>, norm_kept */
@@ -258,20 +261,26 @@ int dirac3_destroy(dirac3_handle* h);
 /* Compile-only check of a Dirac3D instance's kernels (no GPU needed). */
 int dirac3_jit_check(const dirac3_desc* desc, char* log, int64_t log_cap);
 
-/* ---------------------------------------------------------------- batched FP32
+/* ---------------------------------------------------------------- batched form
  * Many independent Wigner2D instances with polynomial potentials
  * V(x) = v4 x^4 + v2 x^2 + v1 x + v0, kinetic p^2/2m, Caldeira-Leggett damping
  * (gamma != 0) with f(p) = |p| or p^2/sqrt(p^2 + f_eps), on uneven grids
- * (powers of two in [64, 1024]), advanced together in FP32 complex (W,
- * FFTs, pointwise factors) with FP64 phase arguments reduced to one turn
- * before sincospif and FP64 observables (per-column moments, compensated
- * per-instance sums).  Real storage: W is a Wigner function, so two real rows
- * (x-pass) or columns (p-pass) share each complex transform; the state keeps
- * the complex64 layout but each step leaves W real (imaginary parts, which are
- * rounding noise for a real initial state, are dropped).  Constants are exact (no
- * '%f' rounding).  No counterpart in the reference, which runs one complex128
- * instance per Run() (GPU_Wigner2D_FFT.py:1843); the step is the same Lie
- * split (:1884-1913). */
+ * (powers of two in [64, 1024]), advanced together.  The state is real FP32
+ * storage, one float per grid point: W is a Wigner function, so two real rows
+ * (x-pass) or columns (p-pass) share each complex transform, and the
+ * imaginary rounding noise of a complex step is not kept.  Precision of the
+ * arithmetic, one per batch:
+ *   WIGB_PREC_F32    FP32 transforms and factors throughout;
+ *   WIGB_PREC_MIXED  the kinetic and Moyal transform pairs and their factors
+ *                    in FP64, the three dissipator pairs in FP32.
+ * Both form the phase arguments in FP64 and reduce them to one turn, and keep
+ * the observables in FP64 (per-column moments, compensated per-instance sums).
+ * Constants are exact (no '%f' rounding).  No counterpart in the reference,
+ * which runs one complex128 instance per Run() (GPU_Wigner2D_FFT.py:1843); the
+ * step is the same Lie split (:1884-1913). */
+#define WIGB_PREC_F32 0
+#define WIGB_PREC_MIXED 1
+
 typedef struct wigb_instance {
   int32_t n_x, n_p;
   int32_t damping_f;  /* 0: f = |p|, 1: f = p^2/sqrt(p^2 + f_eps) */
@@ -283,15 +292,17 @@ typedef struct wigb_instance {
 
 typedef struct wigb_handle wigb_handle;
 
-/* warps: tile shape (warps per CTA, 2 / 4 / 8; 0 = 8 until wigb_autotune picks one). */
-int wigb_create(const wigb_instance* instances, int64_t count, int32_t warps, wigb_handle** out);
+/* warps: tile shape (warps per CTA, 2 / 4 / 8; 0 = 8 until wigb_autotune picks one).
+ * precision: WIGB_PREC_F32 or WIGB_PREC_MIXED. */
+int wigb_create(const wigb_instance* instances, int64_t count, int32_t warps, int32_t precision,
+                wigb_handle** out);
 
-/* offsets[count + 1]: element offset of each instance's (n_p, n_x) complex64
+/* offsets[count + 1]: element offset of each instance's (n_p, n_x) float
  * block in the packed state buffer; offsets[count] = total elements. */
 int wigb_offsets(wigb_handle* h, int64_t* offsets);
 
 /* Normalise (unless flags & WIG_RUN_CONTINUE) and advance every instance of
- * the packed complex64 state W by n_prop propagations (t = t_index * dt).
+ * the packed real FP32 state W (16-byte aligned) by n_prop propagations (t = t_index * dt).
  * obs_host (may be NULL): count x (n_prop + 1) x WIG_NOBS doubles, instance
  * major.  flags & WIG_RUN_GRAPH: the launch sequence is captured into a CUDA
  * graph on first use (per W, t_index0, n_prop, flags, tile shape) and replayed. */
@@ -310,9 +321,10 @@ int wigb_profile(wigb_handle* h, double* ms_out, int64_t* launches);
 
 int wigb_destroy(wigb_handle* h);
 
-/* Compile-only check (no GPU) of the batched kernels for the given grid sizes
- * and tile shape; log receives the NVRTC / ptxas report. */
-int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t warps, char* log, int64_t log_cap);
+/* Compile-only check (no GPU) of the batched kernels for the given grid sizes,
+ * tile shape and precision; log receives the NVRTC / ptxas report. */
+int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t warps, int32_t precision, char* log,
+                   int64_t log_cap);
 
 /* ---- Adjoint (differentiable) FP32 form.  No counterpart in the reference,
  * which has no gradients.  One Wigner2D grid (powers of two in [64, 1024] per

@@ -3,8 +3,8 @@
 The reference (cabrer7/PyWignerCUDA) is Python 2 + PyCUDA and cannot be
 imported under Python 3 as it stands.  This harness:
 
-1. reads a reference module's source text from the reference checkout (default
-   ``/root/reference``; override with ``PYWIGNER_REFERENCE``), expands its tabs
+1. reads a reference module's source text from the reference checkout named by
+   the environment variable ``PYWIGNER_REFERENCE`` (required), expands its tabs
    the way the Python 2 tokenizer does (stops every 8 columns), turns ``print``
    statements into calls and ``np.float(`` into ``float(`` -- nothing else is
    changed -- and executes it as a module;
@@ -42,7 +42,7 @@ import contextlib
 
 import numpy as np
 
-REF_ROOT = os.environ.get('PYWIGNER_REFERENCE', '/root/reference')
+REF_ROOT = os.environ.get('PYWIGNER_REFERENCE', '')
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD_DIR = os.path.join(HERE, '_ref')
 
@@ -354,6 +354,8 @@ def load_reference_module(name):
     fake modules installed; returns the module object."""
     if name in _MODULE_CACHE:
         return _MODULE_CACHE[name]
+    if not REF_ROOT or not os.path.isdir(REF_ROOT):
+        raise RuntimeError('set PYWIGNER_REFERENCE to the reference checkout (cabrer7/PyWignerCUDA)')
     path = os.path.join(REF_ROOT, name + '.py')
     with open(path) as f:
         src = py2_to_py3(f.read())

@@ -12,7 +12,7 @@ from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_uint3
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libwigner_b200.so')
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 WIG_NOBS = 11
 WIG_BLOCH_NSTATS = 10
 DIRAC_NOBS = 10
@@ -20,6 +20,7 @@ DIRAC3_NOBS = 12
 WIG_RUN_CONTINUE = 1
 WIG_RUN_PROFILE = 2
 WIG_RUN_GRAPH = 4
+WIG_RUN_FLUSH_L2 = 8
 
 DAMP_NONE, DAMP_CALDEIRA_LEGGETT, DAMP_ODM = 0, 1, 2
 CONST_CUDA_F, CONST_EXACT = 0, 1
@@ -139,13 +140,13 @@ SIGNATURES = [
     ('dirac3_jit_check', c_int, [POINTER(Dirac3Desc), c_char_p, c_int64]),
     ('wig_jit_check', c_int, [POINTER(WigDesc), c_char_p, c_int64]),
     ('dirac_jit_check', c_int, [POINTER(DiracDesc), c_char_p, c_int64]),
-    ('wigb_create', c_int, [c_void_p, c_int64, c_int32, POINTER(c_void_p)]),
+    ('wigb_create', c_int, [c_void_p, c_int64, c_int32, c_int32, POINTER(c_void_p)]),
     ('wigb_offsets', c_int, [c_void_p, POINTER(c_int64)]),
     ('wigb_run', c_int, [c_void_p, c_void_p, c_int64, c_int64, c_uint32, _DP, c_void_p]),
     ('wigb_autotune', c_int, [c_void_p, c_void_p, c_int64, POINTER(c_int32), _DP, c_void_p]),
     ('wigb_profile', c_int, [c_void_p, _DP, POINTER(c_int64)]),
     ('wigb_destroy', c_int, [c_void_p]),
-    ('wigb_jit_check', c_int, [POINTER(c_int32), c_int64, c_int32, c_char_p, c_int64]),
+    ('wigb_jit_check', c_int, [POINTER(c_int32), c_int64, c_int32, c_int32, c_char_p, c_int64]),
     ('wiga_create', c_int, [POINTER(WigaDesc), POINTER(c_void_p)]),
     ('wiga_forward', c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p]),
     ('wig_step_adjoint', c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),

@@ -1,14 +1,17 @@
-"""Batched FP32 Wigner2D propagation (``wigb_*`` in include/wigner_b200.h).
+"""Batched Wigner2D propagation (``wigb_*`` in include/wigner_b200.h).
 
 Many independent instances -- polynomial potentials V = v4 x^4 + v2 x^2 +
 v1 x + v0, kinetic p^2/2m, Caldeira-Leggett damping with f(p) = |p| (or
 p^2/sqrt(p^2 + eps)), uneven power-of-two grids in [64, 1024] -- advance
 together: one x-pass and one p-pass launch per step over a work list that
 spans all instances, the whole run captured once into a CUDA graph, the tile
-shape picked by ``autotune``.  W, FFTs and the pointwise factors are FP32
-complex; phase arguments are formed and range-reduced in FP64; observables are
-FP64 (Kahan).  The step is the reference's Lie split
-(``GPU_Wigner2D_FFT.py:1884-1913``) with exact constants.
+shape picked by ``autotune``.  The state is the real Wigner function in FP32
+(one float per grid point).  ``precision='f32'`` runs every transform and
+factor in FP32; ``'mixed'`` runs the kinetic and Moyal transform pairs and
+their factors in FP64 and the three dissipator pairs in FP32.  Phase
+arguments are formed and range-reduced in FP64; observables are FP64 (Kahan).
+The step is the reference's Lie split (``GPU_Wigner2D_FFT.py:1884-1913``)
+with exact constants.
 """
 import ctypes
 
@@ -19,6 +22,7 @@ from ._lib import WigbInstance, check, dptr
 from .wigner2d import _torch
 
 OBS_NAMES = ('norm', 'x', 'x2', 'p', 'p2', 'xp', 'dV', 'pdV', 'xdV', 'H', 'negative_area')
+PRECISIONS = {'f32': 0, 'mixed': 1}
 
 
 def instance(n_x, n_p=None, x_amplitude=10., p_amplitude=None, hbar=1., mass=1., dt=0.005, gamma=0.,
@@ -32,9 +36,12 @@ def instance(n_x, n_p=None, x_amplitude=10., p_amplitude=None, hbar=1., mass=1.,
 
 
 class WignerBatch:
-    def __init__(self, instances, warps=0):
+    def __init__(self, instances, warps=0, precision='f32'):
         torch = _torch()
         lib = _lib.load()
+        if precision not in PRECISIONS:
+            raise _lib.WignerArgumentError("precision must be 'f32' or 'mixed'")
+        self.precision = precision
         self.instances = [dict(d) for d in instances]
         arr = (WigbInstance * len(instances))()
         for a, d in zip(arr, instances):
@@ -42,7 +49,8 @@ class WignerBatch:
                 setattr(a, k, v)
         self._desc = arr
         h = ctypes.c_void_p()
-        check(lib.wigb_create(arr, len(instances), int(warps), ctypes.byref(h)), 'wigb_create')
+        check(lib.wigb_create(arr, len(instances), int(warps), PRECISIONS[precision], ctypes.byref(h)),
+              'wigb_create')
         self._handle = h
         off = (ctypes.c_int64 * (len(instances) + 1))()
         check(lib.wigb_offsets(h, off), 'wigb_offsets')
@@ -60,10 +68,11 @@ class WignerBatch:
                 pass
             h.value = None
 
-    # ---- state packing: instance i is a (n_p, n_x) complex64 block at offsets[i]
+    # ---- state packing: instance i is a (n_p, n_x) float32 block at offsets[i] (the real
+    # Wigner function; the real part of a complex W_init is taken)
     def pack(self, states):
         torch = _torch()
-        flat = np.concatenate([np.ascontiguousarray(s, dtype=np.complex64).ravel() for s in states])
+        flat = np.concatenate([np.ascontiguousarray(np.real(s), dtype=np.float32).ravel() for s in states])
         if flat.size != self.total:
             raise _lib.WignerArgumentError('states do not match the batch geometry')
         return torch.from_numpy(flat).to(torch.device('cuda', self.device))
@@ -75,8 +84,8 @@ class WignerBatch:
 
     def _check_W(self, W):
         torch = _torch()
-        if W.dtype != torch.complex64 or not W.is_cuda or not W.is_contiguous() or W.numel() != self.total:
-            raise _lib.WignerArgumentError('W must be the packed contiguous CUDA complex64 state')
+        if W.dtype != torch.float32 or not W.is_cuda or not W.is_contiguous() or W.numel() != self.total:
+            raise _lib.WignerArgumentError('W must be the packed contiguous CUDA float32 state')
 
     def profile(self):
         """(x-pass ms, p-pass ms, steps) of the last run made with profile=True."""
@@ -86,14 +95,17 @@ class WignerBatch:
         return ms[0], ms[1], n.value
 
     def run(self, W, n_prop, t_index0=0, continue_run=False, graph=True, observables=True, stream=None,
-            profile=False):
+            profile=False, flush_l2=False):
         """Advance the packed state W in place; returns obs[count, n_prop+1, 11]
-        (sample k before propagation k, the last after the final one)."""
+        (sample k before propagation k, the last after the final one).
+        profile=True (with graph=False) times every x-pass and p-pass launch
+        (``profile()``); flush_l2=True then also writes a buffer twice the L2
+        size before every step, outside the timed launches."""
         torch = _torch()
         self._check_W(W)
         st = stream if stream is not None else torch.cuda.current_stream(W.device)
         flags = ((_lib.WIG_RUN_CONTINUE if continue_run else 0) | (_lib.WIG_RUN_GRAPH if graph else 0)
-                 | (_lib.WIG_RUN_PROFILE if profile else 0))
+                 | (_lib.WIG_RUN_PROFILE if profile else 0) | (_lib.WIG_RUN_FLUSH_L2 if flush_l2 else 0))
         obs = np.empty((len(self.instances), n_prop + 1, _lib.WIG_NOBS)) if observables else None
         check(_lib.load().wigb_run(self._handle, W.data_ptr(), t_index0, n_prop, flags,
                                    dptr(obs) if obs is not None else None, st.cuda_stream), 'wigb_run')

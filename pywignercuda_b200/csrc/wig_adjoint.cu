@@ -14,6 +14,7 @@
 #include "../../include/wigner_b200.h"
 #include "wig_adjoint.cuh"
 #include "wig_host.h"
+#include "wig_batch_host.h"   // register-FFT twiddle tables
 #include "wig_adjoint_src.inc"   // kJitAdjointSource (generated by build.py)
 
 using namespace wighost;

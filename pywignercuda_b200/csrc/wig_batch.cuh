@@ -1,19 +1,30 @@
-// Batched FP32 Wigner2D propagation: many independent instances of uneven
-// grid sizes advanced together, one x-pass launch and one p-pass launch per
-// step over a work list that spans every instance (x-items: blocks of rows,
-// p-items: blocks of columns).  Every sequence (a row in the x-pass, a column
-// in the p-pass) is transformed by the register-resident FFT of wig_rfft.cuh:
-// rf_g(N) lanes of a warp hold its N elements in registers, so the whole
-// p-pass -- forward FFT, Moyal factor, inverse FFT, the three Caldeira-Leggett
-// dissipator applications (six more FFTs), observables -- runs on registers,
-// with shared memory only for the coalescing tile and one exchange per FFT.
+// Batched Wigner2D propagation: many independent instances of uneven grid
+// sizes advanced together, one x-pass launch and one p-pass launch per step
+// over a work list that spans every instance (x-items: blocks of rows, p-items:
+// blocks of columns).  Every sequence (a row in the x-pass, a column in the
+// p-pass) is transformed by the register-resident FFT of wig_rfft.cuh: rf_g(N)
+// lanes of a warp hold its N elements in registers, so the whole p-pass --
+// forward FFT, Moyal factor, inverse FFT, the three Caldeira-Leggett dissipator
+// applications (six more FFTs), observables -- runs on registers, with shared
+// memory only for the coalescing tile and one exchange per FFT.
 //
-// Precision policy: W, FFTs and the pointwise factors are FP32 complex; FP64
-// is used only to form the large phase arguments (dt*lambda*p/m and
+// Storage: W is the real Wigner function, FP32, one float per grid point
+// (instance i a row-major (n_p, n_x) block at its offset); two real rows or
+// columns share one complex transform.
+//
+// Precision (WIGB_PREC, one value per compiled batch):
+//   0  FP32 transforms and pointwise factors throughout;
+//   1  the kinetic (x-pass) and Moyal (p-pass) transform pairs and their
+//      factors in FP64, the three dissipator pairs in FP32.  The dissipator's
+//      contribution is scaled by 2 gamma dt (~1e-3), so its FP32 rounding is
+//      ~1e-3 of an FP32 transform's; the kinetic and Moyal pairs carry the
+//      full state, and their FP32 rounding, spread over the grid and weighted
+//      by H(x, p) at its edges, is what drifts the energy.
+// In both, FP64 forms the large phase arguments (dt*lambda*p/m and
 // dt*[V(x - hbar theta/2) - V(x + hbar theta/2)]/hbar, the latter from the
-// exact polynomial expansion, both in units of 2 pi) and to reduce them to
-// one turn before sincospif, and for the observables (FP64 per-column
-// moments, FP64 tree / per-instance reductions).
+// exact polynomial expansion, both in units of 2 pi) and reduces them to one
+// turn, and the observables are FP64 (per-column moments, FP64 tree /
+// per-instance reductions).
 //
 // Normalisation (GPU_Wigner2D_FFT.Run :1912-1913): every p-item writes FP64
 // partial sums; the last CTA of an instance to finish (arrival counter, no
@@ -26,6 +37,9 @@
 #ifndef WIGB_WARPS
 #define WIGB_WARPS 8
 #endif
+#ifndef WIGB_PREC
+#define WIGB_PREC 0
+#endif
 #define WIGB_NT (WIGB_WARPS * 32)
 
 namespace wig {
@@ -37,7 +51,8 @@ struct BInst {
   long long off;     // element offset in the packed state buffer
   int xitem0, n_xitems, pitem0, n_pitems;
   int tw_x, tw_p;    // offsets of the instance's twiddle tables (2N entries each) in the table buffer
-  int ft_x, ft_p;    // offsets of its float tables: [rtab n_x][mm n_x] and [rth n_p][sfp n_p][ths n_p]
+  int ft_x, ft_p;    // offsets of its float tables: [rtab n_x][mm n_x][gtab 2 n_x] and [rth n_p][sfp n_p][ths n_p]
+  int fd_x, fd_p;    // offsets of its double tables: [rtab n_x][mm n_x][gtab 2 n_x] and [rth n_p]
   double dt, hbar, mass, dx, dp, dtheta, dlambda, D_theta, D_lambda, f_eps;
   double v4, v2, v1, v0;   // V(x) = v4 x^4 + v2 x^2 + v1 x + v0
   double cl_k1, cl_k12, cl_c3;   // imaginary parts of the Caldeira-Leggett Horner coefficients
@@ -47,13 +62,15 @@ struct BArgs {
   const BInst* inst;
   const int2* xitems;    // (instance, first row)
   const int2* pitems;    // (instance, first column)
-  float2* W;
-  const float2* tw;
+  float* W;              // packed real states
+  const float2* tw;      // register-FFT twiddles, FP32
+  const double2* tw64;   // the same tables in FP64 (same offsets)
   const float* ft;
+  const double* fd;
   double* partials;      // [n_pitems][NACC]
   unsigned* counters;    // [n_inst]
   unsigned* tickets;     // [2] work-list tickets of the x- and p-pass (zero between launches)
-  double2* scale;        // [n_inst]
+  double* scale;         // [n_inst] pending normalisation, applied by the next x-pass
   double* obs;           // [n_inst][obs_stride][NOBS]
   int obs_stride;
 };
@@ -98,6 +115,14 @@ __device__ __forceinline__ float2 turn_factor(double t, float r) {
   return make_float2(r * cs, -r * sn);
 }
 
+// e^{-2 pi i t} * r in FP64, t reduced to one turn
+__device__ __forceinline__ double2 turn_factor64(double t, double r) {
+  const double f = t - rint(t);
+  double sn, cs;
+  sincospi(2. * f, &sn, &cs);
+  return make_double2(r * cs, -r * sn);
+}
+
 struct Kahan {
   double s = 0., c = 0.;
   __device__ __forceinline__ void add(double v) {
@@ -107,13 +132,12 @@ struct Kahan {
   }
 };
 
-__device__ __forceinline__ void accumulate_obs_k(Kahan (&acc)[NACC], float2 v, double x, double p,
+__device__ __forceinline__ void accumulate_obs_k(Kahan (&acc)[NACC], float v, double x, double p,
                                                  const BInst& I) {
-  const double w = v.x;
+  const double w = v;
   const double dV = (4. * I.v4 * x * x + 2. * I.v2) * x + I.v1;
   const double V = ((I.v4 * x * x + I.v2) * x + I.v1) * x + I.v0;
   acc[0].add(w);
-  acc[1].add((double)v.y);
   acc[2].add(w * x);
   acc[3].add(w * x * x);
   acc[4].add(w * p);
@@ -160,12 +184,10 @@ __device__ __forceinline__ void batch_item_done(const BArgs& A, int inst, const 
   __syncthreads();
   if (threadIdx.x == 0) {
     const double dXdP = I.dx * I.dp;
-    const double2 S = make_double2(tot[0], tot[1]);
-    double2 s = make_double2(1., 0.);
-    if (mode == 1) s = crecip(make_double2(S.x * dXdP, S.y * dXdP));
+    const double s = mode == 1 ? 1. / (tot[0] * dXdP) : 1.;   // W is real: a real sum
     double* o = A.obs + ((size_t)inst * A.obs_stride + sample) * NOBS;
-    o[0] = (s.x * S.x - s.y * S.y) * dXdP;
-    for (int k = 1; k < NOBS; ++k) o[k] = s.x * (dXdP * tot[k + 1]);
+    o[0] = s * tot[0] * dXdP;
+    for (int k = 1; k < NOBS; ++k) o[k] = s * (dXdP * tot[k + 1]);
     A.scale[inst] = s;
     A.counters[inst] = 0u;
   }
@@ -207,7 +229,7 @@ __device__ __forceinline__ int next_item(unsigned* ticket, int n_items) {
 // one p step, so fb = fa g(lambda) with g = exp(-i dt dp lambda / m), a table.
 // One transform pair per two rows.
 template <int N>
-__device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BInst& I, int row0) {
+__device__ __forceinline__ void batch_x_item_f32(const BArgs& A, int inst, const BInst& I, int row0) {
   typedef RegFft<float2, N> F;
   constexpr int E = F::E, G = F::G, Q = F::Q, SPW = rf_spw(N);
   constexpr int XS = N + (G == 8 ? 8 : 0);
@@ -220,16 +242,12 @@ __device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BIn
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
   const int pair = warp * SPW + grp;
   const int ra = row0 + 2 * pair;
-  const double2 sd = A.scale[inst];
-  const float2 sc = make_float2((float)sd.x, (float)sd.y);
-  float2* Wa = A.W + I.off + (size_t)ra * N;
-  float2* Wb = Wa + N;
+  const float sc = (float)A.scale[inst];
+  float* Wa = A.W + I.off + (size_t)ra * N;
+  float* Wb = Wa + N;
   float2 v[E];
 #pragma unroll
-  for (int m = 0; m < E; ++m) {
-    const float2 a = Wa[g + G * m], b = Wb[g + G * m];
-    v[m] = make_float2(a.x * sc.x - a.y * sc.y, b.x * sc.x - b.y * sc.y);   // Re(W s) of each row
-  }
+  for (int m = 0; m < E; ++m) v[m] = make_float2(Wa[g + G * m] * sc, Wb[g + G * m] * sc);
   const PlainSlot sl{pair * 2 * XS};            // exchange, then the spectrum in natural order
   const PlainSlot sf{pair * 2 * XS + XS};       // row a's kinetic factors
   F::fwd(v, X, sl, tf, g);
@@ -260,9 +278,91 @@ __device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BIn
   F::inv(v, X, sl, ti, g);
 #pragma unroll
   for (int m = 0; m < E; ++m) {
-    Wa[g + G * m] = make_float2(v[m].x, 0.f);
-    Wb[g + G * m] = make_float2(v[m].y, 0.f);
+    Wa[g + G * m] = v[m].x;
+    Wb[g + G * m] = v[m].y;
   }
+}
+
+// Mirror split of a packed FP64 spectrum staged in natural order in the
+// exchange x (slots 0..N-1), in place:
+//   Z'(k) = Z(k) (fa(k) + fb(k)) + conj Z(N - k) (fa(k) - fb(k))
+// (fab(k, &fa, &fb) returns the two sequences' factors with the 1/2 folded in).
+// Each lane of the group owns the mirror pairs (q, N - q), q = g, g + G, ...,
+// q <= N/2, so no other lane reads a slot it rewrites.  The loop stays rolled:
+// one copy of the factor code (FP64 sincospi) per kernel.
+template <int N, int G, class X, class Fab>
+__device__ __forceinline__ void mirror_split64(const X& x, int g, const Fab& fab) {
+#pragma unroll 1
+  for (int q = g; q <= N / 2; q += G) {
+    const int km = (N - q) & (N - 1);
+    const double2 Z = x.get(q), P = x.get(km);
+    double2 fa, fb;
+    fab(q, &fa, &fb);
+    if (q == N / 2) { fa.y = 0.; fb.y = 0.; }       // Nyquist: see nyquist_real
+    const double2 Zn = cadd(cmul(Z, cadd(fa, fb)), cmul(cconj(P), csub(fa, fb)));
+    if (km != q) {
+      fab(km, &fa, &fb);
+      x.put(km, cadd(cmul(P, cadd(fa, fb)), cmul(cconj(Z), csub(fa, fb))));
+    }
+    x.put(q, Zn);
+  }
+}
+
+// The same row pair in FP64 (WIGB_PREC 1): the rows are widened on load, the
+// transform pair, the kinetic factor exp(-i dt lambda p / m) (FP64 sincospi of
+// the turn-reduced argument) and the mirror split run in FP64, and the result
+// is rounded to FP32 once, on store.  The spectrum is staged in natural order
+// in the pair's exchange region (N double2) and split there in place.
+template <int N>
+__device__ __forceinline__ void batch_x_item_f64(const BArgs& A, int inst, const BInst& I, int row0) {
+  typedef RegFft<double2, N> F;
+  constexpr int E = F::E, G = F::G, Q = F::Q, SPW = rf_spw(N);
+  constexpr int XS = N + (G == 8 ? 8 : 0);     // region stride (double2); bx_smem holds 2 XS float2 per pair
+  extern __shared__ float2 smb[];
+  const double2* tf = A.tw64 + I.tw_x;
+  const double2* ti = tf + N;
+  const double* rtab = A.fd + I.fd_x;                                   // exp(-D_lambda lambda^2) / N
+  const double2* gtab = reinterpret_cast<const double2*>(rtab + 2 * N);  // exp(-i dt dp lambda / m)
+  double2* X = reinterpret_cast<double2*>(smb);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
+  const int pair = warp * SPW + grp;
+  const int ra = row0 + 2 * pair;
+  const double sc = A.scale[inst];
+  float* Wa = A.W + I.off + (size_t)ra * N;
+  float* Wb = Wa + N;
+  double2 v[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m) v[m] = make_double2((double)Wa[g + G * m] * sc, (double)Wb[g + G * m] * sc);
+  const SlotX<double2, PlainSlot> x{X, PlainSlot{pair * XS}};
+  F::fwdx(v, x, tf, g);
+  __syncwarp();   // the transform's exchange reads are done before the spectrum is staged
+#pragma unroll
+  for (int e = 0; e < E; ++e) x.put(g * Q + e / G + E * (e % G), v[e]);
+  __syncwarp();
+  const double cq = I.dt * I.dp * I.dlambda * (double)shifted(ra, I.n_p) / (I.mass * 6.283185307179586477);
+  mirror_split64<N, G>(x, g, [&](int k, double2* fa, double2* fb) {
+    const int lj = k < N / 2 ? k : k - N;
+    *fa = turn_factor64(cq * (double)lj, 0.5 * __ldg(rtab + k));
+    *fb = cmul(*fa, __ldg(gtab + k));
+  });
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = x.get(g * Q + e / G + E * (e % G));
+  F::invx(v, x, ti, g);
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    Wa[g + G * m] = (float)v[m].x;
+    Wb[g + G * m] = (float)v[m].y;
+  }
+}
+
+template <int N>
+__device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BInst& I, int row0) {
+#if WIGB_PREC == 1
+  batch_x_item_f64<N>(A, inst, I, row0);
+#else
+  batch_x_item_f32<N>(A, inst, I, row0);
+#endif
 }
 
 // ------------------------------------------------------------------ p-pass
@@ -296,14 +396,14 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
   const float* ths = sfp + N;         // theta / N
   float2* tile = smb;                 // after packing, c1's slots hold A (the packed post-Moyal pair)
   const int nx = I.n_x;
-  float2* Wi = A.W + I.off;
+  float* Wi = A.W + I.off;
   // coalesced tile load, one register batch per column group (loads in flight
   // before their shared-memory stores)
   constexpr int PER = CT2 * N / NT, LB = PER / BP_PACK;
   static_assert(PER * NT == CT2 * N && PER % LB == 0, "tile load shape");
 #pragma unroll 1
   for (int r0 = 0; r0 < PER; r0 += LB) {
-    float2 buf[LB];
+    float buf[LB];
 #pragma unroll
     for (int r = 0; r < LB; ++r) {
       const int e = threadIdx.x + (r0 + r) * NT;
@@ -312,19 +412,13 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
 #pragma unroll
     for (int r = 0; r < LB; ++r) {
       const int e = threadIdx.x + (r0 + r) * NT, k = e / CT2;
-      tile[k * CT2 + ((e & (CT2 - 1)) ^ tile_sw<CT2>(k))] = buf[r];
+      tile[k * CT2 + ((e & (CT2 - 1)) ^ tile_sw<CT2>(k))] = make_float2(buf[r], 0.f);
     }
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
   const int c1 = rf_col<N>(warp, grp), c2 = c1 + CT;
   const TileSlot<CT2> sl1{c1}, sl2{c2};
-  float2 w[E];
-#pragma unroll
-  for (int m = 0; m < E; ++m) {
-    const float2 a = tile[sl1(g + G * m)], b = tile[sl2(g + G * m)];
-    w[m] = make_float2(a.x, b.x);                  // z = Re W(c1) + i Re W(c2)
-  }
   // Moyal factor exp(-i dt [V(x - u) - V(x + u)] / hbar) r_theta mask1 mask2 / N,
   // u = hbar theta / 2 = h j:  V(x - u) - V(x + u) = -2u (a3 + a1 u^2); phase in turns
   const double h = 0.5 * I.hbar * I.dtheta;
@@ -336,10 +430,54 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
   const float mma = __ldg(A.ft + I.ft_x + nx + col0 + c1), mmb = __ldg(A.ft + I.ft_x + nx + col0 + c2);
   const bool damped = I.damp == 1;
   const int n_it = damped ? 4 : 1;
+  float2 w[E];
+#if WIGB_PREC == 1
+  // FP64 Moyal pair: the packed columns are widened, transformed, split with
+  // the spectrum's mirror and multiplied by the FP64 factors in place (the
+  // exchange and the staged spectrum use c1's and c2's slots as doubles, PairX),
+  // transformed back and rounded to FP32 once; the dissipator pairs below run
+  // in FP32 from there.
+  constexpr int it0 = 1;
+  {
+    typedef RegFft<double2, N> F64;
+    const double2* tf64 = A.tw64 + I.tw_p;
+    const double2* ti64 = tf64 + N;
+    const double* rth64 = A.fd + I.fd_p;
+    const double mma64 = __ldg(A.fd + I.fd_x + nx + col0 + c1), mmb64 = __ldg(A.fd + I.fd_x + nx + col0 + c2);
+    double2 z[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) z[m] = make_double2((double)tile[sl1(g + G * m)].x, (double)tile[sl2(g + G * m)].x);
+    const PairX<TileSlot<CT2>> px{reinterpret_cast<double*>(tile), sl1, sl2};
+    F64::fwdx(z, px, tf64, g);
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < E; ++e) px.put(g * Q + e / G + E * (e % G), z[e]);
+    __syncwarp();
+    mirror_split64<N, G>(px, g, [&](int k, double2* fa, double2* fb) {
+      const double j = (double)(k < N / 2 ? k : k - N);
+      const double r = 0.5 * __ldg(rth64 + k);
+      *fa = turn_factor64(j * fma(bea, j * j, ala), r * mma64);
+      *fb = turn_factor64(j * fma(beb, j * j, alb), r * mmb64);
+    });
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < E; ++e) z[e] = px.get(g * Q + e / G + E * (e % G));
+    F64::invx(z, px, ti64, g);
+#pragma unroll
+    for (int m = 0; m < E; ++m) w[m] = make_float2((float)z[m].x, (float)z[m].y);
+  }
+#else
+  constexpr int it0 = 0;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const float2 a = tile[sl1(g + G * m)], b = tile[sl2(g + G * m)];
+    w[m] = make_float2(a.x, b.x);                  // z = Re W(c1) + i Re W(c2)
+  }
+#endif
   // One transform pair per pass through this loop (kept rolled so the kernel
   // holds a single copy of each FFT); the exchange runs in c2's slots.
 #pragma unroll 1
-  for (int it = 0; it < n_it; ++it) {
+  for (int it = it0; it < n_it; ++it) {
     __syncwarp();   // the previous transform's exchange reads are done before slots change
     if (it == 1) {
 #pragma unroll
@@ -405,7 +543,7 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
 #pragma unroll 1
   for (int q = 0; q < 2; ++q) {
     double s0 = 0., s1 = 0., s2 = 0.;
-    float si = 0.f, sn = 0.f;
+    float sn = 0.f;
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       const float2 v = q == 0 ? tile[sl1(g + G * m)] : w[m];
@@ -415,16 +553,14 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
       const double wp = wr * pj;
       s1 += wp;
       s2 = fma(wp, pj, s2);
-      si += v.y;
       sn += fminf(v.x, 0.f);
     }
-    double sid = (double)si, snd = (double)sn;
+    double snd = (double)sn;
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) {
       s0 += __shfl_xor_sync(0xffffffffu, s0, o);
       s1 += __shfl_xor_sync(0xffffffffu, s1, o);
       s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-      sid += __shfl_xor_sync(0xffffffffu, sid, o);
       snd += __shfl_xor_sync(0xffffffffu, snd, o);
     }
     if (g == 0) {
@@ -433,7 +569,6 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
       const double V = ((I.v4 * x * x + I.v2) * x + I.v1) * x + I.v0;
       const double M1 = s1 * I.dp, M2 = s2 * (I.dp * I.dp);
       acc[0] += s0;
-      acc[1] += sid;
       acc[2] += s0 * x;
       acc[3] += s0 * x * x;
       acc[4] += M1;
@@ -453,7 +588,7 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
 #pragma unroll 8
   for (int r = 0; r < PER; ++r) {
     const int e = threadIdx.x + r * NT, k = e / CT2, cc = e & (CT2 - 1);
-    Wi[(size_t)k * nx + col0 + cc] = tile[k * CT2 + (cc ^ tile_sw<CT2>(k))];
+    Wi[(size_t)k * nx + col0 + cc] = tile[k * CT2 + (cc ^ tile_sw<CT2>(k))].x;
   }
   batch_item_done<NT>(A, inst, I, item, acc, I.damp ? 1 : 0, sample);
 }
@@ -465,7 +600,7 @@ __device__ __forceinline__ void batch_reduce_item(const BArgs& A, int inst, cons
   constexpr int CPB = bp_cols(N, WIGB_WARPS);
   constexpr int NT = WIGB_NT;
   const int nx = I.n_x;
-  const float2* Wi = A.W + I.off;
+  const float* Wi = A.W + I.off;
   Kahan acc[NACC];
   for (int e = threadIdx.x; e < CPB * N; e += NT) {
     const int k = e / CPB, c = e - k * CPB;
@@ -482,13 +617,12 @@ template <int N>
 __device__ __forceinline__ void batch_scale_item(const BArgs& A, int inst, const BInst& I, int col0) {
   constexpr int CPB = bp_cols(N, WIGB_WARPS);
   constexpr int NT = WIGB_NT;
-  const double2 sd = A.scale[inst];
-  const float2 sc = make_float2((float)sd.x, (float)sd.y);
-  float2* Wi = A.W + I.off;
+  const float sc = (float)A.scale[inst];
+  float* Wi = A.W + I.off;
   for (int e = threadIdx.x; e < CPB * N; e += NT) {
     const int k = e / CPB, c = e - k * CPB;
     const size_t g = (size_t)k * I.n_x + col0 + c;
-    Wi[g] = cmul(Wi[g], sc);
+    Wi[g] *= sc;
   }
 }
 

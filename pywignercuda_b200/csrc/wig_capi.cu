@@ -31,6 +31,7 @@
 #include "../../include/wigner_b200.h"
 #include "wig_dirac.cuh"
 #include "wig_batch.cuh"
+#include "wig_batch_host.h"
 #include "wig_device_src.inc"   // kJitWignerSource, kJitDiracSource (generated by build.py)
 #include "wig_host.h"
 
@@ -1352,9 +1353,10 @@ extern "C" const char* wig_last_error(void) { return g_last_error.c_str(); }
 int wig_record_error(int code, const char* msg) { return fail(code, "%s", msg); }
 extern "C" int wig_abi_version(void) { return WIG_ABI_VERSION; }
 
-// ======================================================================== batched FP32
+// ======================================================================== batched form
 // Many independent Wigner2D instances (polynomial potentials, uneven grids) in
-// one x-pass and one p-pass launch per step; see wig_batch.cuh.  A run can be
+// one x-pass and one p-pass launch per step, real FP32 storage, FP32 or mixed
+// (FP64 kinetic / Moyal) transforms; see wig_batch.cuh.  A run can be
 // captured once into a CUDA graph (WIG_RUN_GRAPH) and replayed; the tile shape
 // (warps per CTA) is chosen by wigb_autotune from timed candidates.
 namespace {
@@ -1370,42 +1372,10 @@ int batch_smem_p(int n, int warps) { return wig::bp_smem(n, warps) * (int)sizeof
 
 }  // namespace
 
-namespace wighost {
-// exp(-2 pi i m / n) as a float pair: among the pairs within 2 ulp of the
-// extended-precision value, the one with |w|^2 closest to 1 (ties: the closest
-// in angle).  A forward twiddle and its conjugate in the inverse transform then
-// leave the spectral component's magnitude unbiased.
-float2 twiddle_f(int n, long long m) {
-  const long double pi = 3.141592653589793238462643383279502884L;
-  const long double a = 2.0L * pi * (long double)(m % n) / (long double)n;
-  const long double c = cosl(a), s = -sinl(a);
-  const float c0 = (float)c, s0 = (float)s;
-  float bc = c0, bs = s0;
-  long double best = 1e30L;
-  for (int i = -2; i <= 2; ++i)
-    for (int j = -2; j <= 2; ++j) {
-      float cc = c0, ss = s0;
-      for (int k = 0; k < (i < 0 ? -i : i); ++k) cc = nextafterf(cc, i > 0 ? 2.f : -2.f);
-      for (int k = 0; k < (j < 0 ? -j : j); ++k) ss = nextafterf(ss, j > 0 ? 2.f : -2.f);
-      const long double d = fabsl((long double)cc * cc + (long double)ss * ss - 1.0L);
-      const long double key = d + 1e-3L * (fabsl((long double)cc - c) + fabsl((long double)ss - s));
-      if (key < best) { best = key; bc = cc; bs = ss; }
-    }
-  return make_float2(bc, bs);
-}
-
-void rf_twiddles(int n, std::vector<float2>* tw) {
-  const int E = wig::rf_e(n), G = wig::rf_g(n), Q = E / G;
-  for (int a = 0; a < E; ++a)
-    for (int g = 0; g < G; ++g) tw->push_back(twiddle_f(n, (long long)g * a));
-  for (int i = 0; i < Q; ++i)
-    for (int b = 0; b < G; ++b)
-      for (int t = 0; t < G; ++t) tw->push_back(twiddle_f(n, (long long)b * (t * Q + i)));
-}
-}  // namespace wighost
 
 struct wigb_handle {
   int device = 0, count = 0, n_sm = 148;
+  int precision = WIGB_PREC_F32;
   std::vector<wigb_instance> inst;
   std::vector<wig::BInst> binst;
   std::vector<int> classes;
@@ -1428,15 +1398,24 @@ struct wigb_handle {
   void* g_stream = nullptr;
   std::vector<cudaEvent_t> ev;      // WIG_RUN_PROFILE (non-graph runs): 3 events per step
   size_t ev_used = 0;
+  void* flush = nullptr;            // WIG_RUN_FLUSH_L2 buffer (twice the L2 size)
+  size_t flush_bytes = 0;
 };
 
-static std::string wigb_source(const std::vector<int>& classes, int warps) {
-  // register cap: 8-warp tiles run one CTA per SM (255 registers), smaller
-  // tiles three 4-warp / six 2-warp CTAs (168 registers)
-  char head[192];
-  const int minb = warps == 8 ? 1 : 12 / warps;
-  snprintf(head, sizeof(head), "#define WIGB_WARPS %d\n#define WIGB_XMINB %d\n#define WIGB_PMINB %d\n#define WIGB_CASES(F)",
-           warps, minb, minb);
+static std::string wigb_source(const std::vector<int>& classes, int warps, int precision) {
+  // register cap: 8-warp tiles run one CTA per SM (255 registers); smaller FP32
+  // tiles three 4-warp / six 2-warp CTAs (168 registers), mixed-precision ones
+  // two 4-warp / four 2-warp CTAs (255: an FP64 sequence of 32 elements per
+  // lane is 128 registers)
+  char head[256];
+  const int minb = warps == 8 ? 1 : (precision == WIGB_PREC_MIXED ? 8 : 12) / warps;
+  // tuning override (read per compile): WIG_BATCH_NOINLINE=1 compiles each size class's
+  // pass body as its own function
+  const char* ni = getenv("WIG_BATCH_NOINLINE");
+  const int noinline = ni && atoi(ni) ? 1 : 0;
+  snprintf(head, sizeof(head),
+           "#define WIGB_WARPS %d\n#define WIGB_PREC %d\n#define WIGB_XMINB %d\n#define WIGB_PMINB %d\n"
+           "#define WIGB_NOINLINE %d\n#define WIGB_CASES(F)", warps, precision, minb, minb, noinline);
   std::string src = head;
   for (int n : classes) src += " F(" + std::to_string(n) + ")";
   src += "\n";
@@ -1444,8 +1423,10 @@ static std::string wigb_source(const std::vector<int>& classes, int warps) {
   return src;
 }
 
-extern "C" int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t warps, char* log, int64_t log_cap) {
-  if (!sizes || n_sizes < 1 || (warps != 2 && warps != 4 && warps != 8)) {
+extern "C" int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t warps, int32_t precision, char* log,
+                              int64_t log_cap) {
+  if (!sizes || n_sizes < 1 || (warps != 2 && warps != 4 && warps != 8) ||
+      (precision != WIGB_PREC_F32 && precision != WIGB_PREC_MIXED)) {
     fail(WIG_ERR_ARG, "wigb_jit_check: bad arguments");
     copy_log(g_last_error, log, log_cap);
     return WIG_ERR_ARG;
@@ -1456,13 +1437,13 @@ extern "C" int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t war
   std::lock_guard<std::mutex> lk(g_mu);
   std::vector<char> cubin;
   std::string lg;
-  int rc = nvrtc_compile(wigb_source(cls, warps), &cubin, &lg, true);
+  int rc = nvrtc_compile(wigb_source(cls, warps, precision), &cubin, &lg, true);
   copy_log(rc ? g_last_error : lg, log, log_cap);
   return rc;
 }
 
 static int wigb_compile(wigb_handle* h, int warps, BVariant* v) {
-  const std::string src = wigb_source(h->classes, warps);
+  const std::string src = wigb_source(h->classes, warps, h->precision);
   int smx = 0, smp = 0;
   for (int n : h->classes) {
     smx = std::max(smx, batch_smem_x(n, warps));
@@ -1543,6 +1524,7 @@ extern "C" int wigb_destroy(wigb_handle* h) {
   cudaDeviceSynchronize();
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->flush) cudaFree(h->flush);
   h->bufs.free_all();
   if (h->items_d) cudaFree(h->items_d);
   if (h->partials_d) cudaFree(h->partials_d);
@@ -1551,9 +1533,12 @@ extern "C" int wigb_destroy(wigb_handle* h) {
   return WIG_OK;
 }
 
-extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t warps, wigb_handle** out) {
+extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t warps, int32_t precision,
+                           wigb_handle** out) {
   if (!inst || !out || count < 1) return fail(WIG_ERR_ARG, "wigb_create: empty batch");
   *out = nullptr;
+  if (precision != WIGB_PREC_F32 && precision != WIGB_PREC_MIXED)
+    return fail(WIG_ERR_ARG, "wigb_create: precision must be WIGB_PREC_F32 or WIGB_PREC_MIXED");
   for (int64_t i = 0; i < count; ++i) {
     const wigb_instance& d = inst[i];
     if (d.n_x < 64 || d.n_x > 1024 || d.n_p < 64 || d.n_p > 1024 || (d.n_x & (d.n_x - 1)) || (d.n_p & (d.n_p - 1)))
@@ -1579,86 +1564,42 @@ extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t war
   std::sort(cls.begin(), cls.end());
   cls.erase(std::unique(cls.begin(), cls.end()), cls.end());
   h->classes = cls;
+  h->precision = precision;
   std::vector<float2> tw;
+  std::vector<double2> tw64;
   std::map<int, int> tw_off;
-  for (int n : cls) {
-    tw_off[n] = (int)tw.size();
-    rf_twiddles(n, &tw);
-  }
+  batch_twiddles(cls, &tw, &tw64, &tw_off);
   h->binst.resize(count);
   h->offsets.resize(count + 1);
   std::vector<float> ft;
+  std::vector<double> fd;
   int64_t off = 0;
   for (int64_t i = 0; i < count; ++i) {
     const wigb_instance& d = h->inst[i];
     wig::BInst& b = h->binst[i];
     memset(&b, 0, sizeof(b));
-    b.n_x = d.n_x; b.n_p = d.n_p;
-    b.damp = d.gamma != 0. ? 1 : 0;
-    b.ff = d.damping_f;
+    batch_instance_setup(d, b, &ft, &fd);
     b.off = off;
     h->offsets[i] = off;
     off += (int64_t)d.n_x * d.n_p;
-    b.tw_x = tw_off[d.n_x]; b.tw_p = tw_off[d.n_p];
-    b.dt = d.dt; b.hbar = d.hbar; b.mass = d.mass;
-    b.dx = 2. * d.x_amplitude / d.n_x; b.dp = 2. * d.p_amplitude / d.n_p;
-    b.dtheta = 2. * M_PI / (2. * d.p_amplitude); b.dlambda = 2. * M_PI / (2. * d.x_amplitude);
-    b.D_theta = d.d_theta; b.D_lambda = d.d_lambda; b.f_eps = d.f_eps;
-    b.v4 = d.v4; b.v2 = d.v2; b.v1 = d.v1; b.v0 = d.v0;
-    // CaldeiraDissipatorOrder3 (GPU_Wigner2D_FFT.py:1145-1157) in Horner form, imaginary parts
-    const double g = d.dt * d.gamma, c1 = 2. / 3. * g, c2 = g, c3 = 2. * g;
-    b.cl_k1 = (c1 + c2) != 0. ? c1 * c2 / (c1 + c2) : 0.;
-    b.cl_k12 = c1 + c2;
-    b.cl_c3 = c3;
-    // per-frequency / per-column factors (expPLambda_source :153, expPotential_source :117-123,
-    // theta_fp_source :422-428), FP64 then rounded once
-    b.ft_x = (int)ft.size();
-    for (int k = 0; k < d.n_x; ++k) {   // r_lambda / n_x
-      const double lam = b.dlambda * (((k + d.n_x / 2) % d.n_x) - 0.5 * d.n_x);
-      ft.push_back((float)(exp(-b.D_lambda * lam * lam) / (double)d.n_x));
-    }
-    const double x_max = b.dx * (d.n_x - 1.) / 2.;
-    for (int k = 0; k < d.n_x; ++k) {   // mask1 mask2 / n_p
-      const double x = b.dx * (((k + d.n_x / 2) % d.n_x) - 0.5 * d.n_x);
-      const double w2 = (10. * b.dx) * (10. * b.dx);
-      const double m1 = 1. - exp(-(x - x_max) * (x - x_max) / w2), m2 = 1. - exp(-(x + x_max) * (x + x_max) / w2);
-      ft.push_back((float)(m1 * m2 / (double)d.n_p));
-    }
-    // exp(-i dt dp lambda / m) per x-frequency: the kinetic factor of row p + dp over that of
-    // row p (the x-pass carries rows 2r and 2r + 1 together), as (cos, -sin) of the turn
-    for (int k = 0; k < d.n_x; ++k) {
-      const int lj = k < d.n_x / 2 ? k : k - d.n_x;
-      double t = b.dt * b.dp * b.dlambda * (double)lj / (b.mass * 2. * M_PI);
-      t -= rint(t);
-      ft.push_back((float)cos(2. * M_PI * t));
-      ft.push_back((float)(-sin(2. * M_PI * t)));
-    }
-    b.ft_p = (int)ft.size();
-    for (int k = 0; k < d.n_p; ++k) {   // r_theta
-      const double th = b.dtheta * (((k + d.n_p / 2) % d.n_p) - 0.5 * d.n_p);
-      ft.push_back((float)exp(-b.D_theta * th * th * b.dt));
-    }
-    for (int k = 0; k < d.n_p; ++k) {   // sign(p) f(p)
-      const double p = b.dp * (((k + d.n_p / 2) % d.n_p) - 0.5 * d.n_p);
-      const double f = b.ff == 0 ? fabs(p) : p * p / sqrt(p * p + b.f_eps);
-      ft.push_back((float)(p >= 0. ? f : -f));
-    }
-    for (int k = 0; k < d.n_p; ++k) {   // theta / n_p
-      const double th = b.dtheta * (((k + d.n_p / 2) % d.n_p) - 0.5 * d.n_p);
-      ft.push_back((float)(th / (double)d.n_p));
-    }
+    b.tw_x = tw_off[d.n_x];
+    b.tw_p = tw_off[d.n_p];
   }
   h->total = off;
   h->offsets[count] = off;
   DevBuf& B = h->bufs;
   float2* tw_d = nullptr;
+  double2* tw64_d = nullptr;
   float* ft_d = nullptr;
+  double* fd_d = nullptr;
   wig::BInst* inst_d = nullptr;
   unsigned* cnt_d = nullptr;
   unsigned* tick_d = nullptr;
-  double2* scale_d = nullptr;
+  double* scale_d = nullptr;
   int rc = B.alloc(&tw_d, tw.size(), tw.data());
+  if (!rc) rc = B.alloc(&tw64_d, tw64.size(), tw64.data());
   if (!rc) rc = B.alloc(&ft_d, ft.size(), ft.data());
+  if (!rc) rc = B.alloc(&fd_d, fd.size(), fd.data());
   if (!rc) rc = B.alloc(&inst_d, (size_t)count);
   if (!rc) rc = B.alloc(&cnt_d, (size_t)count);
   if (!rc) rc = B.alloc(&tick_d, (size_t)2);
@@ -1670,7 +1611,9 @@ extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t war
   }
   if (rc) { B.free_all(); delete h; return rc; }
   h->a.tw = tw_d;
+  h->a.tw64 = tw64_d;
   h->a.ft = ft_d;
+  h->a.fd = fd_d;
   h->a.inst = inst_d;
   h->a.counters = cnt_d;
   h->a.tickets = tick_d;
@@ -1686,7 +1629,7 @@ extern "C" int wigb_offsets(wigb_handle* h, int64_t* offsets) {
   return WIG_OK;
 }
 
-static int wigb_launch_run(wigb_handle* h, float2* W, int64_t t_index0, int64_t n_prop, uint32_t flags,
+static int wigb_launch_run(wigb_handle* h, float* W, int64_t t_index0, int64_t n_prop, uint32_t flags,
                            cudaStream_t st) {
   const BVariant& v = h->variants[h->warps];
   wig::BArgs a = h->a;
@@ -1709,7 +1652,9 @@ static int wigb_launch_run(wigb_handle* h, float2* W, int64_t t_index0, int64_t 
     }
     h->ev_used = 3 * (size_t)n_prop;
   }
+  const bool flush = prof && (flags & WIG_RUN_FLUSH_L2) && h->flush;
   for (int64_t n = 0; n < n_prop; ++n) {
+    if (flush) WIG_CUDA(cudaMemsetAsync(h->flush, (int)(n & 0x7f), h->flush_bytes, st));
     if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n], st));
     void* xargs[] = {&a, &nxi};
     if (int rc = launch(v.fx, h->grid_x, nt, v.smem_x, st, xargs)) return rc;
@@ -1737,7 +1682,13 @@ extern "C" int wigb_run(wigb_handle* h, void* W_dev, int64_t t_index0, int64_t n
     if (int rc = ensure_obs(&h->obs, &h->obs_cap, nobs)) return rc;
   }
   cudaStream_t st = (cudaStream_t)stream;
-  float2* W = (float2*)W_dev;
+  float* W = (float*)W_dev;
+  if ((flags & WIG_RUN_FLUSH_L2) && (flags & WIG_RUN_PROFILE) && !(flags & WIG_RUN_GRAPH) && !h->flush) {
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, h->device);
+    h->flush_bytes = 2 * (size_t)std::max(l2, 64 << 20);
+    WIG_CUDA(cudaMalloc(&h->flush, h->flush_bytes));
+  }
   if (flags & WIG_RUN_GRAPH) {
     const uint32_t key_flags = flags & ~(uint32_t)WIG_RUN_GRAPH;
     if (!(h->gexec && h->g_W == W_dev && h->g_t0 == t_index0 && h->g_n == n_prop && h->g_flags == key_flags &&

@@ -37,11 +37,6 @@ int launch(CUfunction f, unsigned grid, unsigned block, unsigned smem, cudaStrea
 int copy_log(const std::string& log, char* out, int64_t cap);
 // Blocks that can be resident per SM for a launch shape (1 when the query is unavailable).
 int occupancy(CUfunction f, int threads, int dyn_smem);
-// exp(-2 pi i m / n) as the float pair within 2 ulp whose |w|^2 is closest to 1.
-float2 twiddle_f(int n, long long m);
-// Register-FFT twiddle tables of size n (wig_rfft.cuh), appended to *tw (2n entries):
-// forward tf[a G + g] = W_n^{g a}, inverse ti[(i G + b) G + t] = W_n^{b (t Q + i)}.
-void rf_twiddles(int n, std::vector<float2>* tw);
 
 int launch2d(CUfunction f, unsigned gx, unsigned gy, unsigned block, unsigned smem, cudaStream_t st, void** args);
 bool pow2_in_range(int n);                    // power of two in [16, 4096]

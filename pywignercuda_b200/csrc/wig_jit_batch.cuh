@@ -2,6 +2,7 @@
 // (its set of grid-size classes and tile shape).  The host prepends
 //   #define WIGB_WARPS <warps per CTA>   (the autotuned tile shape)
 //   #define WIGB_CASES(F) F(128) F(256) ...   (the size classes present)
+//   #define WIGB_PREC 0 | 1                      (FP32 / mixed precision, wig_batch.cuh)
 // Each kernel is persistent over its work list: the x- and p-pass draw items
 // from a ticket counter, the one-off reduce / scale kernels take items
 // b, b + gridDim.x, ...
@@ -15,8 +16,26 @@
 #define WIGB_PMINB 1
 #endif
 
-#define WIGB_X_CASE(N) case N: wig::batch_x_item<N>(A, it.x, sI, it.y); break;
-#define WIGB_P_CASE(N) case N: wig::batch_p_item<N>(A, it.x, sI, it.y, item, sample); break;
+// WIGB_NOINLINE 1: each size class's pass body is its own (non-inlined)
+// function, so registers are allocated per class rather than over the union of
+// every class's code (at the cost of a call and a stack frame per item).
+#ifndef WIGB_NOINLINE
+#define WIGB_NOINLINE 0
+#endif
+#if WIGB_NOINLINE
+#define WIGB_CASE_INLINE __noinline__
+#else
+#define WIGB_CASE_INLINE __forceinline__
+#endif
+template <int N> __device__ WIGB_CASE_INLINE void wigb_x_case(const wig::BArgs& A, int inst, const wig::BInst& I, int row0) {
+  wig::batch_x_item<N>(A, inst, I, row0);
+}
+template <int N> __device__ WIGB_CASE_INLINE void wigb_p_case(const wig::BArgs& A, int inst, const wig::BInst& I, int col0,
+                                                          int item, int sample) {
+  wig::batch_p_item<N>(A, inst, I, col0, item, sample);
+}
+#define WIGB_X_CASE(N) case N: wigb_x_case<N>(A, it.x, sI, it.y); break;
+#define WIGB_P_CASE(N) case N: wigb_p_case<N>(A, it.x, sI, it.y, item, sample); break;
 #define WIGB_R_CASE(N) case N: wig::batch_reduce_item<N>(A, it.x, sI, it.y, item, mode, sample); break;
 #define WIGB_S_CASE(N) case N: wig::batch_scale_item<N>(A, it.x, sI, it.y); break;
 

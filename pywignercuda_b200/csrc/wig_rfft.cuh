@@ -45,27 +45,27 @@ template <class C, int N> struct RegFft {
   static constexpr int E = rf_e(N), G = rf_g(N), Q = E / G;
   static_assert(E * G == N && E >= G && (N & (N - 1)) == 0, "RegFft: N must be a power of two in [64, 1024]");
 
-  // lane g (0 <= g < G) of its group; slot(s) maps the sequence's slot s < N to
-  // a shared-memory index.
-  template <class Slot>
-  __device__ __forceinline__ static void fwd(C (&v)[E], C* sm, const Slot& slot, const C* tf, int g) {
+  // lane g (0 <= g < G) of its group; x.put(s, v) / x.get(s) store and load
+  // the sequence's exchange slot s < N (an exchange functor, see SlotX / PairX).
+  template <class X>
+  __device__ __forceinline__ static void fwdx(C (&v)[E], const X& x, const C* tf, int g) {
     dft_r<E, false>(v);
 #pragma unroll
     for (int a = 1; a < E; ++a) v[a] = cmul(v[a], __ldg(tf + a * G + g));
     __syncwarp();
 #pragma unroll
-    for (int a = 0; a < E; ++a) sm[slot(a * G + (g ^ ((a / Q) & (G - 1))))] = v[a];
+    for (int a = 0; a < E; ++a) x.put(a * G + (g ^ ((a / Q) & (G - 1))), v[a]);
     __syncwarp();
 #pragma unroll
     for (int i = 0; i < Q; ++i)
 #pragma unroll
-      for (int b = 0; b < G; ++b) v[i * G + b] = sm[slot((g * Q + i) * G + (b ^ g))];
+      for (int b = 0; b < G; ++b) v[i * G + b] = x.get((g * Q + i) * G + (b ^ g));
 #pragma unroll
     for (int i = 0; i < Q; ++i) dft_r<G, false>(&v[i * G]);
   }
 
-  template <class Slot>
-  __device__ __forceinline__ static void inv(C (&v)[E], C* sm, const Slot& slot, const C* ti, int g) {
+  template <class X>
+  __device__ __forceinline__ static void invx(C (&v)[E], const X& x, const C* ti, int g) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) dft_r<G, true>(&v[i * G]);
 #pragma unroll
@@ -77,12 +77,18 @@ template <class C, int N> struct RegFft {
 #pragma unroll
     for (int i = 0; i < Q; ++i)
 #pragma unroll
-      for (int b = 0; b < G; ++b) sm[slot((g * Q + i) * G + (b ^ g))] = v[i * G + b];
+      for (int b = 0; b < G; ++b) x.put((g * Q + i) * G + (b ^ g), v[i * G + b]);
     __syncwarp();
 #pragma unroll
-    for (int a = 0; a < E; ++a) v[a] = sm[slot(a * G + (g ^ ((a / Q) & (G - 1))))];
+    for (int a = 0; a < E; ++a) v[a] = x.get(a * G + (g ^ ((a / Q) & (G - 1))));
     dft_r<E, true>(v);
   }
+
+  // slot(s) maps the sequence's slot s < N to an index of sm (same element type)
+  template <class Slot>
+  __device__ __forceinline__ static void fwd(C (&v)[E], C* sm, const Slot& slot, const C* tf, int g);
+  template <class Slot>
+  __device__ __forceinline__ static void inv(C (&v)[E], C* sm, const Slot& slot, const C* ti, int g);
 
   // frequency index of element (i, b) of lane t after fwd
   __device__ __forceinline__ static int kfreq(int t, int i, int b) { return t * Q + i + E * b; }
@@ -102,5 +108,34 @@ template <int CT> struct TileSlot {
   int c;
   __device__ __forceinline__ int operator()(int k) const { return k * CT + (c ^ tile_sw<CT>(k)); }
 };
+
+// Exchange functors of RegFft::fwdx / invx.
+// SlotX: element s at sm[slot(s)] (the element type of the transform).
+template <class C, class Slot> struct SlotX {
+  C* sm;
+  Slot slot;
+  __device__ __forceinline__ void put(int s, C v) const { sm[slot(s)] = v; }
+  __device__ __forceinline__ C get(int s) const { return sm[slot(s)]; }
+};
+// PairX: an FP64 sequence exchanged through the 8-byte slots of two columns of
+// a float2 tile: the real part of element s in slot s of column 1, the
+// imaginary part in slot s of column 2 (each slot reinterpreted as one double).
+template <class Slot> struct PairX {
+  double* sm;
+  Slot s1, s2;
+  __device__ __forceinline__ void put(int s, double2 v) const { sm[s1(s)] = v.x; sm[s2(s)] = v.y; }
+  __device__ __forceinline__ double2 get(int s) const { return make_double2(sm[s1(s)], sm[s2(s)]); }
+};
+
+template <class C, int N>
+template <class Slot>
+__device__ __forceinline__ void RegFft<C, N>::fwd(C (&v)[E], C* sm, const Slot& slot, const C* tf, int g) {
+  fwdx(v, SlotX<C, Slot>{sm, slot}, tf, g);
+}
+template <class C, int N>
+template <class Slot>
+__device__ __forceinline__ void RegFft<C, N>::inv(C (&v)[E], C* sm, const Slot& slot, const C* ti, int g) {
+  invx(v, SlotX<C, Slot>{sm, slot}, ti, g);
+}
 
 }  // namespace wig

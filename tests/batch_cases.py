@@ -33,3 +33,19 @@ def to_params(c, dt=0.005):
 def initial_state(c):
     prm = to_params(c)
     return np.ascontiguousarray(wigner_harmonic_oscillator(prm, 0, 1., c['x0'], c['p0']))
+
+
+def config3_cases(seed=0, count=64):
+    """The 64-instance mixed-grid batch: square grids from {128, 256, 512, 1024},
+    a ~ U[0.01, 0.1], b ~ U[-1, 0.5], gamma ~ U[0, 0.2], D_theta = 2 gamma m kT
+    (kT = 0.5), coherent states at x0 ~ U[-2, 2], p0 ~ U[-1, 1], in the draw order
+    of numpy default_rng(seed) that the benchmark uses."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice([128, 256, 512, 1024], size=count)
+    a = rng.uniform(0.01, 0.1, count)
+    b = rng.uniform(-1., 0.5, count)
+    g = rng.uniform(0., 0.2, count)
+    x0 = rng.uniform(-2., 2., count)
+    p0 = rng.uniform(-1., 1., count)
+    return [dict(n=int(sizes[i]), a=float(a[i]), b=float(b[i]), gamma=float(g[i]), d_theta=float(g[i]),
+                 x0=float(x0[i]), p0=float(p0[i])) for i in range(count)]

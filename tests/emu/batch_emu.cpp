@@ -1,7 +1,8 @@
-// Host execution of the batched FP32 Wigner2D kernels (csrc/wig_jit_batch.cuh)
+// Host execution of the batched Wigner2D kernels (csrc/wig_jit_batch.cuh)
 // in the launch sequence of wigb_run (csrc/wig_capi.cu: wigb_launch_run), over
-// the work lists and tables wigb_create / wigb_set_warps build.  WIGB_WARPS
-// and WIGB_CASES come from the command line.  Test infrastructure:
+// the tables wigb_create builds (csrc/wig_batch_host.h, shared with the
+// library) and the work lists of wigb_set_warps.  WIGB_WARPS, WIGB_PREC and
+// WIGB_CASES come from the command line.  Test infrastructure:
 // tests/test_emu_cpu.py builds it and compares the result with the oracle.
 //
 //   batch_emu params W_in W_out obs_out n_prop grid
@@ -9,84 +10,22 @@
 // params: count x 14 doubles per instance: n_x, n_p, v4, v2, v1, v0, gamma,
 // d_theta, d_lambda, dt, x_amplitude, p_amplitude, damping_f (0: |p|, 1:
 // p^2 / sqrt(p^2 + f_eps)), f_eps; hbar = mass = 1.  W_in / W_out: the
-// instances' (n_p, n_x) states one after another, complex64.  obs_out: count x
-// (n_prop + 1) x 11 doubles.  grid: CTAs of every launch.
+// instances' (n_p, n_x) real states one after another, float32.  obs_out:
+// count x (n_prop + 1) x 11 doubles.  grid: CTAs of every launch.
 #include "shim.h"
 #include "wig_jit_batch.cuh"
+#include "wig_batch_host.h"
 
 #include <algorithm>
 #include <map>
 
 namespace {
 
-// the host's FP32 twiddle: among the float pairs within 2 ulp of exp(-2 pi i m / n), the
-// one with |w|^2 closest to 1 (ties: the closest in angle)
-float2 twiddle_f(int n, long long m) {
-  const long double pi = 3.141592653589793238462643383279502884L;
-  const long double a = 2.0L * pi * (long double)(m % n) / (long double)n;
-  const long double c = cosl(a), s = -sinl(a);
-  const float c0 = (float)c, s0 = (float)s;
-  float bc = c0, bs = s0;
-  long double best = 1e30L;
-  for (int i = -2; i <= 2; ++i)
-    for (int j = -2; j <= 2; ++j) {
-      float cc = c0, ss = s0;
-      for (int k = 0; k < (i < 0 ? -i : i); ++k) cc = nextafterf(cc, i > 0 ? 2.f : -2.f);
-      for (int k = 0; k < (j < 0 ? -j : j); ++k) ss = nextafterf(ss, j > 0 ? 2.f : -2.f);
-      const long double d = fabsl((long double)cc * cc + (long double)ss * ss - 1.0L);
-      const long double key = d + 1e-3L * (fabsl((long double)cc - c) + fabsl((long double)ss - s));
-      if (key < best) { best = key; bc = cc; bs = ss; }
-    }
-  return make_float2(bc, bs);
-}
-
-void rf_twiddles(int n, std::vector<float2>* tw) {
-  const int E = wig::rf_e(n), G = wig::rf_g(n), Q = E / G;
-  for (int a = 0; a < E; ++a)
-    for (int g = 0; g < G; ++g) tw->push_back(twiddle_f(n, (long long)g * a));
-  for (int i = 0; i < Q; ++i)
-    for (int b = 0; b < G; ++b)
-      for (int t = 0; t < G; ++t) tw->push_back(twiddle_f(n, (long long)b * (t * Q + i)));
-}
-
-// wigb_create's per-instance float tables: [r_lambda / n_x][masks / n_p][(cos, -sin) of the
-// row-pair kinetic ratio] and [r_theta][sign(p) f(p)][theta / n_p]
-void instance_tables(wig::BInst& b, std::vector<float>* ft) {
-  const int nx = b.n_x, np = b.n_p;
-  b.ft_x = (int)ft->size();
-  for (int k = 0; k < nx; ++k) {
-    const double lam = b.dlambda * (((k + nx / 2) % nx) - 0.5 * nx);
-    ft->push_back((float)(exp(-b.D_lambda * lam * lam) / (double)nx));
-  }
-  const double x_max = b.dx * (nx - 1.) / 2.;
-  for (int k = 0; k < nx; ++k) {
-    const double x = b.dx * (((k + nx / 2) % nx) - 0.5 * nx);
-    const double w2 = (10. * b.dx) * (10. * b.dx);
-    const double m1 = 1. - exp(-(x - x_max) * (x - x_max) / w2), m2 = 1. - exp(-(x + x_max) * (x + x_max) / w2);
-    ft->push_back((float)(m1 * m2 / (double)np));
-  }
-  for (int k = 0; k < nx; ++k) {
-    const int lj = k < nx / 2 ? k : k - nx;
-    double t = b.dt * b.dp * b.dlambda * (double)lj / (b.mass * 2. * M_PI);
-    t -= rint(t);
-    ft->push_back((float)cos(2. * M_PI * t));
-    ft->push_back((float)(-sin(2. * M_PI * t)));
-  }
-  b.ft_p = (int)ft->size();
-  for (int k = 0; k < np; ++k) {
-    const double th = b.dtheta * (((k + np / 2) % np) - 0.5 * np);
-    ft->push_back((float)exp(-b.D_theta * th * th * b.dt));
-  }
-  for (int k = 0; k < np; ++k) {
-    const double p = b.dp * (((k + np / 2) % np) - 0.5 * np);
-    const double f = b.ff == 0 ? fabs(p) : p * p / sqrt(p * p + b.f_eps);
-    ft->push_back((float)(p >= 0. ? f : -f));
-  }
-  for (int k = 0; k < np; ++k) {
-    const double th = b.dtheta * (((k + np / 2) % np) - 0.5 * np);
-    ft->push_back((float)(th / (double)np));
-  }
-}
+// the fields of wigb_instance (include/wigner_b200.h) that batch_instance_setup reads
+struct Inst {
+  int n_x, n_p, damping_f;
+  double x_amplitude, p_amplitude, hbar, mass, dt, d_theta, d_lambda, gamma, f_eps, v4, v2, v1, v0;
+};
 
 template <class T>
 bool read_all(const char* path, T* p, size_t n) {
@@ -135,36 +74,27 @@ int main(int argc, char** argv) {
   std::sort(cls.begin(), cls.end());
   cls.erase(std::unique(cls.begin(), cls.end()), cls.end());
   std::vector<float2> tw;
+  std::vector<double2> tw64;
   std::map<int, int> tw_off;
-  for (int n : cls) {
-    tw_off[n] = (int)tw.size();
-    rf_twiddles(n, &tw);
-  }
+  wighost::batch_twiddles(cls, &tw, &tw64, &tw_off);
   std::vector<float> ft;
+  std::vector<double> fd;
   long long off = 0;
   for (int i = 0; i < count; ++i) {
     const double* q = &prm[NPRM * i];
+    Inst d{};
+    d.n_x = (int)q[0]; d.n_p = (int)q[1];
+    d.v4 = q[2]; d.v2 = q[3]; d.v1 = q[4]; d.v0 = q[5];
+    d.gamma = q[6]; d.d_theta = q[7]; d.d_lambda = q[8]; d.dt = q[9];
+    d.x_amplitude = q[10]; d.p_amplitude = q[11];
+    d.damping_f = (int)q[12]; d.f_eps = q[13];
+    d.hbar = 1.; d.mass = 1.;
     wig::BInst& b = inst[i];
     std::memset(&b, 0, sizeof(b));
-    const int nx = (int)q[0], np = (int)q[1];
-    const double gamma = q[6], xa = q[10], pa = q[11];
-    b.n_x = nx; b.n_p = np;
-    b.damp = gamma != 0. ? 1 : 0;
-    b.ff = (int)q[12];
-    b.f_eps = q[13];
+    wighost::batch_instance_setup(d, b, &ft, &fd);
     b.off = off;
-    off += (long long)nx * np;
-    b.tw_x = tw_off[nx]; b.tw_p = tw_off[np];
-    b.dt = q[9]; b.hbar = 1.; b.mass = 1.;
-    b.dx = 2. * xa / nx; b.dp = 2. * pa / np;
-    b.dtheta = 2. * M_PI / (2. * pa); b.dlambda = 2. * M_PI / (2. * xa);
-    b.D_theta = q[7]; b.D_lambda = q[8];
-    b.v4 = q[2]; b.v2 = q[3]; b.v1 = q[4]; b.v0 = q[5];
-    const double g = b.dt * gamma, c1 = 2. / 3. * g, c2 = g, c3 = 2. * g;
-    b.cl_k1 = (c1 + c2) != 0. ? c1 * c2 / (c1 + c2) : 0.;
-    b.cl_k12 = c1 + c2;
-    b.cl_c3 = c3;
-    instance_tables(b, &ft);
+    off += (long long)d.n_x * d.n_p;
+    b.tw_x = tw_off[d.n_x]; b.tw_p = tw_off[d.n_p];
   }
   // wigb_set_warps: work lists, instances ordered by decreasing per-item cost
   std::vector<int> order(count);
@@ -184,16 +114,17 @@ int main(int argc, char** argv) {
     b.n_pitems = b.n_x / cpb;
     for (int c = 0; c < b.n_x; c += cpb) pi.push_back(make_int2(i, c));
   }
-  std::vector<float2> W((size_t)off);
+  std::vector<float> W((size_t)off);
   if (!read_all(argv[2], W.data(), W.size())) return 4;
   std::vector<double> partials(pi.size() * wig::NACC, 0.);
   std::vector<unsigned> counters(count, 0u), tickets(2, 0u);
-  std::vector<double2> scale(count, make_double2(1., 0.));
+  std::vector<double> scale(count, 1.);
   std::vector<double> obs((size_t)count * (n_prop + 1) * wig::NOBS, 0.);
 
   wig::BArgs A{};
   A.inst = inst.data(); A.xitems = xi.data(); A.pitems = pi.data();
-  A.W = W.data(); A.tw = tw.data(); A.ft = ft.data(); A.partials = partials.data();
+  A.W = W.data(); A.tw = tw.data(); A.tw64 = tw64.data(); A.ft = ft.data(); A.fd = fd.data();
+  A.partials = partials.data();
   A.counters = counters.data(); A.tickets = tickets.data(); A.scale = scale.data();
   A.obs = obs.data(); A.obs_stride = (int)(n_prop + 1);
   const int nxi = (int)xi.size(), npi = (int)pi.size();

@@ -76,6 +76,13 @@ inline void sincospif(float x, float* s, float* c) {
   *c = (float)::cos(a);
 }
 
+// sin / cos of pi x in double, from extended precision
+inline void sincospi(double x, double* s, double* c) {
+  const long double a = 3.141592653589793238462643383279502884L * (long double)x;
+  *s = (double)::sinl(a);
+  *c = (double)::cosl(a);
+}
+
 // (grid_x, grid_y) x block threads; a block's threads run concurrently, blocks in turn
 inline void emu_launch2d(unsigned grid_x, unsigned grid_y, unsigned block, const std::function<void()>& body) {
   if (block == 0 || block > 1024 || (block % 32) != 0) {

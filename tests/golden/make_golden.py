@@ -22,9 +22,9 @@ arrays are fed to the reference run); ``init_sum`` records their checksum.
 The reference GPU class needs X_gridDIM to be a multiple of 512 (its kernels
 launch X/512 blocks of 512 threads), so Wigner cases use 512 x-points.
 
-Usage:  PYTHONPATH=. python tests/golden/make_golden.py [case ...]
-This needs the reference checkout (``PYWIGNER_REFERENCE``, default
-``/root/reference``); the tests only read the .npz files it writes.
+Usage:  PYWIGNER_REFERENCE=<reference checkout> PYTHONPATH=. python tests/golden/make_golden.py [case ...]
+The environment variable names the reference checkout; the tests only read
+the .npz files this script writes.
 """
 import json
 import os

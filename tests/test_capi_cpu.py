@@ -188,13 +188,31 @@ def test_python_classes_fail_loudly_without_gpu():
         Inst()
 
 
-def test_batch_jit_compiles_without_spills():
-    sizes = (ctypes.c_int32 * 4)(128, 256, 512, 1024)
+@pytest.mark.parametrize('warps', [8, 4, 2])
+@pytest.mark.parametrize('precision', [0, 1])
+def test_batch_jit_spills_bounded(warps, precision):
+    """All size classes in one kernel.  The FP32 passes at 168 registers (3 / 6 CTAs of
+    4 / 2 warps per SM) spill ~20 bytes in the 1024-point p-pass; the mixed form's FP64
+    Moyal pair holds 32 double2 per lane and spills up to ~270 bytes at 255 registers
+    (each size class alone: at most 40)."""
+    sizes = (ctypes.c_int32 * 5)(64, 128, 256, 512, 1024)
     buf = ctypes.create_string_buffer(1 << 17)
-    rc = _lib.load().wigb_jit_check(sizes, 4, 8, buf, len(buf))
+    rc = _lib.load().wigb_jit_check(sizes, 5, warps, precision, buf, len(buf))
     log = buf.value.decode()
     assert rc == 0, log
-    assert 'wigb_xpass' in log and 'wigb_ppass' in log
+    lines = log.splitlines()
+    for k in ('wigb_xpass', 'wigb_ppass', 'wigb_reduce', 'wigb_scale'):
+        at = [i for i, l in enumerate(lines) if "Compiling entry function '%s'" % k in l]
+        assert at, k
+        props = ' '.join(lines[at[0] + 1:at[0] + 3])
+        spill = int(props.split(' bytes spill stores')[0].split()[-1])
+        assert spill <= (32 if precision == 0 else 320), (k, props)
+
+
+def test_batch_precision_validated():
+    sizes = (ctypes.c_int32 * 1)(128)
+    buf = ctypes.create_string_buffer(4096)
+    assert _lib.load().wigb_jit_check(sizes, 1, 4, 2, buf, len(buf)) == 1
 
 
 def d3_desc(nx=64, ny=32, nz=128, **kw):

@@ -26,7 +26,7 @@ CSRC = os.path.join(ROOT, 'pywignercuda_b200', 'csrc')
 EMU = os.path.join(ROOT, 'tests', 'emu')
 HEADERS = ('wig_fft.cuh', 'wig_wigner.cuh', 'wig_dirac.cuh', 'wig_jit_dirac.cuh', 'wig_jit_wigner.cuh',
            'wig_dirac3.cuh', 'wig_jit_dirac3.cuh', 'wig_rfft.cuh', 'wig_batch.cuh', 'wig_jit_batch.cuh',
-           'wig_adjoint.cuh', 'wig_jit_adjoint.cuh')
+           'wig_adjoint.cuh', 'wig_jit_adjoint.cuh', 'wig_batch_host.h')
 EXTERN_SHARED = re.compile(r'extern\s+__shared__\s+(\w+)\s+(\w+)\s*\[\s*\]\s*;')
 
 NX, NY = 32, 16
@@ -210,13 +210,14 @@ BSHAPES = ((64, 128, 10., 8.), (128, 64, 8., 10.))
 BEXTRA = {1: dict(ff=1, f_eps=0.5, d_lambda=0.01, v1=0.3, v0=0.2), 4: dict(v1=-0.2)}
 
 
-@pytest.mark.parametrize('warps,grid', [(4, 3), (2, 5)])
-def test_batch_device_code_matches_oracle(staged, warps, grid):
-    """The FP32 real-storage passes (two rows / columns per complex transform, the
-    Nyquist split), the persistent work lists and the last-CTA normalisation,
-    against the FP64 oracle at FP32 accuracy, 2 steps (each emulated step costs
-    seconds of barrier traffic)."""
-    exe = build(staged, 'batch_emu.cpp', {'WIGB_WARPS': warps, 'WIGB_XMINB': 1, 'WIGB_PMINB': 1,
+@pytest.mark.parametrize('warps,grid,prec', [(4, 3, 0), (2, 5, 0), (4, 3, 1), (2, 5, 1)])
+def test_batch_device_code_matches_oracle(staged, warps, grid, prec):
+    """The real-storage passes (two rows / columns per complex transform, the
+    Nyquist split), in FP32 (prec 0) and with the FP64 kinetic and Moyal pairs
+    and their in-place mirror split (prec 1), the persistent work lists and the
+    last-CTA normalisation, against the FP64 oracle, 2 steps (each emulated step
+    costs seconds of barrier traffic)."""
+    exe = build(staged, 'batch_emu.cpp', {'WIGB_WARPS': warps, 'WIGB_XMINB': 1, 'WIGB_PMINB': 1, 'WIGB_PREC': prec,
                                           'WIGB_CASES(F)': 'F(64) F(128)'})
     cases = random_batch(list(BSIZES) + [s[0] for s in BSHAPES], seed=11)
     cases[2]['gamma'] = 0.
@@ -244,14 +245,14 @@ def test_batch_device_code_matches_oracle(staged, warps, grid):
                             d_theta=c['gamma'], d_lambda=g(c, 'd_lambda'), damping='CaldeiraLeggett',
                             fp_damping=f, constants='exact')
     W0 = [np.ascontiguousarray(wigner_harmonic_oscillator(params(c), 0, 1., c['x0'], c['p0'])) for c in cases]
-    packed = np.concatenate([w.real.astype(np.float32).ravel() for w in W0]).astype(np.complex64)
+    packed = np.concatenate([w.real.astype(np.float32).ravel() for w in W0])
     fprm, fin, fout, fobs = (os.path.join(staged, n) for n in ('b_prm.bin', 'b_in.bin', 'b_out.bin', 'b_obs.bin'))
     prm.tofile(fprm)
     packed.tofile(fin)
     r = subprocess.run([exe, fprm, fin, fout, fobs, str(steps), str(grid)], capture_output=True, text=True,
                        timeout=900)
     assert r.returncode == 0, r.stderr[-2000:]
-    out = np.fromfile(fout, dtype=np.complex64)
+    out = np.fromfile(fout, dtype=np.float32)
     obs = np.fromfile(fobs).reshape(len(cases), steps + 1, 11)
     off = 0
     for i, c in enumerate(cases):
@@ -259,9 +260,12 @@ def test_batch_device_code_matches_oracle(staged, warps, grid):
         W = out[off:off + nx * npp].reshape(npp, nx)
         off += nx * npp
         ref_obs, ref = WignerOracle(params(c)).run(W0[i], steps)
-        assert rel_l2(W, ref) < 2e-6, (i, rel_l2(W, ref))
+        # measured: FP32 2.4e-7 .. 3.1e-7 (state), 2.6e-7 .. 2.8e-6 (energy); mixed 5e-8 .. 2.3e-7
+        # (state, FP32 storage rounding), 7e-10 .. 8e-9 (energy)
+        assert rel_l2(W, ref) < (2e-6 if prec == 0 else 5e-7), (i, rel_l2(W, ref))
         assert np.max(np.abs(obs[i, :, 0] - ref_obs[:, 0])) < (1e-6 if c['gamma'] else 2e-8 * steps), i
         assert np.max(np.abs(obs[i, :, 1:10] - ref_obs[:, 1:10])) < 1e-4, i
+        assert np.max(np.abs(obs[i, :, 9] - ref_obs[:, 9])) < (1e-5 if prec == 0 else 3e-8), i
 
 
 def test_adjoint_device_code_matches_twin(staged):
