@@ -560,20 +560,23 @@ def run_batch(args, world, rank, local):
     from pywignercuda_b200.shard import gather_observables, partition
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
-    cases_all = batch_config(count=64 * world)
+    cases_all = batch_config(count=(args.instances or 64) * world)
     parts = partition([dict(n_x=c['n'], n_p=c['n'], gamma=c['gamma']) for c in cases_all], world)
     cases = [cases_all[i] for i in parts[rank]]
     grand_total = sum(c['n'] * c['n'] for c in cases_all)
     states = [coherent_state(c['n'], c['x0'], c['p0']) for c in cases]
     K = args.steps
+    precs = ('mixed', 'f32') if args.precision == 'both' else (args.precision,)
     with ClockSampler(local) as clk:
-        legs = {p: batch_leg(cases, states, p, args, world, dev) for p in ('mixed', 'f32')}
+        legs = {p: batch_leg(cases, states, p, args, world, dev) for p in precs}
     val = validation(cases, states, dev) if rank == 0 and not args.profile_only else None
-    head_p = 'mixed'
+    head_p = precs[0]
     if val is not None:
         ok = all(v['norm_max_abs'] <= 1e-6 and v['energy_rel_max'] <= 1e-6 for v in val['mixed'].values()
                  if isinstance(v, dict))
         head_p = 'mixed' if ok else 'f32'
+        if head_p not in legs:
+            head_p = precs[0]
     head = legs[head_p]
     value = grand_total * K / (head['ms'] / 1e3)
     if args.profile_only:
@@ -882,6 +885,10 @@ def main():
     ap.add_argument('--workload', default='batch', choices=['batch', 'c128', 'dirac', 'dirac3d', 'gp'])
     ap.add_argument('--profile-only', action='store_true',
                     help='batch workload: only the timed section (for profiler launch lists)')
+    ap.add_argument('--precision', default='both', choices=['both', 'mixed', 'f32'],
+                    help='batch workload: the precisions timed (profiling runs)')
+    ap.add_argument('--instances', type=int, default=0,
+                    help='batch workload: instances per rank (default 64; profiling runs)')
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == 'reference':

@@ -326,40 +326,57 @@ int wigb_destroy(wigb_handle* h);
 int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t warps, int32_t precision, char* log,
                    int64_t log_cap);
 
-/* ---- Adjoint (differentiable) FP32 form.  No counterpart in the reference,
- * which has no gradients.  One Wigner2D grid (powers of two in [64, 1024] per
- * axis) advanced by the Lie step of GPU_Wigner2D_FFT.Run (:1884-1899)
- *   W_{n+1} = P(eps_n) K W_n,
+/* ---- Adjoint (differentiable) form.  No counterpart in the reference, which
+ * has no gradients.  One Wigner2D grid (powers of two in [64, 1024] per axis)
+ * advanced by the Lie step of GPU_Wigner2D_FFT.Run (:1884-1913)
+ *   W_{n+1} = N(C P(eps_n) K W_n),
  * K the kinetic x-pass (p^2/2m, r_lambda), P the Moyal p-pass with
- * V(x) = v4 x^4 + v2 x^2 + v0 + eps_n x, r_theta and the absorbing masks; eps_n
- * is a control per step read from device memory; no damping, no
- * normalisation.  State: (n_p, n_x) complex64, FFT-shifted, device. */
+ * V(x) = v4 x^4 + v2 x^2 + v0 + eps_n x, r_theta and the absorbing masks;
+ * eps_n is a control per step read from device memory.  With gamma != 0, C is
+ * the Caldeira-Leggett order-3 step (:1145-1157, f(p) = |p| when f_eps = 0,
+ * else p^2/sqrt(p^2 + f_eps)) and N the normalisation U -> U / (dX dP sum U)
+ * (:1912-1913); with gamma = 0 both are the identity.  State: (n_p, n_x)
+ * FFT-shifted, device, complex64 (WIGA_PREC_C64: FP32 transforms) or
+ * complex128 (WIGA_PREC_C128: FP64 transforms). */
+#define WIGA_PREC_C64 0
+#define WIGA_PREC_C128 1
 typedef struct wiga_desc {
   int32_t abi_version;   /* WIG_ABI_VERSION */
   int32_t n_x, n_p;
-  int32_t reserved;
+  int32_t precision;     /* WIGA_PREC_C64 or WIGA_PREC_C128 */
   double x_amplitude, p_amplitude, hbar, mass, dt, d_theta, d_lambda;
   double v4, v2, v0;
+  double gamma, f_eps;
 } wiga_desc;
 
 typedef struct wiga_handle wiga_handle;
 
 int wiga_create(const wiga_desc* desc, wiga_handle** out);
 
-/* n_steps forward steps from step index step0, W in place.  eps_dev: device
- * double array indexed by step (>= step0 + n_steps entries).  Y_dev (may be
- * NULL): device complex64 [n_steps][n_p][n_x], receives Y_n = K W_n of each
- * step, the input wig_step_adjoint needs.  Asynchronous on `stream`. */
-int wiga_forward(wiga_handle* h, void* W_dev, const double* eps_dev, int64_t step0, int64_t n_steps,
-                 void* Y_dev, void* stream);
+/* Replace the potential coefficients of the handle (the next forward and
+ * adjoint steps use them). */
+int wiga_set_potential(wiga_handle* h, double v4, double v2, double v0);
 
-/* One adjoint step n.  On entry lam_dev (complex64, device) holds dL/dW_{n+1},
- * on exit dL/dW_n = K^H P(eps_n)^H dL/dW_{n+1} (gradients in the convention
- * dL = Re sum conj(grad) dW, the one torch uses for complex tensors).  Y_dev:
- * Y_n from wiga_forward.  grad_dev[step] (device double) receives dL/d eps_n.
+/* n_steps forward steps from step index step0, W in place (normalised on
+ * return when damped).  eps_dev: device double array indexed by step
+ * (>= step0 + n_steps entries).  Optional (may be NULL) records of each step,
+ * the inputs wig_step_adjoint needs: Y_dev [n_steps][n_p][n_x] receives
+ * Y_n = K W_n; U_dev [n_steps][n_p][n_x] the damped step's output before
+ * normalisation; s_dev (device double2, indexed by step) its sum dX dP sum U.
  * Asynchronous on `stream`. */
-int wig_step_adjoint(wiga_handle* h, void* lam_dev, const void* Y_dev, const double* eps_dev, int64_t step,
-                     double* grad_dev, void* stream);
+int wiga_forward(wiga_handle* h, void* W_dev, const double* eps_dev, int64_t step0, int64_t n_steps,
+                 void* Y_dev, void* U_dev, void* s_dev, void* stream);
+
+/* One adjoint step n.  On entry lam_dev (device, the state's type) holds
+ * dL/dW_{n+1}, on exit dL/dW_n = K^H P(eps_n)^H C^H N_n^H dL/dW_{n+1}
+ * (gradients in the convention dL = Re sum conj(grad) dW, the one torch uses
+ * for complex tensors).  Y_dev: Y_n; damped: U_dev = U_n and s_dev (indexed by
+ * step) from wiga_forward (NULL when undamped).  grad_dev (device double,
+ * [steps][3]) receives at [3 step .. 3 step + 2] dL/d eps_n and step n's
+ * shares of dL/dv4 and dL/dv2 (dL/dv4 is their sum over the steps).
+ * Asynchronous on `stream`. */
+int wig_step_adjoint(wiga_handle* h, void* lam_dev, const void* Y_dev, const void* U_dev, const void* s_dev,
+                     const double* eps_dev, int64_t step, double* grad_dev, void* stream);
 
 int wiga_destroy(wiga_handle* h);
 

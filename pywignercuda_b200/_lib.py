@@ -89,11 +89,15 @@ class WigbInstance(ctypes.Structure):
                 ('f_eps', c_double), ('v4', c_double), ('v2', c_double), ('v1', c_double), ('v0', c_double)]
 
 
+WIGA_PREC_C64 = 0
+WIGA_PREC_C128 = 1
+
+
 class WigaDesc(ctypes.Structure):
-    _fields_ = [('abi_version', c_int32), ('n_x', c_int32), ('n_p', c_int32), ('reserved', c_int32),
+    _fields_ = [('abi_version', c_int32), ('n_x', c_int32), ('n_p', c_int32), ('precision', c_int32),
                 ('x_amplitude', c_double), ('p_amplitude', c_double), ('hbar', c_double), ('mass', c_double),
                 ('dt', c_double), ('d_theta', c_double), ('d_lambda', c_double),
-                ('v4', c_double), ('v2', c_double), ('v0', c_double)]
+                ('v4', c_double), ('v2', c_double), ('v0', c_double), ('gamma', c_double), ('f_eps', c_double)]
 
 
 class DiracDesc(ctypes.Structure):
@@ -148,8 +152,11 @@ SIGNATURES = [
     ('wigb_destroy', c_int, [c_void_p]),
     ('wigb_jit_check', c_int, [POINTER(c_int32), c_int64, c_int32, c_int32, c_char_p, c_int64]),
     ('wiga_create', c_int, [POINTER(WigaDesc), POINTER(c_void_p)]),
-    ('wiga_forward', c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p]),
-    ('wig_step_adjoint', c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    ('wiga_set_potential', c_int, [c_void_p, c_double, c_double, c_double]),
+    ('wiga_forward', c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_void_p,
+                             c_void_p]),
+    ('wig_step_adjoint', c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p,
+                                 c_void_p]),
     ('wiga_destroy', c_int, [c_void_p]),
     ('wiga_jit_check', c_int, [POINTER(WigaDesc), c_char_p, c_int64]),
     ('wig_observables_noalloc', c_int, [c_void_p, c_int32, c_int32, c_double, c_double, c_double, c_void_p,

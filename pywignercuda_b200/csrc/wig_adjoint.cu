@@ -1,7 +1,7 @@
-// Adjoint (differentiable) FP32 Wigner2D form: host side of the wiga_* /
+// Adjoint (differentiable) Wigner2D form: host side of the wiga_* /
 // wig_step_adjoint entry points (include/wigner_b200.h).  The kernels
-// (wig_adjoint.cuh, wig_jit_adjoint.cuh) are compiled by NVRTC per grid size.
-// No counterpart in the reference.
+// (wig_adjoint.cuh, wig_jit_adjoint.cuh) are compiled by NVRTC per grid size
+// and precision.  No counterpart in the reference.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -14,7 +14,8 @@
 #include "../../include/wigner_b200.h"
 #include "wig_adjoint.cuh"
 #include "wig_host.h"
-#include "wig_batch_host.h"   // register-FFT twiddle tables
+#include "wig_batch_host.h"     // register-FFT twiddle tables
+#include "wig_adjoint_host.h"
 #include "wig_adjoint_src.inc"   // kJitAdjointSource (generated by build.py)
 
 using namespace wighost;
@@ -24,9 +25,11 @@ struct wiga_handle {
   wiga_desc d{};
   wig::AArgs a{};
   DevBuf bufs;
-  CUfunction fx = nullptr, fp = nullptr, fpt = nullptr, ffin = nullptr;
-  int pw = 1, grid_x = 1, grid_p = 1, smem_x = 0, smem_p = 0, smem_pt = 0;
-  double* partials = nullptr;
+  CUfunction fx = nullptr, fp = nullptr, fpt = nullptr, ffin = nullptr, ffwd = nullptr, fsc = nullptr,
+             frs = nullptr, fdot = nullptr, fcoef = nullptr;
+  int pw = 1, grid_x = 1, grid_p = 1, smem_x = 0, smem_p = 0, grid_d = 1;
+  size_t esize = 8;                 // bytes per element of the state
+  double* part = nullptr;           // CTA partials (max of 3 per p-pass CTA, 2 per dot CTA)
 };
 
 namespace {
@@ -42,16 +45,17 @@ int check_desc(const wiga_desc* d) {
   if (!(d->x_amplitude > 0) || !(d->p_amplitude > 0) || !(d->hbar != 0) || !(d->mass != 0) ||
       !std::isfinite(d->dt))
     return fail(WIG_ERR_ARG, "wiga: amplitudes > 0, hbar and mass nonzero, dt finite");
+  if (d->precision != WIGA_PREC_C64 && d->precision != WIGA_PREC_C128)
+    return fail(WIG_ERR_ARG, "wiga: precision must be WIGA_PREC_C64 or WIGA_PREC_C128");
+  if (!std::isfinite(d->gamma) || !(d->f_eps >= 0.))
+    return fail(WIG_ERR_ARG, "wiga: gamma must be finite and f_eps >= 0");
   return WIG_OK;
 }
 
-// p-pass tile: 4 columns (32-byte row segments)
-int p_warps(int n_p) { return 4 / wig::rf_spw(n_p) > 0 ? 4 / wig::rf_spw(n_p) : 1; }
-
 std::string source(const wiga_desc* d) {
-  char head[160];
-  snprintf(head, sizeof(head), "#define WIGA_NX %d\n#define WIGA_NP %d\n#define WIGA_PW %d\n", d->n_x, d->n_p,
-           p_warps(d->n_p));
+  char head[200];
+  snprintf(head, sizeof(head), "#define WIGA_NX %d\n#define WIGA_NP %d\n#define WIGA_PW %d\n#define WIGA_PREC %d\n",
+           d->n_x, d->n_p, adjoint_p_warps(d->n_p), d->precision);
   return std::string(head) + kJitAdjointSource;
 }
 
@@ -88,54 +92,78 @@ extern "C" int wiga_create(const wiga_desc* d, wiga_handle** out) {
   h->device = device;
   h->d = *d;
   const int nx = d->n_x, np = d->n_p;
+  const bool c128 = d->precision == WIGA_PREC_C128;
+  h->esize = c128 ? 16 : 8;
   wig::AArgs& a = h->a;
-  a.n_x = nx; a.n_p = np;
-  a.dt = d->dt; a.hbar = d->hbar; a.mass = d->mass;
-  a.dx = 2. * d->x_amplitude / nx; a.dp = 2. * d->p_amplitude / np;
-  a.dtheta = 2. * M_PI / (2. * d->p_amplitude); a.dlambda = 2. * M_PI / (2. * d->x_amplitude);
-  a.v4 = d->v4; a.v2 = d->v2; a.v0 = d->v0;
-  std::vector<float2> twx, twp;
-  rf_twiddles(nx, &twx);
-  rf_twiddles(np, &twp);
-  // per-frequency / per-column factors (expPLambda_source :153, expPotential_source :117-123), FP64 then rounded
-  std::vector<float> rtab(nx), mm(nx), rth(np);
-  const double x_max = a.dx * (nx - 1.) / 2., w2 = (10. * a.dx) * (10. * a.dx);
-  for (int k = 0; k < nx; ++k) {
-    const double j = ((k + nx / 2) % nx) - 0.5 * nx;
-    const double lam = a.dlambda * j, x = a.dx * j;
-    rtab[k] = (float)(exp(-d->d_lambda * lam * lam) / (double)nx);
-    const double m1 = 1. - exp(-(x - x_max) * (x - x_max) / w2), m2 = 1. - exp(-(x + x_max) * (x + x_max) / w2);
-    mm[k] = (float)(m1 * m2 / (double)np);
+  AdjTables t;
+  adjoint_setup(*d, a, &t);
+  int rc = WIG_OK;
+  if (c128) {
+    std::vector<double2> twx, twp;
+    rf_twiddles64(nx, &twx);
+    rf_twiddles64(np, &twp);
+    double2 *x_d = nullptr, *p_d = nullptr;
+    rc = h->bufs.alloc(&x_d, twx.size(), twx.data());
+    if (!rc) rc = h->bufs.alloc(&p_d, twp.size(), twp.data());
+    a.tw_x = x_d;
+    a.tw_p = p_d;
+  } else {
+    std::vector<float2> twx, twp;
+    rf_twiddles(nx, &twx);
+    rf_twiddles(np, &twp);
+    float2 *x_d = nullptr, *p_d = nullptr;
+    rc = h->bufs.alloc(&x_d, twx.size(), twx.data());
+    if (!rc) rc = h->bufs.alloc(&p_d, twp.size(), twp.data());
+    a.tw_x = x_d;
+    a.tw_p = p_d;
   }
-  for (int k = 0; k < np; ++k) {
-    const double th = a.dtheta * (((k + np / 2) % np) - 0.5 * np);
-    rth[k] = (float)exp(-d->d_theta * th * th * d->dt);
-  }
-  float2 *twx_d, *twp_d;
-  float *rtab_d, *mm_d, *rth_d;
-  int rc = h->bufs.alloc(&twx_d, twx.size(), twx.data());
-  if (!rc) rc = h->bufs.alloc(&twp_d, twp.size(), twp.data());
-  if (!rc) rc = h->bufs.alloc(&rtab_d, rtab.size(), rtab.data());
-  if (!rc) rc = h->bufs.alloc(&mm_d, mm.size(), mm.data());
-  if (!rc) rc = h->bufs.alloc(&rth_d, rth.size(), rth.data());
-  h->pw = p_warps(np);
+  double *rtab_d = nullptr, *mm_d = nullptr, *rth_d = nullptr, *sfp_d = nullptr, *ths_d = nullptr;
+  double2* sc_d = nullptr;
+  const double2 sc_init[3] = {make_double2(1., 0.), make_double2(1., 0.), make_double2(0., 0.)};
+  if (!rc) rc = h->bufs.alloc(&rtab_d, t.rtab.size(), t.rtab.data());
+  if (!rc) rc = h->bufs.alloc(&mm_d, t.mm.size(), t.mm.data());
+  if (!rc) rc = h->bufs.alloc(&rth_d, t.rth.size(), t.rth.data());
+  if (!rc) rc = h->bufs.alloc(&sfp_d, t.sfp.size(), t.sfp.data());
+  if (!rc) rc = h->bufs.alloc(&ths_d, t.ths.size(), t.ths.data());
+  if (!rc) rc = h->bufs.alloc(&sc_d, (size_t)3, sc_init);   // pend, coef[2]
+  h->pw = adjoint_p_warps(np);
   const int spw_x = wig::rf_spw(nx), spw_p = wig::rf_spw(np), ct = h->pw * spw_p;
   h->grid_x = np / spw_x;
   h->grid_p = nx / ct;
-  h->smem_x = spw_x * (nx + (wig::rf_g(nx) == 8 ? 8 : 0)) * (int)sizeof(float2);
-  h->smem_p = ct * np * (int)sizeof(float2);
-  h->smem_pt = 2 * ct * np * (int)sizeof(float2);
-  if (!rc) rc = h->bufs.alloc(&h->partials, (size_t)h->grid_p);
+  h->grid_d = 148;
+  h->smem_x = spw_x * (nx + (wig::rf_g(nx) == 8 ? 8 : 0)) * (int)h->esize;
+  h->smem_p = 2 * ct * np * (int)h->esize;
+  if (!rc) rc = h->bufs.alloc(&h->part, (size_t)3 * std::max(h->grid_p, h->grid_d));
   if (rc) { wiga_destroy(h); return rc; }
-  a.tw_x = twx_d; a.tw_p = twp_d; a.rtab = rtab_d; a.mm = mm_d; a.rth = rth_d;
+  a.rtab = rtab_d; a.mm = mm_d; a.rth = rth_d; a.sfp = sfp_d; a.ths = ths_d;
+  a.pend = sc_d;
+  a.coef = sc_d + 1;
   CUmodule mod;
   rc = get_module(source(d), device, &mod);
   if (!rc) rc = get_fn(mod, "wiga_xpass", &h->fx, h->smem_x);
   if (!rc) rc = get_fn(mod, "wiga_ppass", &h->fp, h->smem_p);
-  if (!rc) rc = get_fn(mod, "wiga_ppass_T", &h->fpt, h->smem_pt);
+  if (!rc) rc = get_fn(mod, "wiga_ppass_T", &h->fpt, h->smem_p);
   if (!rc) rc = get_fn(mod, "wiga_grad_finalize", &h->ffin, 0);
+  if (!rc) rc = get_fn(mod, "wiga_fwd_finalize", &h->ffwd, 0);
+  if (!rc) rc = get_fn(mod, "wiga_scale", &h->fsc, 0);
+  if (!rc) rc = get_fn(mod, "wiga_reset_pend", &h->frs, 0);
+  if (!rc) rc = get_fn(mod, "wiga_dot", &h->fdot, 0);
+  if (!rc) rc = get_fn(mod, "wiga_adj_coef", &h->fcoef, 0);
   if (rc) { wiga_destroy(h); return rc; }
   *out = h;
+  return WIG_OK;
+}
+
+extern "C" int wiga_set_potential(wiga_handle* h, double v4, double v2, double v0) {
+  if (!h) return fail(WIG_ERR_ARG, "wiga_set_potential: null handle");
+  if (!std::isfinite(v4) || !std::isfinite(v2) || !std::isfinite(v0))
+    return fail(WIG_ERR_ARG, "wiga_set_potential: coefficients must be finite");
+  h->a.v4 = v4;
+  h->a.v2 = v2;
+  h->a.v0 = v0;
+  h->d.v4 = v4;
+  h->d.v2 = v2;
+  h->d.v0 = v0;
   return WIG_OK;
 }
 
@@ -153,51 +181,84 @@ static int check_device(wiga_handle* h, const char* what) {
 }
 
 extern "C" int wiga_forward(wiga_handle* h, void* W_dev, const double* eps_dev, int64_t step0, int64_t n_steps,
-                            void* Y_dev, void* stream) {
+                            void* Y_dev, void* U_dev, void* s_dev, void* stream) {
   if (!h) return fail(WIG_ERR_ARG, "wiga_forward: null handle");
   if (int rc = check_ptr(W_dev, "wiga_forward W")) return rc;
   if (int rc = check_ptr(eps_dev, "wiga_forward eps")) return rc;
   if (Y_dev)
     if (int rc = check_ptr(Y_dev, "wiga_forward Y")) return rc;
+  if (U_dev)
+    if (int rc = check_ptr(U_dev, "wiga_forward U")) return rc;
+  if (s_dev)
+    if (int rc = check_ptr(s_dev, "wiga_forward s")) return rc;
+  if ((U_dev || s_dev) && !h->a.damped) return fail(WIG_ERR_ARG, "wiga_forward: U and s are records of damped steps");
   if (step0 < 0 || n_steps < 0) return fail(WIG_ERR_ARG, "wiga_forward: step0 and n_steps must be >= 0");
   if (int rc = check_device(h, "wiga_forward")) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   const size_t plane = (size_t)h->d.n_x * h->d.n_p;
-  float2* W = (float2*)W_dev;
-  float sgn = 1.f;
+  char* W = (char*)W_dev;
+  double sgn = 1.;
   for (int64_t n = 0; n < n_steps; ++n) {
-    float2* Y = Y_dev ? (float2*)Y_dev + (size_t)n * plane : W;
-    const float2* Wc = W;
-    void* xa[] = {&h->a, (void*)&Wc, &Y, &sgn};
+    char* Y = Y_dev ? (char*)Y_dev + (size_t)n * plane * h->esize : W;
+    char* U = U_dev ? (char*)U_dev + (size_t)n * plane * h->esize : nullptr;
+    const char* Wc = W;
+    int use_pend = (h->a.damped && n > 0) ? 1 : 0;
+    void* xa[] = {&h->a, (void*)&Wc, &Y, &sgn, &use_pend};
     if (int rc = launch(h->fx, h->grid_x, 32, h->smem_x, st, xa)) return rc;
-    const float2* Yc = Y;
+    const char* Yc = Y;
     long long step = (long long)(step0 + n);
-    void* pa[] = {&h->a, (void*)&Yc, &W, (void*)&eps_dev, &step};
+    void* pa[] = {&h->a, (void*)&Yc, &W, &U, (void*)&eps_dev, &step, &h->part};
     if (int rc = launch(h->fp, h->grid_p, h->pw * 32, h->smem_p, st, pa)) return rc;
+    if (h->a.damped) {
+      int np = h->grid_p;
+      void* fa[] = {&h->a, &h->part, &np, &s_dev, &step};
+      if (int rc = launch(h->ffwd, 1, 32, 0, st, fa)) return rc;
+    }
+  }
+  if (h->a.damped && n_steps > 0) {
+    long long n = (long long)plane;
+    void* sa[] = {&h->a, &W, &n};
+    if (int rc = launch(h->fsc, 148 * 4, 256, 0, st, sa)) return rc;
+    void* ra[] = {&h->a};
+    if (int rc = launch(h->frs, 1, 32, 0, st, ra)) return rc;
   }
   return WIG_OK;
 }
 
-extern "C" int wig_step_adjoint(wiga_handle* h, void* lam_dev, const void* Y_dev, const double* eps_dev,
-                                int64_t step, double* grad_dev, void* stream) {
+extern "C" int wig_step_adjoint(wiga_handle* h, void* lam_dev, const void* Y_dev, const void* U_dev,
+                                const void* s_dev, const double* eps_dev, int64_t step, double* grad_dev,
+                                void* stream) {
   if (!h) return fail(WIG_ERR_ARG, "wig_step_adjoint: null handle");
   if (int rc = check_ptr(lam_dev, "wig_step_adjoint lam")) return rc;
   if (int rc = check_ptr(Y_dev, "wig_step_adjoint Y")) return rc;
   if (int rc = check_ptr(eps_dev, "wig_step_adjoint eps")) return rc;
+  if (h->a.damped) {
+    if (int rc = check_ptr(U_dev, "wig_step_adjoint U")) return rc;
+    if (int rc = check_ptr(s_dev, "wig_step_adjoint s")) return rc;
+  }
   if (!grad_dev || ((uintptr_t)grad_dev & 7) != 0) return fail(WIG_ERR_ARG, "wig_step_adjoint: bad grad pointer");
   if (step < 0) return fail(WIG_ERR_ARG, "wig_step_adjoint: step must be >= 0");
   if (int rc = check_device(h, "wig_step_adjoint")) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  float2* lam = (float2*)lam_dev;
-  const float2* Y = (const float2*)Y_dev;
+  char* lam = (char*)lam_dev;
   long long s = (long long)step;
-  void* pa[] = {&h->a, &lam, (void*)&Y, (void*)&eps_dev, &s, &h->partials};
-  if (int rc = launch(h->fpt, h->grid_p, h->pw * 32, h->smem_pt, st, pa)) return rc;
+  if (h->a.damped) {
+    long long n = (long long)h->d.n_x * h->d.n_p;
+    const char* lc = lam;
+    void* da[] = {(void*)&lc, (void*)&U_dev, &n, &h->part};
+    if (int rc = launch(h->fdot, h->grid_d, 256, 0, st, da)) return rc;
+    int nd = h->grid_d;
+    void* ca[] = {&h->a, &h->part, &nd, (void*)&s_dev, &s};
+    if (int rc = launch(h->fcoef, 1, 32, 0, st, ca)) return rc;
+  }
+  void* pa[] = {&h->a, &lam, (void*)&Y_dev, (void*)&eps_dev, &s, &h->part};
+  if (int rc = launch(h->fpt, h->grid_p, h->pw * 32, h->smem_p, st, pa)) return rc;
   int n = h->grid_p;
-  void* fa[] = {&h->partials, &n, &grad_dev, &s};
+  void* fa[] = {&h->part, &n, &grad_dev, &s};
   if (int rc = launch(h->ffin, 1, 32, 0, st, fa)) return rc;
-  const float2* lc = lam;
-  float sgn = -1.f;
-  void* xa[] = {&h->a, (void*)&lc, &lam, &sgn};
+  const char* lc = lam;
+  double sgn = -1.;
+  int use_pend = 0;
+  void* xa[] = {&h->a, (void*)&lc, &lam, &sgn, &use_pend};
   return launch(h->fx, h->grid_x, 32, h->smem_x, st, xa);
 }

@@ -15,11 +15,16 @@
 // Precision (WIGB_PREC, one value per compiled batch):
 //   0  FP32 transforms and pointwise factors throughout;
 //   1  the kinetic (x-pass) and Moyal (p-pass) transform pairs and their
-//      factors in FP64, the three dissipator pairs in FP32.  The dissipator's
-//      contribution is scaled by 2 gamma dt (~1e-3), so its FP32 rounding is
-//      ~1e-3 of an FP32 transform's; the kinetic and Moyal pairs carry the
-//      full state, and their FP32 rounding, spread over the grid and weighted
-//      by H(x, p) at its edges, is what drifts the energy.
+//      factors in FP64; the three dissipator pairs in FP64 on grids of at most
+//      WIGB_DISS64_MAXN points along p and in FP32 on larger ones.  The
+//      dissipator's contribution is scaled by 2 gamma dt (~1e-3), so its FP32
+//      rounding is a small fraction of an FP32 transform's -- except on coarse
+//      grids, where theta_max p_max = pi p_max^2 / dp is small and strongly
+//      damped instances (gamma ~ 0.2) would otherwise carry ~1e-6 energy
+//      error after 2000 steps; those grids are a few percent of a batch's
+//      points.  The kinetic and Moyal pairs carry the full state, and their
+//      FP32 rounding, spread over the grid and weighted by H(x, p) at its
+//      edges, is what drifts the energy in the FP32 form.
 // In both, FP64 forms the large phase arguments (dt*lambda*p/m and
 // dt*[V(x - hbar theta/2) - V(x + hbar theta/2)]/hbar, the latter from the
 // exact polynomial expansion, both in units of 2 pi) and reduces them to one
@@ -40,6 +45,9 @@
 #ifndef WIGB_PREC
 #define WIGB_PREC 0
 #endif
+#ifndef WIGB_DISS64_MAXN
+#define WIGB_DISS64_MAXN 256
+#endif
 #define WIGB_NT (WIGB_WARPS * 32)
 
 namespace wig {
@@ -52,7 +60,7 @@ struct BInst {
   int xitem0, n_xitems, pitem0, n_pitems;
   int tw_x, tw_p;    // offsets of the instance's twiddle tables (2N entries each) in the table buffer
   int ft_x, ft_p;    // offsets of its float tables: [rtab n_x][mm n_x][gtab 2 n_x] and [rth n_p][sfp n_p][ths n_p]
-  int fd_x, fd_p;    // offsets of its double tables: [rtab n_x][mm n_x][gtab 2 n_x] and [rth n_p]
+  int fd_x, fd_p;    // offsets of its double tables: [rtab n_x][mm n_x][gtab 2 n_x] and [rth n_p][sfp n_p][ths n_p]
   double dt, hbar, mass, dx, dp, dtheta, dlambda, D_theta, D_lambda, f_eps;
   double v4, v2, v1, v0;   // V(x) = v4 x^4 + v2 x^2 + v1 x + v0
   double cl_k1, cl_k12, cl_c3;   // imaginary parts of the Caldeira-Leggett Horner coefficients
@@ -242,6 +250,7 @@ __device__ __forceinline__ void batch_x_item_f32(const BArgs& A, int inst, const
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
   const int pair = warp * SPW + grp;
   const int ra = row0 + 2 * pair;
+  WIG_BOUNDS_CHECK("batched x-pass row", ra + 1, I.n_p);
   const float sc = (float)A.scale[inst];
   float* Wa = A.W + I.off + (size_t)ra * N;
   float* Wb = Wa + N;
@@ -327,6 +336,7 @@ __device__ __forceinline__ void batch_x_item_f64(const BArgs& A, int inst, const
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
   const int pair = warp * SPW + grp;
   const int ra = row0 + 2 * pair;
+  WIG_BOUNDS_CHECK("batched x-pass row", ra + 1, I.n_p);
   const double sc = A.scale[inst];
   float* Wa = A.W + I.off + (size_t)ra * N;
   float* Wb = Wa + N;
@@ -407,6 +417,8 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
 #pragma unroll
     for (int r = 0; r < LB; ++r) {
       const int e = threadIdx.x + (r0 + r) * NT;
+      WIG_BOUNDS_CHECK("batched p-pass tile column", col0 + (e & (CT2 - 1)), nx);
+      WIG_BOUNDS_CHECK("batched p-pass tile row", e / CT2, N);
       buf[r] = Wi[(size_t)(e / CT2) * nx + col0 + (e & (CT2 - 1))];
     }
 #pragma unroll
@@ -463,11 +475,37 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
 #pragma unroll
     for (int e = 0; e < E; ++e) z[e] = px.get(g * Q + e / G + E * (e % G));
     F64::invx(z, px, ti64, g);
+    if constexpr (N <= WIGB_DISS64_MAXN) {
+      // the dissipator in FP64 as well (coarse grids): A kept in registers, D through PairX
+      if (damped) {
+        const double* sfp64 = rth64 + N;   // sign(p) f(p)
+        const double* ths64 = sfp64 + N;   // theta / N
+        double2 A[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) A[m] = z[m];
+#pragma unroll 1
+        for (int it = 0; it < 3; ++it) {
+#pragma unroll
+          for (int m = 0; m < E; ++m) z[m] = cscale(z[m], __ldg(sfp64 + g + G * m));
+          F64::fwdx(z, px, tf64, g);
+#pragma unroll
+          for (int i = 0; i < Q; ++i)
+#pragma unroll
+            for (int b = 0; b < G; ++b) z[i * G + b] = cscale(z[i * G + b], __ldg(ths64 + g * Q + i + E * b));
+          F64::invx(z, px, ti64, g);
+          const double cf = it == 0 ? I.cl_k1 : (it == 1 ? I.cl_k12 : I.cl_c3);
+#pragma unroll
+          for (int m = 0; m < E; ++m) z[m] = make_double2(A[m].x - cf * z[m].y, A[m].y + cf * z[m].x);
+        }
+      }
+    }
 #pragma unroll
     for (int m = 0; m < E; ++m) w[m] = make_float2((float)z[m].x, (float)z[m].y);
   }
+  const int n_it_run = N <= WIGB_DISS64_MAXN ? 1 : n_it;
 #else
   constexpr int it0 = 0;
+  const int n_it_run = n_it;
 #pragma unroll
   for (int m = 0; m < E; ++m) {
     const float2 a = tile[sl1(g + G * m)], b = tile[sl2(g + G * m)];
@@ -477,7 +515,7 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
   // One transform pair per pass through this loop (kept rolled so the kernel
   // holds a single copy of each FFT); the exchange runs in c2's slots.
 #pragma unroll 1
-  for (int it = it0; it < n_it; ++it) {
+  for (int it = it0; it < n_it_run; ++it) {
     __syncwarp();   // the previous transform's exchange reads are done before slots change
     if (it == 1) {
 #pragma unroll
@@ -588,6 +626,7 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
 #pragma unroll 8
   for (int r = 0; r < PER; ++r) {
     const int e = threadIdx.x + r * NT, k = e / CT2, cc = e & (CT2 - 1);
+    WIG_BOUNDS_CHECK("batched p-pass store column", col0 + cc, nx);
     Wi[(size_t)k * nx + col0 + cc] = tile[k * CT2 + (cc ^ tile_sw<CT2>(k))].x;
   }
   batch_item_done<NT>(A, inst, I, item, acc, I.damp ? 1 : 0, sample);
@@ -605,6 +644,7 @@ __device__ __forceinline__ void batch_reduce_item(const BArgs& A, int inst, cons
   for (int e = threadIdx.x; e < CPB * N; e += NT) {
     const int k = e / CPB, c = e - k * CPB;
     const int col = col0 + c;
+    WIG_BOUNDS_CHECK("batched reduce column", col, nx);
     accumulate_obs_k(acc, Wi[(size_t)k * nx + col], I.dx * shifted(col, nx), I.dp * shifted(k, N), I);
   }
   double v[NACC];

@@ -62,7 +62,7 @@ inline void rf_twiddles64(int n, std::vector<double2>* tw) { rf_twiddles_t(n, tw
 //   ft at ft_x: [r_lambda / n_x][mask1 mask2 / n_p][(cos, -sin) of the row-pair kinetic ratio]
 //   ft at ft_p: [r_theta][sign(p) f(p)][theta / n_p]
 //   fd at fd_x: [r_lambda / n_x][mask1 mask2 / n_p][(cos, -sin) of the row-pair kinetic ratio]
-//   fd at fd_p: [r_theta]
+//   fd at fd_p: [r_theta][sign(p) f(p)][theta / n_p]
 // (expPLambda_source :153, expPotential_source :117-123, theta_fp_source
 // :422-428 of GPU_Wigner2D_FFT.py; every entry formed in FP64.)
 // D: any struct with the fields of wigb_instance.
@@ -133,6 +133,8 @@ void batch_instance_setup(const D& d, wig::BInst& b, std::vector<float>* ft, std
   for (int k = 0; k < nx; ++k) { fd->push_back(gc[k]); fd->push_back(gs[k]); }
   b.fd_p = (int)fd->size();
   for (double v : rt) fd->push_back(v);
+  for (double v : sf) fd->push_back(v);
+  for (double v : th) fd->push_back(v);
 }
 
 // Twiddle tables of every size class (float and double, same offsets).

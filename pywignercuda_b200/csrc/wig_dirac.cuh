@@ -220,6 +220,7 @@ __device__ __forceinline__ void dirac_col_body(const DiracArgs& a, double2* __re
   for (int e = threadIdx.x; e < 4 * C * NY; e += NT) {
     const int k = e / (4 * C), q = e - k * (4 * C);
     const int m = q / C, c = q - m * C;
+    WIG_BOUNDS_CHECK("Dirac column-pass tile column", col0 + c, NX);
     sm[pad8(e)] = psi[m * comp + (size_t)k * NX + col0 + c];
   }
   __syncthreads();

@@ -19,6 +19,21 @@
 // pointwise factor, which is exact because N is a power of two).
 #pragma once
 
+// WIG_BOUNDS_CHECK(what, i, n): 0 <= i < n.  Compiled in only when WIG_BOUNDS is
+// defined, which only the host execution of this device code does (its shim
+// provides wig_bounds_fail, which reports and aborts); the kernels the library
+// compiles for the GPU carry no such checks and never trap.
+#ifdef WIG_BOUNDS
+#define WIG_BOUNDS_CHECK(what, i, n)                                                   \
+  do {                                                                                 \
+    if ((long long)(i) < 0 || (long long)(i) >= (long long)(n)) wig_bounds_fail(what, (long long)(i), (long long)(n)); \
+  } while (0)
+#else
+#define WIG_BOUNDS_CHECK(what, i, n) \
+  do {                               \
+  } while (0)
+#endif
+
 namespace wig {
 
 template <class T> struct V2;

@@ -246,6 +246,7 @@ __device__ __forceinline__ void xpass_body(const WigArgs& a, const Phys& ph, dou
     s = consume_partials<NT>(a, scale_mode, blockIdx.x == 0 ? obs_row : nullptr, red);
 
   const int row0 = blockIdx.x * ROWS;
+  WIG_BOUNDS_CHECK("x-pass rows", row0 + ROWS - 1, NP);
   double2* Wb = W + (size_t)row0 * NX;
   for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
     const int r = e / NX, k = e - r * NX;
@@ -330,6 +331,7 @@ __device__ __forceinline__ void ppass_body(const WigArgs& a, const Phys& ph, dou
   }
   for (int e = threadIdx.x; e < C * NP; e += NT) {
     const int k = e / C, c = e - k * C;
+    WIG_BOUNDS_CHECK("p-pass tile column", col0 + c, NX);
     double2 v = W[(size_t)k * NX + col0 + c];
     if (scale_mode != 0) v = cmul(v, s);
     A[pad8(e)] = v;
@@ -482,6 +484,7 @@ __device__ __forceinline__ void bloch_ppass_body(const WigArgs& a, const Phys& p
   const int col0 = blockIdx.x * C;
   for (int e = threadIdx.x; e < C * NP; e += NT) {
     const int k = e / C, c = e - k * C;
+    WIG_BOUNDS_CHECK("ODM p-pass tile column", col0 + c, NX);
     A[pad8(e)] = W[(size_t)k * NX + col0 + c];
   }
   __syncthreads();
@@ -512,6 +515,7 @@ __device__ __forceinline__ void bloch_xpass_body(const WigArgs& a, const Phys& p
   typedef RowMap<NX> M;
   extern __shared__ double2 sm[];
   const int row0 = blockIdx.x * ROWS;
+  WIG_BOUNDS_CHECK("x-pass rows", row0 + ROWS - 1, NP);
   double2* Wb = W + (size_t)row0 * NX;
   for (int e = threadIdx.x; e < ROWS * NX; e += NT) {
     const int r = e / NX, k = e - r * NX;

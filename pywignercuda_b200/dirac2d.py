@@ -31,6 +31,23 @@ class GPU_Dirac2D:
     constants_mode = _lib.CONST_CUDA_F
 
     def __init__(self, gridDIM, amplitude, dt, timeSteps, skipFrames=1, frameSaveMode='Density'):
+        self._set_grids(gridDIM, amplitude)
+        self.timeSteps = timeSteps
+        self.skipFrames = skipFrames
+        self.frameSaveMode = frameSaveMode
+        self.dt = dt
+        if not hasattr(self, 'hBar'):
+            self.hBar = 1.
+        for name in ('mass', 'c'):
+            if not hasattr(self, name):
+                raise _lib.WignerArgumentError('set self.%s before GPU_Dirac2D.__init__' % name)
+        for k in range(4):
+            if not hasattr(self, 'Potential_%d_String' % k):
+                setattr(self, 'Potential_%d_String' % k, '0.')
+        self._build()
+
+    def _set_grids(self, gridDIM, amplitude):
+        """Shifted x, y and momentum grids (GPU_Dirac2D.py:306-352); host only."""
         X_amplitude, Y_amplitude = amplitude
         X_gridDIM, Y_gridDIM = gridDIM
         self.dX = 2. * X_amplitude / float(X_gridDIM)
@@ -38,9 +55,6 @@ class GPU_Dirac2D:
         self.X_amplitude, self.Y_amplitude = X_amplitude, Y_amplitude
         self.X_gridDIM, self.Y_gridDIM = X_gridDIM, Y_gridDIM
         self.min_X, self.min_Y = -X_amplitude, -Y_amplitude
-        self.timeSteps = timeSteps
-        self.skipFrames = skipFrames
-        self.frameSaveMode = frameSaveMode
         rangeX = np.linspace(-X_amplitude, X_amplitude - self.dX, X_gridDIM)
         rangeY = np.linspace(-Y_amplitude, Y_amplitude - self.dY, Y_gridDIM)
         self.X = np.fft.fftshift(rangeX)[np.newaxis, :]
@@ -53,16 +67,6 @@ class GPU_Dirac2D:
         Py_range = np.linspace(-Py_amplitude, Py_amplitude - self.dPy, self.Y_gridDIM)
         self.Px = np.fft.fftshift(Px_range)[np.newaxis, :]
         self.Py = np.fft.fftshift(Py_range)[:, np.newaxis]
-        self.dt = dt
-        if not hasattr(self, 'hBar'):
-            self.hBar = 1.
-        for name in ('mass', 'c'):
-            if not hasattr(self, name):
-                raise _lib.WignerArgumentError('set self.%s before GPU_Dirac2D.__init__' % name)
-        for k in range(4):
-            if not hasattr(self, 'Potential_%d_String' % k):
-                setattr(self, 'Potential_%d_String' % k, '0.')
-        self._build()
 
     def _build(self):
         lib = _lib.load()

@@ -129,12 +129,18 @@ int main(int argc, char** argv) {
   A.obs = obs.data(); A.obs_stride = (int)(n_prop + 1);
   const int nxi = (int)xi.size(), npi = (int)pi.size();
 
+  // dynamic shared memory of the passes (wigb_compile: the largest size class)
+  size_t smx = 0, smp = 0;
+  for (int n : cls) {
+    smx = std::max(smx, (size_t)wig::bx_smem(n, WIGB_WARPS) * sizeof(float2));
+    smp = std::max(smp, (size_t)wig::bp_smem(n, WIGB_WARPS) * sizeof(float2));
+  }
   // wigb_launch_run: reduce (normalisation, sample 0), then per step x-pass and p-pass, then scale
   emu_launch(grid, WIGB_NT, [&] { wigb_reduce(A, npi, 1, 0); });
   for (long n = 0; n < n_prop; ++n) {
-    emu_launch(grid, WIGB_NT, [&] { wigb_xpass(A, nxi); });
+    emu_launch(grid, WIGB_NT, [&] { wigb_xpass(A, nxi); }, smx);
     const int sample = (int)(n + 1);
-    emu_launch(grid, WIGB_NT, [&] { wigb_ppass(A, npi, sample); });
+    emu_launch(grid, WIGB_NT, [&] { wigb_ppass(A, npi, sample); }, smp);
   }
   emu_launch(grid, WIGB_NT, [&] { wigb_scale(A, npi); });
   if (tickets[0] != 0u || tickets[1] != 0u) {

@@ -86,6 +86,9 @@ int main(int argc, char** argv) {
   const double Pxa = M_PI / dX, Pya = M_PI / dY;
   const double dPx = 2. * Pxa / NX, dPy = 2. * Pya / NY;
   const int n_row = NY / DIR_ROWS, n_col = NX / DIR_C;
+  // dirac_plan's dynamic shared memory
+  const size_t sm_row = (size_t)wig::padded_size(4 * DIR_ROWS * NX) * sizeof(double2);
+  const size_t sm_col = (size_t)wig::padded_size(4 * DIR_C * NY) * sizeof(double2);
 
   std::vector<double> xt = shifted_range(xa, NX), yt = shifted_range(ya, NY);
   std::vector<double> pxt = shifted_range(Pxa, NX), pyt = shifted_range(Pya, NY);
@@ -109,15 +112,15 @@ int main(int argc, char** argv) {
   // dirac_run_begin: first row pass (x sums, row FFT)
   {
     const double t_obs = dt * 1.;
-    emu_launch(n_row, DIR_RNT, [&] { dirac_rowpass(a, P, 0, 0, 0., t_obs, nullptr); });
+    emu_launch(n_row, DIR_RNT, [&] { dirac_rowpass(a, P, 0, 0, 0., t_obs, nullptr); }, sm_row);
   }
   // dirac_run_step
   for (long n = 0; n < n_steps; ++n) {
-    emu_launch(n_col, DIR_CNT, [&] { dirac_colpass(a, P); });
+    emu_launch(n_col, DIR_CNT, [&] { dirac_colpass(a, P); }, sm_col);
     const int mode = (n == n_steps - 1) ? 2 : 1, parity = (int)((n + 1) & 1);
     const double t_step = dt * (double)(n + 1), t_obs = dt * (double)(n + 2);
     double* orow = obs.data() + (size_t)n * wig::DNOBS;
-    emu_launch(n_row, DIR_RNT, [&] { dirac_rowpass(a, P, mode, parity, t_step, t_obs, orow); });
+    emu_launch(n_row, DIR_RNT, [&] { dirac_rowpass(a, P, mode, parity, t_step, t_obs, orow); }, sm_row);
   }
   // dirac_run_end: the final Normalize_X factor and its application
   {

@@ -80,6 +80,10 @@ int main(int argc, char** argv) {
   const int gy = clampi(4 * NZ * (NX / D3_YC), 1, max_cta);
   const int gz = clampi(NY * (NX / D3_ZC), 1, max_cta);
   const int gn = clampi((int)(npts / (4L * D3_SNT)), 1, max_cta);
+  // dirac3_plan's dynamic shared memory
+  const size_t sm_x = (size_t)wig::padded_size(4 * D3_ROWS * NX) * sizeof(double2);
+  const size_t sm_y = (size_t)wig::padded_size(NY * D3_YC) * sizeof(double2);
+  const size_t sm_z = (size_t)wig::padded_size(4 * D3_ZC * NZ) * sizeof(double2);
 
   wig::Dirac3Args a{};
   a.hbar = 1.; a.mass = mass; a.c = c; a.dt = dt;
@@ -102,15 +106,15 @@ int main(int argc, char** argv) {
     emu_launch(gn, D3_SNT, [&] { d3_norm(a, P, n); });
     emu_launch(1, D3_SNT, [&] { d3_norm_fin(a, gn); });
   }
-  emu_launch(gx, D3_XNT, [&] { d3_xpass(a, P, 0, 0, 1, 0., dt, 0, nullptr); });
+  emu_launch(gx, D3_XNT, [&] { d3_xpass(a, P, 0, 0, 1, 0., dt, 0, nullptr); }, sm_x);
   for (long k = 1; k <= n_steps; ++k) {
-    emu_launch(gy, D3_YNT, [&] { d3_ypass_fwd(a, P); });
-    emu_launch(gz, D3_ZNT, [&] { d3_zpass(a, P); });
-    emu_launch(gy, D3_YNT, [&] { d3_ypass_inv(a, P); });
+    emu_launch(gy, D3_YNT, [&] { d3_ypass_fwd(a, P); }, sm_y);
+    emu_launch(gz, D3_ZNT, [&] { d3_zpass(a, P); }, sm_z);
+    emu_launch(gy, D3_YNT, [&] { d3_ypass_inv(a, P); }, sm_y);
     const int mode = (k == n_steps) ? 2 : 1, parity = (int)(k & 1);
     const double tA = dt * (double)k, tobs = dt * (double)(k + 1);
     double* oprev = obs.data() + (size_t)(k - 1) * wig::D3NOBS;
-    emu_launch(gx, D3_XNT, [&] { d3_xpass(a, P, mode, parity, 0, tA, tobs, (long long)k, oprev); });
+    emu_launch(gx, D3_XNT, [&] { d3_xpass(a, P, mode, parity, 0, tA, tobs, (long long)k, oprev); }, sm_x);
   }
   if (!write_all(argv[2], psi.data(), npts * sizeof(double2))) return 4;
   if (!write_all(argv[3], obs.data(), obs.size() * sizeof(double))) return 4;

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <functional>
 #include <memory>
+#include <new>
 #include <thread>
 #include <vector>
 
@@ -43,7 +44,10 @@ inline emu_dim3 blockDim, gridDim;
 #define __launch_bounds__(...)
 #define __shared__ static
 
-alignas(256) inline unsigned char emu_smem[1 << 22];
+inline unsigned char* emu_smem = nullptr;   // the running launch's dynamic shared memory
+struct emu_aligned_delete {
+  void operator()(unsigned char* p) const { ::operator delete[](p, std::align_val_t(256)); }
+};
 
 inline std::barrier<>* emu_block_barrier = nullptr;
 inline std::vector<std::unique_ptr<std::barrier<>>> emu_warp_barriers;
@@ -83,16 +87,22 @@ inline void sincospi(double x, double* s, double* c) {
   *c = (double)::cosl(a);
 }
 
-// (grid_x, grid_y) x block threads; a block's threads run concurrently, blocks in turn
-inline void emu_launch2d(unsigned grid_x, unsigned grid_y, unsigned block, const std::function<void()>& body) {
+// (grid_x, grid_y) x block threads; a block's threads run concurrently, blocks in turn.
+// smem: bytes of dynamic shared memory (0: a 4 MiB buffer, for kernels with none).
+inline void emu_launch2d(unsigned grid_x, unsigned grid_y, unsigned block, const std::function<void()>& body,
+                         size_t smem = 0) {
   if (block == 0 || block > 1024 || (block % 32) != 0) {
     std::fprintf(stderr, "emu_launch: block of %u threads\n", block);
     std::exit(3);
   }
+  const size_t bytes = smem ? smem : ((size_t)1 << 22);
+  std::unique_ptr<unsigned char[], emu_aligned_delete> buf(new (std::align_val_t(256)) unsigned char[bytes]);
   gridDim = {grid_x, grid_y, 1};
   blockDim = {block, 1, 1};
   for (unsigned by = 0; by < grid_y; ++by)
     for (unsigned bx = 0; bx < grid_x; ++bx) {
+      std::memset(buf.get(), 0xff, bytes);
+      emu_smem = buf.get();
       std::barrier<> bar((std::ptrdiff_t)block);
       emu_block_barrier = &bar;
       emu_warp_barriers.clear();
@@ -109,6 +119,12 @@ inline void emu_launch2d(unsigned grid_x, unsigned grid_y, unsigned block, const
     }
 }
 
-inline void emu_launch(unsigned grid, unsigned block, const std::function<void()>& body) {
-  emu_launch2d(grid, 1, block, body);
+inline void emu_launch(unsigned grid, unsigned block, const std::function<void()>& body, size_t smem = 0) {
+  emu_launch2d(grid, 1, block, body, smem);
+}
+
+// WIG_BOUNDS: an index check of the device code failed
+inline void wig_bounds_fail(const char* what, long long i, long long n) {
+  std::fprintf(stderr, "WIG_BOUNDS: %s index %lld outside [0, %lld)\n", what, i, n);
+  std::abort();
 }

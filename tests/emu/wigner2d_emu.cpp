@@ -105,6 +105,12 @@ int main(int argc, char** argv) {
   dtheta = 2. * M_PI / (2. * pa);
   dlambda = 2. * M_PI / (2. * xa);
   const int n_cta_x = NP / WIG_XROWS, n_cta_p = NX / WIG_PC;
+  // wig_plan's dynamic shared memory
+  const size_t tile_x = (size_t)wig::padded_size(WIG_XROWS * NX) * sizeof(double2);
+  const size_t tile_p = (size_t)wig::padded_size(WIG_PC * NP) * sizeof(double2);
+  const size_t sm_x = tile_x, sm_p = WIG_DAMP == 1 ? 2 * tile_p + 2 * NP * sizeof(double) : tile_p;
+  const size_t sm_ox = 2 * tile_x, sm_op = 2 * tile_p, sm_ph = tile_p;
+  const size_t sm_gph = ((size_t)wig::padded_size(NX) + wig::padded_size(WIG_XROWS * NX)) * sizeof(double2);
   const int n_cta_r = clampi(NX * NP / (4 * WIG_RNT), 1, 296);
 
   wig::WigArgs a{};
@@ -180,17 +186,17 @@ int main(int argc, char** argv) {
     auto exponent = [&]() -> const double* {
       if (!gp) return nullptr;
       marginal(nullptr);
-      emu_launch(n_cta_x, WIG_XNT, [&] { wig_gp_bloch(a, Px.data(), dtb, gexp.data()); });
+      emu_launch(n_cta_x, WIG_XNT, [&] { wig_gp_bloch(a, Px.data(), dtb, gexp.data()); }, sm_gph);
       return gexp.data();
     };
     std::vector<double> stats((size_t)bloch_steps * 10, 0.);
     for (long k = 0; k < bloch_steps; ++k) {
       const double t = (double)k * dt;
       const double* ge = exponent();
-      emu_launch(n_cta_p, WIG_PNT, [&] { wig_bloch_ppass(a, Wp, t, dtb, ge); });
-      emu_launch(n_cta_x, WIG_XNT, [&] { wig_bloch_xpass(a, Wp, dtb); });
+      emu_launch(n_cta_p, WIG_PNT, [&] { wig_bloch_ppass(a, Wp, t, dtb, ge); }, sm_ph);
+      emu_launch(n_cta_x, WIG_XNT, [&] { wig_bloch_xpass(a, Wp, dtb); }, sm_x);
       ge = exponent();
-      emu_launch(n_cta_p, WIG_PNT, [&] { wig_bloch_ppass(a, Wp, t, dtb, ge); });
+      emu_launch(n_cta_p, WIG_PNT, [&] { wig_bloch_ppass(a, Wp, t, dtb, ge); }, sm_ph);
       double sm[wig::NBL];
       if (W0p) {
         sums(W0p, sm);
@@ -236,7 +242,7 @@ int main(int argc, char** argv) {
   auto gp_terms = [&](int scale_mode, double* psq_out) {
     emu_launch2d(NX / gcnt, NP / 16, gcnt, [&] { wig_gp_colsum(Wp, chunks.data()); });
     emu_launch(1, 256, [&] { wig_gp_marginal(a, chunks.data(), n_chunks, scale_mode, Px.data(), psq_out); });
-    emu_launch(n_cta_x, WIG_XNT, [&] { wig_gp_phase(a, Px.data(), phase.data()); });
+    emu_launch(n_cta_x, WIG_XNT, [&] { wig_gp_phase(a, Px.data(), phase.data()); }, sm_gph);
   };
   const double* gph = gp ? phase.data() : nullptr;
 #endif
@@ -246,18 +252,18 @@ int main(int argc, char** argv) {
     const double t = (double)n * dt;
 #if WIG_STRANG
     if (gp) gp_terms(mode, nullptr);
-    emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass_half(a, Wp, t, mode, orow, gph); });
-    emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, 0, nullptr); });
+    emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass_half(a, Wp, t, mode, orow, gph); }, sm_ph);
+    emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, 0, nullptr); }, sm_x);
     if (gp) gp_terms(0, psq.data() + n);
-    emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass_half_final(a, Wp, t, gph); });
+    emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass_half_final(a, Wp, t, gph); }, sm_p);
 #else
-    emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, mode, orow); });
-    emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass(a, Wp, t); });
+    emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, mode, orow); }, sm_x);
+    emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass(a, Wp, t); }, sm_p);
 #endif
     for (int j = 0; j < odm; ++j) {
       const double coef = dt * 2 * gamma * odm_w[j] / 1. * (1.0 / (double)NP), sign = odm_sign[j];
-      emu_launch(n_cta_x, WIG_XNT, [&] { wig_odm_xpass(a, Wp, T.data()); });
-      emu_launch(n_cta_p, WIG_PNT, [&] { wig_odm_ppass(a, Wp, T.data(), coef, sign); });
+      emu_launch(n_cta_x, WIG_XNT, [&] { wig_odm_xpass(a, Wp, T.data()); }, sm_ox);
+      emu_launch(n_cta_p, WIG_PNT, [&] { wig_odm_ppass(a, Wp, T.data(), coef, sign); }, sm_op);
     }
     a.n_partials = n_cta_p;
   }

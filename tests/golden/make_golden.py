@@ -302,7 +302,64 @@ def run_dirac3d_case(name, c):
                 init_sum=np.array([np.sum(np.abs(p) ** 2) for p in psi0]))
 
 
+# initial-state helpers: Propagator_Base.Wigner_HarmonicOscillator /
+# Wigner_Half_HarmonicOscillator (GPU_Wigner2D_FFT.py:715-771) and the
+# GPU_Dirac2D spinors (GPU_Dirac2D.py:419-497, 503-535, 646-701)
+INIT_WIGNER = dict(n_x=64, n_p=32, x_amplitude=8., p_amplitude=6., mass=1.3, hbar=0.7)
+INIT_HO = ((0, 1., 1.5, -0.5), (1, 0.8, -1., 0.3), (2, 1.2, 0.5, 1.0))
+INIT_HALF = ((0, 1., 0.5, 0.2), (1, 1.1, -0.5, 0.4))
+INIT_DIRAC = dict(n_x=32, n_y=16, x_amplitude=10., y_amplitude=8., mass=1., c=3.0, hbar=1.)
+INIT_P = (1.5, -0.5)
+INIT_LANDAU = ((5.0, 0, 1.0, -0.5, 1), (5.0, 1, 0.5, 0.5, 1), (4.0, 2, -0.5, 0.0, 2))
+
+
+def modulation(x, y):
+    return np.exp(-((x - 0.5) ** 2 + 1.3 * (y + 0.2) ** 2) / 2.)
+
+
+def run_initial_states():
+    m = h.load_reference_module('GPU_Wigner2D_FFT')
+    d = h.load_reference_module('GPU_Dirac2D')
+    w = INIT_WIGNER
+    out = {'params': json.dumps(dict(wigner=w, ho=INIT_HO, half=INIT_HALF, dirac=INIT_DIRAC, p=INIT_P,
+                                     landau=INIT_LANDAU))}
+    with h.quiet():
+        pb = m.Propagator_Base.__new__(m.Propagator_Base)
+        pb.mass, pb.hBar = w['mass'], w['hbar']
+        pb.SetPhaseSpaceBox2D(w['n_x'], w['n_p'], w['x_amplitude'], w['p_amplitude'])
+        for i, a in enumerate(INIT_HO):
+            out['ho_%d' % i] = np.asarray(pb.Wigner_HarmonicOscillator(*a))
+        for i, a in enumerate(INIT_HALF):
+            out['half_%d' % i] = np.asarray(pb.Wigner_Half_HarmonicOscillator(*a))
+        c = INIT_DIRAC
+
+        class Instance(d.GPU_Dirac2D):
+            def __init__(self):
+                self.mass, self.c, self.hBar = c['mass'], c['c'], c['hbar']
+                self.Potential_0_String = self.Potential_1_String = '0.'
+                self.Potential_2_String = self.Potential_3_String = '0.'
+                self.fileName = '/tmp/_golden_init.hdf5'
+                d.GPU_Dirac2D.__init__(self, (c['n_x'], c['n_y']), (c['x_amplitude'], c['y_amplitude']), 1e-3, 1,
+                                       10 ** 9, frameSaveMode='Density')
+        inst = Instance()
+        for name in ('Spinor_Particle_SpinUp', 'Spinor_Particle_SpinDown', 'Spinor_AntiParticle_SpinDown',
+                     'Spinor_AntiParticle_SpinUp'):
+            out[name] = np.asarray(getattr(inst, name)(INIT_P, modulation))
+        for i, a in enumerate(INIT_LANDAU):
+            out['landau_%d' % i] = np.asarray(inst.LandauLevelSpinor(*a))
+        for sign in (1, -1):
+            out['filter_%+d' % sign] = np.asarray(inst.FilterElectrons(sign, out['Spinor_Particle_SpinUp']))
+    return out
+
+
 def main(names):
+    if 'initial_states' in names:
+        path = os.path.join(HERE, 'initial_states.npz')
+        np.savez_compressed(path, **run_initial_states())
+        print('%-22s %7.1f KB' % ('initial_states', os.path.getsize(path) / 1e3))
+        names = [n for n in names if n != 'initial_states']
+        if not names:
+            return
     cases = dict(WIGNER_CASES)
     cases.update(GP_CASES)
     cases.update(BLOCH_CASES)

@@ -1,0 +1,72 @@
+"""The drop-in classes' initial-state helpers against the reference's own
+(tests/golden/initial_states.npz, made by tests/golden/make_golden.py from the
+reference's Propagator_Base and GPU_Dirac2D methods under the CPU harness):
+
+* Propagator_Base.Wigner_HarmonicOscillator, Wigner_Half_HarmonicOscillator
+  (GPU_Wigner2D_FFT.py:715-771);
+* GPU_Dirac2D.Spinor_Particle_SpinUp / SpinDown, Spinor_AntiParticle_SpinDown /
+  SpinUp (GPU_Dirac2D.py:419-497), LandauLevelSpinor (:503-535) and
+  FilterElectrons (:646-701).
+
+All host code: no GPU.  The helpers evaluate the same formulas; the bar is
+1e-12 relative (the reference uses scipy.fftpack and poly1d Laguerre /
+Legendre polynomials, this package numpy.fft and scipy's eval_* functions)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle.common import rel_l2
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope='module')
+def gold():
+    return np.load(os.path.join(HERE, 'golden', 'initial_states.npz'))
+
+
+def _wigner_base(p):
+    from pywignercuda_b200.wigner2d import Propagator_Base
+    pb = Propagator_Base()
+    pb.mass, pb.hBar = p['mass'], p['hbar']
+    pb.SetPhaseSpaceBox2D(p['n_x'], p['n_p'], p['x_amplitude'], p['p_amplitude'])
+    return pb
+
+
+def _dirac(p):
+    from pywignercuda_b200.dirac2d import GPU_Dirac2D
+    d = GPU_Dirac2D.__new__(GPU_Dirac2D)
+    d.mass, d.c, d.hBar = p['mass'], p['c'], p['hbar']
+    d._set_grids((p['n_x'], p['n_y']), (p['x_amplitude'], p['y_amplitude']))
+    return d
+
+
+def modulation(x, y):
+    return np.exp(-((x - 0.5) ** 2 + 1.3 * (y + 0.2) ** 2) / 2.)
+
+
+def test_wigner_harmonic_oscillator_and_half_oscillator(gold):
+    prm = json.loads(str(gold['params']))
+    pb = _wigner_base(prm['wigner'])
+    for i, a in enumerate(prm['ho']):
+        ref = gold['ho_%d' % i]
+        assert rel_l2(pb.Wigner_HarmonicOscillator(*a), ref) < 1e-12, i
+    for i, a in enumerate(prm['half']):
+        ref = gold['half_%d' % i]
+        assert rel_l2(pb.Wigner_Half_HarmonicOscillator(*a), ref) < 1e-12, i
+
+
+def test_dirac_spinors_landau_levels_and_filter(gold):
+    prm = json.loads(str(gold['params']))
+    d = _dirac(prm['dirac'])
+    p = tuple(prm['p'])
+    for name in ('Spinor_Particle_SpinUp', 'Spinor_Particle_SpinDown', 'Spinor_AntiParticle_SpinDown',
+                 'Spinor_AntiParticle_SpinUp'):
+        assert rel_l2(getattr(d, name)(p, modulation), gold[name]) < 1e-12, name
+    for i, a in enumerate(prm['landau']):
+        assert rel_l2(d.LandauLevelSpinor(*a), gold['landau_%d' % i]) < 1e-12, i
+    up = d.Spinor_Particle_SpinUp(p, modulation)
+    for sign in (1, -1):
+        assert rel_l2(d.FilterElectrons(sign, up), gold['filter_%+d' % sign]) < 1e-12, sign
