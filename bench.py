@@ -659,6 +659,38 @@ def run_batch(args, world, rank, local):
         print(json.dumps(line))
 
 
+def run_shardcost(args, world, rank, local):
+    """Per-size-class cost of the batched form for the multi-GPU partition
+    (pywignercuda_b200/shard.py): for each grid size and damping, a batch of one
+    class holding about 32 M points, K steps with the L2 flushed before each,
+    device time per grid point per step.  Rank 0 prints one JSON line."""
+    import torch
+    from pywignercuda_b200.batch import WignerBatch, instance
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    prec = 'mixed' if args.precision == 'both' else args.precision
+    out = {}
+    for n in (128, 256, 512, 1024):
+        for damped in (False, True):
+            count = max(1, (1 << 25) // (n * n))
+            g = 0.1 if damped else 0.
+            b = WignerBatch([instance(n, x_amplitude=10., dt=DT, gamma=g, d_theta=g, v4=0.05, v2=-0.5)] * count,
+                            precision=prec)
+            states = [coherent_state(n, 0.5, -0.2)] * count
+            scratch = b.pack(states)
+            b.autotune(scratch, probe_steps=2)
+            W = b.pack(states)
+            b.run(W, args.warmup)
+            b.run(W, args.steps, continue_run=True, graph=False, observables=False, profile=True, flush_l2=True)
+            torch.cuda.synchronize()
+            x_ms, p_ms, nl = b.profile()
+            out['%d%s' % (n, 'd' if damped else '')] = (x_ms + p_ms) / nl * 1e6 / (count * n * n)
+            del b, W, scratch
+    if rank == 0:
+        print(json.dumps({'workload': 'shardcost', 'precision': prec, 'unit': 'ns per grid point per step',
+                          'ns_per_point_step': out}))
+
+
 def batch_flops(cases, world, ms_step, clocks):
     """Algorithmic FP32 flops of one batched step: 5 N log2 N per length-N transform, N transforms
     per axis pass; 2 in the x-pass, 2 for the potential and 6 for Caldeira-Leggett order 3 (when
@@ -882,7 +914,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--replicas', type=int, default=REPLICAS)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
-    ap.add_argument('--workload', default='batch', choices=['batch', 'c128', 'dirac', 'dirac3d', 'gp'])
+    ap.add_argument('--workload', default='batch', choices=['batch', 'c128', 'dirac', 'dirac3d', 'gp', 'shardcost'])
     ap.add_argument('--profile-only', action='store_true',
                     help='batch workload: only the timed section (for profiler launch lists)')
     ap.add_argument('--precision', default='both', choices=['both', 'mixed', 'f32'],
@@ -905,6 +937,8 @@ def main():
             run_gp(args, world, rank, local)
         elif args.workload == 'dirac3d':
             run_dirac3d(args, world, rank, local)
+        elif args.workload == 'shardcost':
+            run_shardcost(args, world, rank, local)
         else:
             run_batch(args, world, rank, local)
     finally:

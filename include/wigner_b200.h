@@ -427,8 +427,10 @@ int dirac_jit_check(const dirac_desc* desc, char* log, int64_t log_cap);
  * the 11 values wig_run records for a sample it does not renormalise (norm,
  * <x>, <x^2>, <p>, <p^2>, <xp>, <V'>, <pV'>, <xV'>, <H>, negative area) --
  * written to obs_dev[WIG_NOBS] (device), for callers that cannot allocate
- * device memory (host callbacks and allocator hooks where cudaMalloc would
- * re-enter or deadlock, deployments that forbid allocation after start-up).
+ * device memory (an allocator hook, where cudaMalloc would re-enter the
+ * allocator; a deployment that forbids allocation after start-up).  Host
+ * functions run by cudaLaunchHostFunc may not call it: CUDA forbids every
+ * CUDA call there.
  * No counterpart in the reference.  It allocates nothing: its per-row partial
  * sums live in a fixed device array of 4096 rows x 12 doubles (384 KB per
  * device, held until the process exits), so n_p <= 4096 and n_x <= 4096,
@@ -438,7 +440,10 @@ int dirac_jit_check(const dirac_desc* desc, char* log, int64_t log_cap);
  * a device share the array and each overwrites the rows it reads, so calls
  * whose kernels overlap on the GPU race.  The first call on a device looks up
  * the array's address with that device current: make it before any stream
- * capture.  Asynchronous on `stream`. */
+ * capture.  Under lazy module loading (CUDA's default) that first call also
+ * loads the module that holds the array, an allocation by the driver: make it
+ * at start-up (a warm-up call), before allocation is forbidden.  Asynchronous
+ * on `stream`. */
 int wig_observables_noalloc(const void* W_dev, int32_t n_x, int32_t n_p, double dx, double dp, double mass,
                             const double* x_tab_dev, const double* p_tab_dev, const double* dv_tab_dev,
                             const double* v0_tab_dev, double* obs_dev, void* stream);

@@ -32,6 +32,7 @@
 #include "wig_dirac.cuh"
 #include "wig_batch.cuh"
 #include "wig_batch_host.h"
+#include "wig_wigner_rf.cuh"
 #include "wig_device_src.inc"   // kJitWignerSource, kJitDiracSource (generated by build.py)
 #include "wig_host.h"
 
@@ -58,6 +59,7 @@ struct Driver {
   PFN_cuLaunchKernel launch = nullptr;
   PFN_cuFuncSetAttribute setattr = nullptr;
   PFN_cuGetErrorString errstr = nullptr;
+  PFN_cuTensorMapEncodeTiled encode = nullptr;   // optional: TMA tile loads need it
   bool ok = false;
 };
 
@@ -82,6 +84,7 @@ int driver(Driver** out) {
           entry("cuLaunchKernel", g_drv.launch) && entry("cuFuncSetAttribute", g_drv.setattr) &&
           entry("cuGetErrorString", g_drv.errstr)))
       return fail(WIG_ERR_CUDA, "CUDA driver entry points unavailable (no GPU driver?)");
+    if (!entry("cuTensorMapEncodeTiled", g_drv.encode)) g_drv.encode = nullptr;
     g_drv.ok = true;
   }
   *out = &g_drv;
@@ -337,6 +340,11 @@ struct wig_handle {
   int odm = 0, smem_odm_x = 0, smem_odm_p = 0;
   double2* odm_T = nullptr;                    // 5 planes of ODM intermediates
   double odm_coef[2] = {0., 0.}, odm_sign[2] = {1., -1.};
+  int rf = 0;                                   // register-FFT x- and p-pass (wig_wigner_rf.cuh)
+  int tma = 0, rf_c = 1;                        // the p-pass tile (rf_c columns) arrives by 2-D tensor copies
+  wig::TensorMap tmap{};                        // tensor map of the W it was last encoded for
+  const void* tmap_W = nullptr;
+  int* status = nullptr;                        // [1] bounded-wait status of the kernels
   int xrows = 1, xnt = 256, pc = 1, pnt = 256, rnt = 256;
   int n_cta_x = 1, n_cta_p = 1, n_cta_r = 1;
   int smem_x = 0, smem_p = 0;
@@ -351,6 +359,8 @@ struct wig_handle {
 
 // Validation, tiling and the JIT source of one Wigner instance (no CUDA calls).
 struct WigPlan {
+  int rf = 0, rfxw = 4, rfpw = 2;   // register-FFT passes (wig_wigner_rf.cuh) and their warps per CTA
+  int tma = 0;                      // their p-pass tile by 2-D tensor copies (WIG_TMA)
   int xrows, xnt, pc, pnt, rnt, n_cta_x, n_cta_p, n_cta_r, smem_x, smem_p, damp;
   int strang, gp, smem_ph, smem_gph;
   int xminb, pminb, xr, pr;
@@ -451,6 +461,40 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
   P->smem_ph = tile_p;                                                     // first half: no damping
   P->smem_gph = (wig::padded_size(NX) + wig::padded_size(P->xrows * NX)) * (int)sizeof(double2);
 
+  // ---- register-FFT passes (wig_wigner_rf.cuh) for Lie plans without ODM damping on
+  // 64..1024-point axes, with the p-pass tile loaded by 2-D tensor copies: opt-in (WIG_RF="1",
+  // or WIG_RF="xw,pw" with the warps per x-pass / p-pass CTA).  On the 1024^2 Caldeira-Leggett
+  // case they measured slower than the Stockham passes (2.47 vs 2.18 ms per 16-replica step:
+  // 255 registers a thread leave 5 warps per SM), so the Stockham passes are the default.
+  const auto rf_size = [](int n) { return n >= 64 && n <= 1024; };
+  P->rf = 0;
+  if (const char* rv = getenv("WIG_RF")) {
+    const int eligible = (!P->strang && !P->odm && rf_size(NX) && rf_size(NP)) ? 1 : 0;
+    int v[2];
+    if (sscanf(rv, "%d,%d", &v[0], &v[1]) == 2) {
+      if (v[0] == 1 || v[0] == 2 || v[0] == 4 || v[0] == 8) P->rfxw = v[0];
+      if (v[1] == 1 || v[1] == 2 || v[1] == 4 || v[1] == 8) P->rfpw = v[1];
+      P->rf = eligible;
+    } else if (atoi(rv) != 0) {
+      P->rf = eligible;
+    }
+  }
+  if (P->rf) {
+    const int spx = wig::rf_spw(NX), spp = wig::rf_spw(NP);
+    P->rfxw = std::min(P->rfxw, std::max(1, NP / spx));   // a CTA's rows within the grid
+    P->rfpw = std::min(P->rfpw, std::max(1, NX / spp));
+    while (P->rfpw > 1 && P->rfpw * spp > 8) P->rfpw /= 2;  // a tile of at most 8 columns (128-byte rows)
+    // TMA tile loads: on unless WIG_TMA="0" (the thread loads fill the same layout)
+    const char* tv = getenv("WIG_TMA");
+    P->tma = (tv && atoi(tv) == 0) ? 0 : 1;
+    P->xnt = 32 * P->rfxw;
+    P->n_cta_x = NP / (P->rfxw * spx);
+    P->smem_x = P->rfxw * spx * (NX + (wig::rf_g(NX) == 8 ? 8 : 0)) * (int)sizeof(double2);
+    P->pnt = 32 * P->rfpw;
+    P->n_cta_p = NX / (P->rfpw * spp);
+    P->smem_p = (P->damp ? 2 : 1) * P->rfpw * spp * NP * (int)sizeof(double2) + 1024;   // + alignment slack
+  }
+
   // ---- JIT source
   P->dX = 2. * d->x_amplitude / (double)NX;
   P->dP = 2. * d->p_amplitude / (double)NP;
@@ -475,6 +519,14 @@ static int wig_plan(const wig_desc* d, WigPlan* P) {
            NX, NP, P->xrows, P->xnt, d->kinetic_from_string ? 1 : 0, P->pc, P->pnt, P->damp, P->rnt,
            P->xminb, P->pminb, d->potential_phase == WIG_PHASE_KVN ? 1 : 0, P->strang, P->xr, P->pr);
   src += macros;
+  if (P->rf) {
+    // 255 registers a thread (a 32-element FP64 sequence per lane is 128 of them)
+    snprintf(macros, sizeof(macros),
+             "#define WIG_RF 1\n#define WIG_RFXW %d\n#define WIG_RFPW %d\n#define WIG_RFXMB %d\n#define WIG_RFPMB %d\n",
+             P->rfxw, P->rfpw, std::max(1, 8 / P->rfxw), std::max(1, 8 / P->rfpw));
+    src += macros;
+    if (P->tma) src += "#define WIG_TMA 1\n";
+  }
   src += kJitWignerSource;
   P->src.swap(src);
   return WIG_OK;
@@ -511,8 +563,12 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   const std::string& src = P.src;
   CUmodule mod;
   int rc = get_module(src, h->device, &mod);
-  if (!rc) rc = get_fn(mod, "wig_xpass", &h->f_x, h->smem_x);
-  if (!rc) rc = get_fn(mod, "wig_ppass", &h->f_p, h->smem_p);
+  h->rf = P.rf;
+  h->tma = P.tma;
+  if (P.rf) h->rf_c = P.rfpw * wig::rf_spw(NP);
+  if (h->tma && !g_drv.encode) { delete h; return fail(WIG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable (set WIG_TMA=0)"); }
+  if (!rc) rc = get_fn(mod, P.rf ? "wig_xpass_rf" : "wig_xpass", &h->f_x, h->smem_x);
+  if (!rc) rc = get_fn(mod, P.rf ? "wig_ppass_rf" : "wig_ppass", &h->f_p, h->smem_p);
   if (!rc) rc = get_fn(mod, "wig_reduce", &h->f_r, 0);
   if (!rc) rc = get_fn(mod, "wig_finalize", &h->f_fin, 0);
   if (!rc) rc = get_fn(mod, "wig_scale", &h->f_scale, 0);
@@ -596,7 +652,22 @@ extern "C" int wig_create(const wig_desc* d, wig_handle** out) {
   if (!rc && h->strang) rc = B.alloc(&h->bloch_part, (size_t)h->n_cta_r * wig::NBL);
   if (!rc && h->strang) rc = B.alloc(&h->rowsums, (size_t)NP);
   if (!rc && h->gp) rc = B.alloc(&h->bloch_psq, (size_t)1);
+  double2 *rtwx_d = nullptr, *rtwp_d = nullptr;
+  if (!rc && h->rf) {
+    std::vector<double2> rx, rp;
+    rf_twiddles64(NX, &rx);
+    rf_twiddles64(NP, &rp);
+    rc = B.alloc(&rtwx_d, rx.size(), rx.data());
+    if (!rc) rc = B.alloc(&rtwp_d, rp.size(), rp.data());
+  }
   if (rc) { B.free_all(); delete h; return rc; }
+  a.rtw_x = rtwx_d;
+  a.rtw_p = rtwp_d;
+  {
+    int zero = 0;
+    if (int rc2 = B.alloc(&h->status, (size_t)1, &zero)) { B.free_all(); delete h; return rc2; }
+    a.status = h->status;
+  }
   a.r_theta_half = rth_d;
   a.gp_coef = kval(d->gp_coefficient, cm);
   a.lambda_tab = lam_d;
@@ -725,6 +796,42 @@ static int wig_run_step_strang(wig_handle* h, WigRunState* S, int64_t n, cudaStr
   return WIG_OK;
 }
 
+// The tensor map of the p-pass tile over W: (NP, NX) complex128 as a 2-D FP64 array of
+// 2 NX x NP, boxes of 2 rf_c doubles x min(NP, 256) rows, the swizzle of a rf_c * 16-byte
+// row (wig_wigner_rf.cuh: tma_sw).  The map holds W's address: it is encoded again for
+// another W.
+static int encode_tile_map(wig_handle* h, const void* W) {
+  const int NX = h->d.n_x, NP = h->d.n_p, C = h->rf_c;
+  CUtensorMap m;
+  cuuint64_t dims[2] = {(cuuint64_t)2 * NX, (cuuint64_t)NP};
+  cuuint64_t strides[1] = {(cuuint64_t)2 * NX * sizeof(double)};
+  cuuint32_t box[2] = {(cuuint32_t)(2 * C), (cuuint32_t)(NP < 256 ? NP : 256)};
+  cuuint32_t estr[2] = {1, 1};
+  const CUtensorMapSwizzle swz = C == 1 ? CU_TENSOR_MAP_SWIZZLE_NONE
+                                 : (C == 2 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                           : (C == 4 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B));
+  CUresult r = g_drv.encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(W), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(WIG_ERR_CUDA, "cuTensorMapEncodeTiled: %s", cu_err(r));
+  static_assert(sizeof(CUtensorMap) == sizeof(wig::TensorMap), "tensor map size");
+  memcpy(&h->tmap, &m, sizeof(m));
+  h->tmap_W = W;
+  return WIG_OK;
+}
+
+// Status word of the kernels' bounded waits: WIG_ERR_TIMEOUT (and cleared) if one gave up.
+static int wig_check_status(wig_handle* h, cudaStream_t st) {
+  int v = 0;
+  WIG_CUDA(cudaMemcpyAsync(&v, h->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  WIG_CUDA(cudaStreamSynchronize(st));
+  if (v) {
+    WIG_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), st));
+    return fail(WIG_ERR_TIMEOUT, "a kernel's bounded wait for its tile copy gave up");
+  }
+  return WIG_OK;
+}
+
 static int wig_run_step(wig_handle* h, WigRunState* S, int64_t n, cudaStream_t st) {
   if (h->strang) return wig_run_step_strang(h, S, n, st);
   const int first = (S->flags & WIG_RUN_CONTINUE) ? 0 : 1;
@@ -736,8 +843,15 @@ static int wig_run_step(wig_handle* h, WigRunState* S, int64_t n, cudaStream_t s
   if (int rc = launch(h->f_x, h->n_cta_x, h->xnt, h->smem_x, st, xargs)) return rc;
   if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 1], st));
   double t = (double)(S->t_index0 + n) * h->d.dt;
-  void* pargs[] = {&S->a, &S->W, &t};
-  if (int rc = launch(h->f_p, h->n_cta_p, h->pnt, h->smem_p, st, pargs)) return rc;
+  if (h->rf) {
+    if (h->tma && h->tmap_W != (const void*)S->W)
+      if (int rc = encode_tile_map(h, S->W)) return rc;
+    void* rargs[] = {&S->a, &S->W, &t, &h->tmap};
+    if (int rc = launch(h->f_p, h->n_cta_p, h->pnt, h->smem_p, st, rargs)) return rc;
+  } else {
+    void* pargs[] = {&S->a, &S->W, &t};
+    if (int rc = launch(h->f_p, h->n_cta_p, h->pnt, h->smem_p, st, pargs)) return rc;
+  }
   if (h->odm) {
     // Lindbladian_ODM_Order1 (:1637-1643); GPU_Wigner2D_ODM2 applies a damping
     // (sign +1, weight1) then a pumping (sign -1, weight2) term (:2169-2176)
@@ -787,6 +901,8 @@ extern "C" int wig_run(wig_handle* h, void* W_dev, int64_t t_index0, int64_t n_p
   if (obs_host) {
     if (int rc = wig_copy_obs(h, n_prop, obs_host, st)) return rc;
     WIG_CUDA(cudaStreamSynchronize(st));
+    if (h->tma)
+      if (int rc = wig_check_status(h, st)) return rc;
     return check_finite(obs_host, (size_t)(n_prop + 1) * WIG_NOBS, "wig_run observables");
   }
   return WIG_OK;

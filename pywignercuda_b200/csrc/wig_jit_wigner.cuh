@@ -21,7 +21,11 @@
 #ifndef WIG_STRANG
 #define WIG_STRANG 0
 #endif
+#ifndef WIG_RF
+#define WIG_RF 0
+#endif
 #include "wig_wigner.cuh"
+#include "wig_wigner_rf.cuh"
 
 __device__ __forceinline__ UserPhys user_phys(const wig::WigArgs& a) {
   UserPhys ph;
@@ -40,6 +44,24 @@ extern "C" __global__ void __launch_bounds__(WIG_PNT, WIG_PMINB)
 wig_ppass(wig::WigArgs a, double2* W, double t) {
   wig::ppass_body<UserPhys, WIG_NX, WIG_NP, WIG_PC, WIG_PNT, WIG_DAMP, WIG_KVN>(a, user_phys(a), W, t, a.partials);
 }
+
+#if WIG_RF
+// The Lie step's passes on the register-resident FFT (wig_wigner_rf.cuh): WIG_RFXW
+// warps per x-pass CTA (rf_spw(n_x) rows each), WIG_RFPW warps per p-pass CTA
+// (rf_spw(n_p) columns each); the host picks them instead of wig_xpass /
+// wig_ppass for Lie plans without ODM damping on grids of 64 to 1024 points.
+extern "C" __global__ void __launch_bounds__(WIG_RFXW * 32, WIG_RFXMB)
+wig_xpass_rf(wig::WigArgs a, double2* W, int scale_mode, double* obs_row) {
+  wig::xpass_rf_body<UserPhys, WIG_NX, WIG_NP, WIG_RFXW, WIG_KIN_STRING != 0>(a, user_phys(a), W, scale_mode,
+                                                                              obs_row);
+}
+
+// map: the tensor map of W for the tile's 2-D tensor copies (used when WIG_TMA is defined)
+extern "C" __global__ void __launch_bounds__(WIG_RFPW * 32, WIG_RFPMB)
+wig_ppass_rf(wig::WigArgs a, double2* W, double t, const __grid_constant__ wig::TensorMap map) {
+  wig::ppass_rf_body<UserPhys, WIG_NX, WIG_NP, WIG_RFPW, WIG_DAMP, WIG_KVN>(a, user_phys(a), W, t, a.partials, &map);
+}
+#endif
 
 #if WIG_STRANG
 // Strang-split step of GPU_Wigner2D_GPitaevskii (:1897-1975): first half p-pass

@@ -3,9 +3,11 @@
 //
 // The regular path (wig_run) reduces the observables through partial sums in
 // scratch that the handle allocates with cudaMalloc.  Some callers cannot
-// allocate at all -- for example code running inside a host callback or a
-// custom allocator hook where a cudaMalloc would deadlock or re-enter, or
-// deployments that forbid device allocation after start-up.  This entry point
+// allocate at all -- for example a custom allocator hook, where a cudaMalloc
+// would re-enter the allocator, or a deployment that forbids device allocation
+// after start-up.  (Host functions enqueued with cudaLaunchHostFunc are not
+// such callers: CUDA forbids any CUDA call inside them, this one included.)
+// This entry point
 // computes the same 11 observables (the sample wig_run records for a W it does
 // not normalise) with its per-row partial sums in a file-scope device array of
 // fixed size, so it allocates nothing.
@@ -15,7 +17,11 @@
 // rows it reads before reading them (nothing has to start at zero), but calls
 // whose kernels overlap on the GPU race on the array.  The first call on a
 // device looks up the array's device address (cudaGetSymbolAddress) with that
-// device current; make that first call before any stream capture.
+// device current; make that first call before any stream capture.  With CUDA's
+// lazy module loading (the default) that first call also loads this module,
+// which places the array and the kernels in device memory -- an allocation
+// the driver makes -- so make it (a warm-up call on a small W will do) at
+// start-up, before allocation is forbidden or an allocator hook is installed.
 #include <cuda_runtime.h>
 
 #include <cstdint>

@@ -71,6 +71,11 @@ struct WigArgs {
   const double* r_theta_half;  // [n_p] exp(-0.5 D_Theta theta^2 dt)  (expPotential_source :66)
   double gp_coef;              // a_GP as the kernels see it
   double coef[8];           // cf[0..7] of the expression strings
+  // register-FFT twiddle tables (wig_rfft.cuh layout, 2 n entries) of the
+  // register-FFT passes (wig_wigner_rf.cuh); null when the plan uses the Stockham ones
+  const double2* rtw_x;
+  const double2* rtw_p;
+  int* status;              // [1] set to 1 by a bounded wait that gave up (read and cleared by the host)
 };
 
 // ------------------------------------------------------------------ reductions

@@ -1,19 +1,33 @@
-"""Multi-GPU sharding of the batched FP32 form: one process per GPU, the
+"""Multi-GPU sharding of the batched form: one process per GPU, the
 independent instances partitioned across ranks, no data-path collective.
 
 Each rank advances its own share with a ``WignerBatch`` (its own persistent
 CUDA graph); the only exchange is the gather of the per-step observables to
 rank 0 at the end of a run.  Work is balanced greedily (longest processing
-time first) on the per-step cost of an instance, N_x N_p log2(N_x N_p), times
-four for a damped instance (its p-pass runs eight transforms instead of two).
+time first) on the per-step device cost of an instance: its grid points times
+the measured device time per point of its size class and damping
+(``MEASURED_NS``, from ``python bench.py --workload shardcost``); sizes outside
+the table fall back to N_x N_p log2(N_x N_p), times four when damped (the
+transform count of a damped p-pass).
 """
 import math
 
+# device time per grid point per step (ns) of the mixed-precision batched form on one B200,
+# by square size class; 'd': damped.  Measured with
+#   python bench.py --workload shardcost --steps 20 --warmup 3
+MEASURED_NS = {}
 
-def instance_cost(d):
+
+def instance_cost(d, table=None):
     """Relative per-step device cost of one batched instance descriptor."""
-    n = int(d['n_x']) * int(d['n_p'])
-    return n * math.log2(n) * (4. if float(d.get('gamma', 0.)) != 0. else 1.)
+    t = MEASURED_NS if table is None else table
+    n_x, n_p = int(d['n_x']), int(d['n_p'])
+    damped = float(d.get('gamma', 0.)) != 0.
+    key = '%d%s' % (max(n_x, n_p), 'd' if damped else '')
+    if key in t:
+        return n_x * n_p * float(t[key])
+    n = n_x * n_p
+    return n * math.log2(n) * (4. if damped else 1.) * 1e-3
 
 
 def partition(instances, world):

@@ -15,6 +15,7 @@
 #include <math.h>
 
 #include <atomic>
+#include <cstdint>
 #include <barrier>
 #include <cstdio>
 #include <cstdlib>
@@ -43,6 +44,8 @@ inline emu_dim3 blockDim, gridDim;
 #define __restrict__
 #define __launch_bounds__(...)
 #define __shared__ static
+#define __grid_constant__
+#define __align__(n) __attribute__((aligned(n)))
 
 inline unsigned char* emu_smem = nullptr;   // the running launch's dynamic shared memory
 struct emu_aligned_delete {
@@ -71,6 +74,7 @@ template <class T> inline T __ldg(const T* p) { return *p; }
 template <class T> inline T __ldcg(const T* p) { return *p; }
 
 inline unsigned atomicAdd(unsigned* p, unsigned v) { return std::atomic_ref<unsigned>(*p).fetch_add(v); }
+inline int atomicExch(int* p, int v) { return std::atomic_ref<int>(*p).exchange(v); }
 inline void __threadfence() { std::atomic_thread_fence(std::memory_order_seq_cst); }
 
 // sin / cos of pi x, evaluated in double and rounded once

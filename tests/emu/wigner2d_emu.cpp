@@ -30,6 +30,7 @@ struct UserPhys {
 };
 
 #include "wig_jit_wigner.cuh"
+#include "wig_batch_host.h"   // register-FFT twiddle tables
 
 namespace {
 
@@ -90,7 +91,10 @@ int main(int argc, char** argv) {
   const double gamma = std::atof(argv[8]);
   const int odm = std::atoi(argv[11]);
   const double a_gp = std::atof(argv[12]);
-  if (n_prop < 1 || NP % WIG_XROWS != 0 || NX % WIG_PC != 0 || (odm != 0) != (WIG_DAMP == 0)) return 2;
+  // WIG_DAMP 1: Caldeira-Leggett; 0: ODM damping (odm 1, 2) or none (gamma 0)
+  if (n_prop < 1 || NP % WIG_XROWS != 0 || NX % WIG_PC != 0 || (odm != 0 && WIG_DAMP != 0) ||
+      (odm == 0 && WIG_DAMP == 0 && gamma != 0.))
+    return 2;
   dt = std::atof(argv[7]);
   D_Theta = std::atof(argv[9]);
   D_Lambda = std::atof(argv[10]);
@@ -112,6 +116,18 @@ int main(int argc, char** argv) {
   const size_t sm_ox = 2 * tile_x, sm_op = 2 * tile_p, sm_ph = tile_p;
   const size_t sm_gph = ((size_t)wig::padded_size(NX) + wig::padded_size(WIG_XROWS * NX)) * sizeof(double2);
   const int n_cta_r = clampi(NX * NP / (4 * WIG_RNT), 1, 296);
+#if WIG_RF
+  // the register-FFT passes (wig_plan's rf branch)
+  const int rf_gx = NP / (WIG_RFXW * wig::rf_spw(NX)), rf_gp = NX / (WIG_RFPW * wig::rf_spw(NP));
+  const size_t sm_rx = (size_t)WIG_RFXW * wig::rf_spw(NX) * (NX + (wig::rf_g(NX) == 8 ? 8 : 0)) * sizeof(double2);
+  const size_t sm_rp = (size_t)(WIG_DAMP == 1 ? 2 : 1) * WIG_RFPW * wig::rf_spw(NP) * NP * sizeof(double2) + 1024;
+  const wig::TensorMap no_map{};   // the thread-load path of the emulation takes no tensor map
+  std::vector<double2> rtwx, rtwp;
+  wighost::rf_twiddles64(NX, &rtwx);
+  wighost::rf_twiddles64(NP, &rtwp);
+#else
+  const int rf_gx = 1, rf_gp = 1;
+#endif
 
   wig::WigArgs a{};
   a.dt = dt; a.dx = dx; a.dp = dp; a.dtheta = dtheta; a.dlambda = dlambda; a.mass = mass; a.hbar = hBar;
@@ -137,7 +153,7 @@ int main(int argc, char** argv) {
   }
   std::vector<double2> twx = twiddles(NX), twp = twiddles(NP);
   std::vector<double> rl(NX), rt(NP), m1(NX), m2(NX), sfp(NP), rth(NP);
-  const int nparts = n_cta_x > n_cta_p ? (n_cta_x > n_cta_r ? n_cta_x : n_cta_r) : (n_cta_p > n_cta_r ? n_cta_p : n_cta_r);
+  const int nparts = std::max(std::max(std::max(n_cta_x, n_cta_p), n_cta_r), std::max(rf_gx, rf_gp));
   std::vector<double> partials((size_t)nparts * wig::NACC, 0.), partials_im(odm ? (size_t)nparts * wig::NIM : 0, 0.);
   std::vector<double> obs((size_t)(n_prop + 1) * NOBS, 0.);
   double2 scale{1., 0.};
@@ -148,6 +164,12 @@ int main(int argc, char** argv) {
   a.lambda_tab = lt.data(); a.hbar_exact = hBar; a.L_material = 1.;
   a.r_theta_half = rth.data();
   a.gp_coef = a_gp;
+#if WIG_RF
+  a.rtw_x = rtwx.data();
+  a.rtw_p = rtwp.data();
+#endif
+  int status = 0;
+  a.status = &status;
   emu_launch(1, 64, [&] { wig_setup(a, rl.data(), rt.data(), m1.data(), m2.data(), sfp.data(), rth.data()); });
   // Lindbladian_ODM_Order1: scale dt 2 gamma weight / n_p, five intermediate planes; odm 1: one term
   // (weight 1, sign 1), odm 2: GPU_Wigner2D_ODM2's damping (weight 1, sign 1) then pumping (weight 0.5,
@@ -256,6 +278,9 @@ int main(int argc, char** argv) {
     emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, 0, nullptr); }, sm_x);
     if (gp) gp_terms(0, psq.data() + n);
     emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass_half_final(a, Wp, t, gph); }, sm_p);
+#elif WIG_RF
+    emu_launch(rf_gx, WIG_RFXW * 32, [&] { wig_xpass_rf(a, Wp, mode, orow); }, sm_rx);
+    emu_launch(rf_gp, WIG_RFPW * 32, [&] { wig_ppass_rf(a, Wp, t, no_map); }, sm_rp);
 #else
     emu_launch(n_cta_x, WIG_XNT, [&] { wig_xpass(a, Wp, mode, orow); }, sm_x);
     emu_launch(n_cta_p, WIG_PNT, [&] { wig_ppass(a, Wp, t); }, sm_p);
@@ -265,7 +290,7 @@ int main(int argc, char** argv) {
       emu_launch(n_cta_x, WIG_XNT, [&] { wig_odm_xpass(a, Wp, T.data()); }, sm_ox);
       emu_launch(n_cta_p, WIG_PNT, [&] { wig_odm_ppass(a, Wp, T.data(), coef, sign); }, sm_op);
     }
-    a.n_partials = n_cta_p;
+    a.n_partials = WIG_RF ? rf_gp : n_cta_p;
   }
   // wig_run_end
   {

@@ -26,7 +26,7 @@ CSRC = os.path.join(ROOT, 'pywignercuda_b200', 'csrc')
 EMU = os.path.join(ROOT, 'tests', 'emu')
 HEADERS = ('wig_fft.cuh', 'wig_wigner.cuh', 'wig_dirac.cuh', 'wig_jit_dirac.cuh', 'wig_jit_wigner.cuh',
            'wig_dirac3.cuh', 'wig_jit_dirac3.cuh', 'wig_rfft.cuh', 'wig_batch.cuh', 'wig_jit_batch.cuh',
-           'wig_adjoint.cuh', 'wig_jit_adjoint.cuh', 'wig_batch_host.h', 'wig_adjoint_host.h')
+           'wig_adjoint.cuh', 'wig_jit_adjoint.cuh', 'wig_batch_host.h', 'wig_adjoint_host.h', 'wig_wigner_rf.cuh')
 EXTERN_SHARED = re.compile(r'extern\s+__shared__\s+(\w+)\s+(\w+)\s*\[\s*\]\s*;')
 
 NX, NY = 32, 16
@@ -135,6 +135,37 @@ def test_wigner2d_device_code_matches_oracle(staged, xrows, xnt, pc, pnt, odm, k
     assert np.all(np.abs(obs[:, :10] - ref_obs[:, :10]) / scale < 1e-10), (obs[:, :10] - ref_obs[:, :10]) / scale
     # the negative area (here ~ -4e-5) sums the points below zero: points within rounding of zero
     # enter one sum and not the other, so it is held to an absolute 1e-12
+    assert np.all(np.abs(obs[:, 10] - ref_obs[:, 10]) < 1e-12), obs[:, 10] - ref_obs[:, 10]
+
+
+# The register-FFT x- and p-pass of Lie plans (wig_wigner_rf.cuh) on a 128 x 64 grid: Caldeira-Leggett,
+# undamped, the Fokker-Planck (KvN) factor; one and several warps per CTA
+@pytest.mark.parametrize('xw,pw,kvn,gamma', [(4, 2, 0, WGAMMA), (1, 1, 0, WGAMMA), (2, 2, 0, 0.), (4, 1, 1, WGAMMA)])
+def test_wigner2d_rf_device_code_matches_oracle(staged, xw, pw, kvn, gamma):
+    nx, npp = 128, 64
+    damp = int(gamma != 0.)
+    exe = build(staged, 'wigner2d_emu.cpp', dict(WIG_NX=nx, WIG_NP=npp, WIG_XROWS=1, WIG_XNT=32, WIG_KIN_STRING=0,
+                                                 WIG_PC=2, WIG_PNT=32, WIG_DAMP=damp, WIG_RNT=256, WIG_XMINB=1,
+                                                 WIG_PMINB=1, WIG_KVN=kvn, WIG_RF=1, WIG_RFXW=xw, WIG_RFPW=pw,
+                                                 WIG_RFXMB=1, WIG_RFPMB=1))
+    prm = WignerParams(nx, npp, WXA, WPA, WDT, d_theta=WDTH, d_lambda=WDLA, gamma=gamma, potential=WPOT,
+                       dpotential=WDPOT, kinetic='0.5*p*p', damping='CaldeiraLeggett', fp_damping='fabs(p)',
+                       kvn=bool(kvn), constants='exact')
+    X = np.fft.fftshift(np.linspace(-WXA, WXA - 2 * WXA / nx, nx))[np.newaxis, :]
+    P = np.fft.fftshift(np.linspace(-WPA, WPA - 2 * WPA / npp, npp))[:, np.newaxis]
+    W0 = np.ascontiguousarray(np.exp(-(X - 1.5) ** 2 - (P + 0.5) ** 2 * 1.3) + 0. * 1j)
+    steps = 2
+    fin, fout, fobs = (os.path.join(staged, n) for n in ('wr_in.bin', 'wr_out.bin', 'wr_obs.bin'))
+    W0.tofile(fin)
+    r = subprocess.run([exe, fin, fout, fobs, str(steps)] + [repr(v) for v in (WXA, WPA, WDT, gamma, WDTH, WDLA)] +
+                       ['0', '0.'], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.fromfile(fout, dtype=np.complex128).reshape(npp, nx)
+    obs = np.fromfile(fobs).reshape(steps + 1, 11)
+    ref_obs, ref = WignerOracle(prm).run(W0, steps)
+    assert rel_l2(got, ref) < 1e-12, rel_l2(got, ref)
+    scale = np.maximum(np.abs(ref_obs[:, :10]).max(axis=0), 1e-3)
+    assert np.all(np.abs(obs[:, :10] - ref_obs[:, :10]) / scale < 1e-10), (obs[:, :10] - ref_obs[:, :10]) / scale
     assert np.all(np.abs(obs[:, 10] - ref_obs[:, 10]) < 1e-12), obs[:, 10] - ref_obs[:, 10]
 
 
