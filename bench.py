@@ -582,6 +582,9 @@ def run_batch(args, world, rank, local):
     if args.profile_only:
         if rank == 0:
             print(json.dumps({'metric': METRIC, 'value': value, 'unit': UNIT, 'steps': K,
+                              'forms': {p: {'ms_per_step': legs[p]['ms'] / K, 'x_pass_us': legs[p]['x_us'],
+                                            'p_pass_us': legs[p]['p_us'], 'warps_per_cta': legs[p]['warps']}
+                                        for p in legs},
                               'note': 'profile-only run (timed section only)'}))
         return
     batch, total = head['batch'], head['batch'].total

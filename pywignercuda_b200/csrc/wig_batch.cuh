@@ -79,17 +79,19 @@ struct BArgs {
   unsigned* counters;    // [n_inst]
   unsigned* tickets;     // [2] work-list tickets of the x- and p-pass (zero between launches)
   double* scale;         // [n_inst] pending normalisation, applied by the next x-pass
+  unsigned* status;      // [1] set to 1 by a bounded wait that gave up (read and cleared by the host)
   double* obs;           // [n_inst][obs_stride][NOBS]
   int obs_stride;
 };
 
-// Shared memory of one item (float2 units): the x-pass exchange regions; the
-// p-pass tile and its Caldeira-Leggett copy A.  The twiddle and factor tables
-// are read through the read-only data path (a few KB per size, L1-resident).
-// x-pass: each lane group carries two rows packed into one complex sequence and
-// holds, per row pair, the transform exchange / spectrum region and a factor region.
+// Shared memory of one item: the x-pass exchange regions and row staging buffer
+// (bx_exch, bx_stage), the p-pass tile (float2 units).  The twiddle and factor
+// tables are read through the read-only data path (a few KB per size,
+// L1-resident).  x-pass: each lane group carries two rows packed into one
+// complex sequence and holds, per row pair, the transform exchange / spectrum
+// region.
 __host__ __device__ constexpr int bx_rows(int n, int warps) { return 2 * warps * rf_spw(n); }
-__host__ __device__ constexpr int bx_smem(int n, int warps) { return 2 * warps * rf_spw(n) * (n + (rf_g(n) == 8 ? 8 : 0)); }
+// (the x-pass's shared memory: bx_exch / bx_stage below)
 // The p-pass packs two real columns into one complex sequence for the
 // Caldeira-Leggett part (see batch_p_item): an item is BP_PACK column groups.
 constexpr int BP_PACK = 2;
@@ -228,87 +230,32 @@ __device__ __forceinline__ int next_item(unsigned* ticket, int n_items) {
 
 // ------------------------------------------------------------------ x-pass
 // Item: bx_rows(N) consecutive rows; lane group `pair` carries rows ra = row0 +
-// 2 pair and rb = ra + 1 packed into z = Re W(ra) + i Re W(rb) (W is real), lane
-// g holding elements g + G m.  The kinetic factor differs between the two rows,
+// 2 pair and rb = ra + 1 packed into z = W(ra) + i W(rb) (W is real), lane g
+// holding elements g + G m.  The kinetic factor differs between the two rows,
 // so the spectrum is split with its mirror: for real rows a, b with z = a + i b,
 //   Z'(k) = [Z(k) (fa + fb) + conj Z(N - k) (fa - fb)] / 2
 // is the spectrum of a' + i b', a' = IFFT[fa FFT a], b' = IFFT[fb FFT b]
 // (fa, fb map Hermitian spectra to Hermitian spectra).  Rows ra, rb differ by
 // one p step, so fb = fa g(lambda) with g = exp(-i dt dp lambda / m), a table.
 // One transform pair per two rows.
-template <int N>
-__device__ __forceinline__ void batch_x_item_f32(const BArgs& A, int inst, const BInst& I, int row0) {
-  typedef RegFft<float2, N> F;
-  constexpr int E = F::E, G = F::G, Q = F::Q, SPW = rf_spw(N);
-  constexpr int XS = N + (G == 8 ? 8 : 0);
-  extern __shared__ float2 smb[];
-  const float2* tf = A.tw + I.tw_x;
-  const float2* ti = tf + N;
-  const float* rtab = A.ft + I.ft_x;            // exp(-D_lambda lambda^2) / N
-  const float* gtab = rtab + 2 * N;             // exp(-i dt dp lambda / m): (cos, -sin) pairs
-  float2* X = smb;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
-  const int pair = warp * SPW + grp;
-  const int ra = row0 + 2 * pair;
-  WIG_BOUNDS_CHECK("batched x-pass row", ra + 1, I.n_p);
-  const float sc = (float)A.scale[inst];
-  float* Wa = A.W + I.off + (size_t)ra * N;
-  float* Wb = Wa + N;
-  float2 v[E];
-#pragma unroll
-  for (int m = 0; m < E; ++m) v[m] = make_float2(Wa[g + G * m] * sc, Wb[g + G * m] * sc);
-  const PlainSlot sl{pair * 2 * XS};            // exchange, then the spectrum in natural order
-  const PlainSlot sf{pair * 2 * XS + XS};       // row a's kinetic factors
-  F::fwd(v, X, sl, tf, g);
-  __syncwarp();   // the transform's exchange reads are done before the spectrum is staged
-#pragma unroll
-  for (int e = 0; e < E; ++e) X[sl(g * Q + e / G + E * (e % G))] = v[e];
-  // kinetic factor of row a, exp(-i dt lambda p / m), in turns (rolled: one copy of the
-  // FP64 reduction + sincospif per kernel)
-  const double cq = I.dt * I.dp * I.dlambda * (double)shifted(ra, I.n_p) / (I.mass * 6.283185307179586477);
-#pragma unroll 2
-  for (int e = 0; e < E; ++e) {
-    const int i = e / G, b = e % G;
-    const int k = g * Q + i + E * b;
-    const int lj = b < G / 2 ? k : k - N;
-    X[sf(e * G + g)] = turn_factor(cq * (double)lj, 1.f);
-  }
-  __syncwarp();
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const int k = g * Q + e / G + E * (e % G);
-    const float2 P = X[sl((N - k) & (N - 1))];
-    float2 fa = X[sf(e * G + g)];
-    float2 fb = cmul(fa, make_float2(__ldg(gtab + 2 * k), __ldg(gtab + 2 * k + 1)));
-    if (k == N / 2) { fa.y = 0.f; fb.y = 0.f; }     // Nyquist: see nyquist_real
-    const float r = 0.5f * __ldg(rtab + k);
-    v[e] = cscale(cadd(cmul(v[e], cadd(fa, fb)), cmul(cconj(P), csub(fa, fb))), r);
-  }
-  F::inv(v, X, sl, ti, g);
-#pragma unroll
-  for (int m = 0; m < E; ++m) {
-    Wa[g + G * m] = v[m].x;
-    Wb[g + G * m] = v[m].y;
-  }
-}
 
-// Mirror split of a packed FP64 spectrum staged in natural order in the
-// exchange x (slots 0..N-1), in place:
+// Mirror split of a packed spectrum staged in natural order in the exchange x
+// (slots 0..N-1), in place:
 //   Z'(k) = Z(k) (fa(k) + fb(k)) + conj Z(N - k) (fa(k) - fb(k))
 // (fab(k, &fa, &fb) returns the two sequences' factors with the 1/2 folded in).
 // Each lane of the group owns the mirror pairs (q, N - q), q = g, g + G, ...,
 // q <= N/2, so no other lane reads a slot it rewrites.  The loop stays rolled:
-// one copy of the factor code (FP64 sincospi) per kernel.
-template <int N, int G, class X, class Fab>
-__device__ __forceinline__ void mirror_split64(const X& x, int g, const Fab& fab) {
+// one copy of the factor code (the phase reduction and sincospi) per kernel.
+template <int N, int G, class C, class X, class Fab>
+__device__ __forceinline__ void mirror_split(const X& x, int g, const Fab& fab) {
 #pragma unroll 1
   for (int q = g; q <= N / 2; q += G) {
     const int km = (N - q) & (N - 1);
-    const double2 Z = x.get(q), P = x.get(km);
-    double2 fa, fb;
+    const C Z = x.get(q), P = x.get(km);
+    C fa, fb;
     fab(q, &fa, &fb);
     if (q == N / 2) { fa.y = 0.; fb.y = 0.; }       // Nyquist: see nyquist_real
-    const double2 Zn = cadd(cmul(Z, cadd(fa, fb)), cmul(cconj(P), csub(fa, fb)));
+    const C Zn = cadd(cmul(Z, cadd(fa, fb)), cmul(cconj(P), csub(fa, fb)));
     if (km != q) {
       fab(km, &fa, &fb);
       x.put(km, cadd(cmul(P, cadd(fa, fb)), cmul(cconj(Z), csub(fa, fb))));
@@ -317,48 +264,79 @@ __device__ __forceinline__ void mirror_split64(const X& x, int g, const Fab& fab
   }
 }
 
-// The same row pair in FP64 (WIGB_PREC 1): the rows are widened on load, the
-// transform pair, the kinetic factor exp(-i dt lambda p / m) (FP64 sincospi of
-// the turn-reduced argument) and the mirror split run in FP64, and the result
-// is rounded to FP32 once, on store.  The spectrum is staged in natural order
-// in the pair's exchange region (N double2) and split there in place.
-template <int N>
-__device__ __forceinline__ void batch_x_item_f64(const BArgs& A, int inst, const BInst& I, int row0) {
-  typedef RegFft<double2, N> F;
+// The precision of an x-pass: its complex type's twiddle and factor tables.
+template <class C> struct XPrec;
+template <> struct XPrec<float2> {
+  __device__ __forceinline__ static const float2* tw(const BArgs& A, const BInst& I) { return A.tw + I.tw_x; }
+  // 0.5 r_lambda(k) exp(-2 pi i t), and the row-pair ratio exp(-i dt dp lambda / m)
+  __device__ __forceinline__ static float2 fa(const BArgs& A, const BInst& I, double t, int k) {
+    return turn_factor(t, 0.5f * __ldg(A.ft + I.ft_x + k));
+  }
+  __device__ __forceinline__ static float2 g(const BArgs& A, const BInst& I, int N, int k) {
+    const float* gt = A.ft + I.ft_x + 2 * N;
+    return make_float2(__ldg(gt + 2 * k), __ldg(gt + 2 * k + 1));
+  }
+};
+template <> struct XPrec<double2> {
+  __device__ __forceinline__ static const double2* tw(const BArgs& A, const BInst& I) { return A.tw64 + I.tw_x; }
+  __device__ __forceinline__ static double2 fa(const BArgs& A, const BInst& I, double t, int k) {
+    return turn_factor64(t, 0.5 * __ldg(A.fd + I.fd_x + k));
+  }
+  __device__ __forceinline__ static double2 g(const BArgs& A, const BInst& I, int N, int k) {
+    return __ldg(reinterpret_cast<const double2*>(A.fd + I.fd_x + 2 * N) + k);
+  }
+};
+
+// One x-item in the arithmetic of C (float2: FP32; double2: FP64, rounded to
+// FP32 once on store).  rows: the item's bx_rows(N) rows of W (in global memory
+// or staged in shared memory); after_load() runs once every lane holds its two
+// rows in registers (the caller may then reuse the staging buffer).  The
+// spectrum is staged in natural order in the pair's exchange region (N
+// elements of C) and split there in place.
+template <class C, int N, class After>
+__device__ __forceinline__ void batch_x_item_t(const BArgs& A, int inst, const BInst& I, int row0, const float* rows,
+                                               const After& after_load) {
+  typedef RegFft<C, N> F;
+  typedef XPrec<C> PR;
   constexpr int E = F::E, G = F::G, Q = F::Q, SPW = rf_spw(N);
-  constexpr int XS = N + (G == 8 ? 8 : 0);     // region stride (double2); bx_smem holds 2 XS float2 per pair
+  constexpr int XS = N + (G == 8 ? 8 : 0);     // region stride (elements of C)
   extern __shared__ float2 smb[];
-  const double2* tf = A.tw64 + I.tw_x;
-  const double2* ti = tf + N;
-  const double* rtab = A.fd + I.fd_x;                                   // exp(-D_lambda lambda^2) / N
-  const double2* gtab = reinterpret_cast<const double2*>(rtab + 2 * N);  // exp(-i dt dp lambda / m)
-  double2* X = reinterpret_cast<double2*>(smb);
+  C* X = reinterpret_cast<C*>(smb);
+  const C* tf = PR::tw(A, I);
+  const C* ti = tf + N;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, grp = lane / G, g = lane % G;
   const int pair = warp * SPW + grp;
   const int ra = row0 + 2 * pair;
   WIG_BOUNDS_CHECK("batched x-pass row", ra + 1, I.n_p);
   const double sc = A.scale[inst];
-  float* Wa = A.W + I.off + (size_t)ra * N;
-  float* Wb = Wa + N;
-  double2 v[E];
+  const float* Ra = rows + (size_t)(2 * pair) * N;
+  const float* Rb = Ra + N;
+  C v[E];
 #pragma unroll
-  for (int m = 0; m < E; ++m) v[m] = make_double2((double)Wa[g + G * m] * sc, (double)Wb[g + G * m] * sc);
-  const SlotX<double2, PlainSlot> x{X, PlainSlot{pair * XS}};
+  for (int m = 0; m < E; ++m) {
+    v[m].x = (decltype(v[m].x))((double)Ra[g + G * m] * sc);
+    v[m].y = (decltype(v[m].y))((double)Rb[g + G * m] * sc);
+  }
+  after_load();
+  const SlotX<C, PlainSlot> x{X, PlainSlot{pair * XS}};
   F::fwdx(v, x, tf, g);
   __syncwarp();   // the transform's exchange reads are done before the spectrum is staged
 #pragma unroll
   for (int e = 0; e < E; ++e) x.put(g * Q + e / G + E * (e % G), v[e]);
   __syncwarp();
+  // kinetic factor of row a, exp(-i dt lambda p / m), in turns
   const double cq = I.dt * I.dp * I.dlambda * (double)shifted(ra, I.n_p) / (I.mass * 6.283185307179586477);
-  mirror_split64<N, G>(x, g, [&](int k, double2* fa, double2* fb) {
+  mirror_split<N, G, C>(x, g, [&](int k, C* fa, C* fb) {
     const int lj = k < N / 2 ? k : k - N;
-    *fa = turn_factor64(cq * (double)lj, 0.5 * __ldg(rtab + k));
-    *fb = cmul(*fa, __ldg(gtab + k));
+    *fa = PR::fa(A, I, cq * (double)lj, k);
+    *fb = cmul(*fa, PR::g(A, I, N, k));
   });
   __syncwarp();
 #pragma unroll
   for (int e = 0; e < E; ++e) v[e] = x.get(g * Q + e / G + E * (e % G));
   F::invx(v, x, ti, g);
+  float* Wa = A.W + I.off + (size_t)ra * N;
+  float* Wb = Wa + N;
 #pragma unroll
   for (int m = 0; m < E; ++m) {
     Wa[g + G * m] = (float)v[m].x;
@@ -366,14 +344,18 @@ __device__ __forceinline__ void batch_x_item_f64(const BArgs& A, int inst, const
   }
 }
 
-template <int N>
-__device__ __forceinline__ void batch_x_item(const BArgs& A, int inst, const BInst& I, int row0) {
 #if WIGB_PREC == 1
-  batch_x_item_f64<N>(A, inst, I, row0);
+typedef double2 XC;
 #else
-  batch_x_item_f32<N>(A, inst, I, row0);
+typedef float2 XC;
 #endif
+
+// The x-pass's exchange regions (elements of float2: an FP64 region of N double2
+// spans 2 N of them) and staging buffer (floats) of one item of size class N.
+__host__ __device__ constexpr int bx_exch(int n, int warps, int prec) {
+  return warps * rf_spw(n) * (n + (rf_g(n) == 8 ? 8 : 0)) * (prec == 1 ? 2 : 1);
 }
+__host__ __device__ constexpr int bx_stage(int n, int warps) { return bx_rows(n, warps) * n; }
 
 // ------------------------------------------------------------------ p-pass
 // Item: a tile of CT2 = BP_PACK * WIGB_WARPS * rf_spw(N) columns x N rows, staged
@@ -465,7 +447,7 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
 #pragma unroll
     for (int e = 0; e < E; ++e) px.put(g * Q + e / G + E * (e % G), z[e]);
     __syncwarp();
-    mirror_split64<N, G>(px, g, [&](int k, double2* fa, double2* fb) {
+    mirror_split<N, G, double2>(px, g, [&](int k, double2* fa, double2* fb) {
       const double j = (double)(k < N / 2 ? k : k - N);
       const double r = 0.5 * __ldg(rth64 + k);
       *fa = turn_factor64(j * fma(bea, j * j, ala), r * mma64);

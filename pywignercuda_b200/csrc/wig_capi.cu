@@ -1483,7 +1483,25 @@ struct BVariant {
   int smem_x = 0, smem_p = 0, occ_x = 1, occ_p = 1;
 };
 
-int batch_smem_x(int n, int warps) { return wig::bx_smem(n, warps) * (int)sizeof(float2); }
+// Whether the x-pass stages its rows in shared memory (WIGB_XSTAGE): on for the
+// mixed form, whose FP64 transforms leave the loads' latency exposed; off for the
+// FP32 form, which hides it with more resident warps.  Tuning override (read per
+// compile): WIG_BATCH_XSTAGE=0|1.
+int batch_xstage(int prec) {
+  const char* e = getenv("WIG_BATCH_XSTAGE");
+  if (e && *e) return atoi(e) ? 1 : 0;
+  return prec == WIGB_PREC_MIXED ? 1 : 0;
+}
+
+// the x-pass's exchange regions and row staging buffer (wigb_xpass: the largest size class's each)
+int batch_smem_x(const std::vector<int>& classes, int warps, int prec, int xstage) {
+  int ex = 0, st = 0;
+  for (int n : classes) {
+    ex = std::max(ex, wig::bx_exch(n, warps, prec));
+    st = std::max(st, wig::bx_stage(n, warps));
+  }
+  return ex * (int)sizeof(float2) + (xstage ? st * (int)sizeof(float) : 0);
+}
 int batch_smem_p(int n, int warps) { return wig::bp_smem(n, warps) * (int)sizeof(float2); }
 
 }  // namespace
@@ -1518,7 +1536,7 @@ struct wigb_handle {
   size_t flush_bytes = 0;
 };
 
-static std::string wigb_source(const std::vector<int>& classes, int warps, int precision) {
+static std::string wigb_source(const std::vector<int>& classes, int warps, int precision, int xstage) {
   // register cap: 8-warp tiles run one CTA per SM (255 registers); smaller FP32
   // tiles three 4-warp / six 2-warp CTAs (168 registers), mixed-precision ones
   // two 4-warp / four 2-warp CTAs (255: an FP64 sequence of 32 elements per
@@ -1531,7 +1549,8 @@ static std::string wigb_source(const std::vector<int>& classes, int warps, int p
   const int noinline = ni && atoi(ni) ? 1 : 0;
   snprintf(head, sizeof(head),
            "#define WIGB_WARPS %d\n#define WIGB_PREC %d\n#define WIGB_XMINB %d\n#define WIGB_PMINB %d\n"
-           "#define WIGB_NOINLINE %d\n#define WIGB_CASES(F)", warps, precision, minb, minb, noinline);
+           "#define WIGB_NOINLINE %d\n#define WIGB_XSTAGE %d\n#define WIGB_BULK 1\n#define WIGB_CASES(F)", warps,
+           precision, minb, minb, noinline, xstage);
   std::string src = head;
   for (int n : classes) src += " F(" + std::to_string(n) + ")";
   src += "\n";
@@ -1553,18 +1572,16 @@ extern "C" int wigb_jit_check(const int32_t* sizes, int64_t n_sizes, int32_t war
   std::lock_guard<std::mutex> lk(g_mu);
   std::vector<char> cubin;
   std::string lg;
-  int rc = nvrtc_compile(wigb_source(cls, warps, precision), &cubin, &lg, true);
+  int rc = nvrtc_compile(wigb_source(cls, warps, precision, batch_xstage(precision)), &cubin, &lg, true);
   copy_log(rc ? g_last_error : lg, log, log_cap);
   return rc;
 }
 
 static int wigb_compile(wigb_handle* h, int warps, BVariant* v) {
-  const std::string src = wigb_source(h->classes, warps, h->precision);
-  int smx = 0, smp = 0;
-  for (int n : h->classes) {
-    smx = std::max(smx, batch_smem_x(n, warps));
-    smp = std::max(smp, batch_smem_p(n, warps));
-  }
+  const int xstage = batch_xstage(h->precision);
+  const std::string src = wigb_source(h->classes, warps, h->precision, xstage);
+  int smx = batch_smem_x(h->classes, warps, h->precision, xstage), smp = 0;
+  for (int n : h->classes) smp = std::max(smp, batch_smem_p(n, warps));
   if (smx > 227 * 1024 || smp > 227 * 1024)
     return fail(WIG_ERR_ARG, "batched tile of %d warps needs %d / %d bytes of shared memory", warps, smx, smp);
   CUmodule mod;
@@ -1711,6 +1728,7 @@ extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t war
   wig::BInst* inst_d = nullptr;
   unsigned* cnt_d = nullptr;
   unsigned* tick_d = nullptr;
+  unsigned* status_d = nullptr;
   double* scale_d = nullptr;
   int rc = B.alloc(&tw_d, tw.size(), tw.data());
   if (!rc) rc = B.alloc(&tw64_d, tw64.size(), tw64.data());
@@ -1719,10 +1737,12 @@ extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t war
   if (!rc) rc = B.alloc(&inst_d, (size_t)count);
   if (!rc) rc = B.alloc(&cnt_d, (size_t)count);
   if (!rc) rc = B.alloc(&tick_d, (size_t)2);
+  if (!rc) rc = B.alloc(&status_d, (size_t)1);
   if (!rc) rc = B.alloc(&scale_d, (size_t)count);
   if (!rc) {
     cudaError_t e = cudaMemset(cnt_d, 0, count * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(tick_d, 0, 2 * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(status_d, 0, sizeof(unsigned));
     if (e != cudaSuccess) rc = fail(WIG_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
   }
   if (rc) { B.free_all(); delete h; return rc; }
@@ -1733,6 +1753,7 @@ extern "C" int wigb_create(const wigb_instance* inst, int64_t count, int32_t war
   h->a.inst = inst_d;
   h->a.counters = cnt_d;
   h->a.tickets = tick_d;
+  h->a.status = status_d;
   h->a.scale = scale_d;
   if ((rc = wigb_set_warps(h, warps ? warps : 8))) { wigb_destroy(h); return rc; }
   *out = h;
@@ -1830,8 +1851,14 @@ extern "C" int wigb_run(wigb_handle* h, void* W_dev, int64_t t_index0, int64_t n
     if (int rc = wigb_launch_run(h, W, t_index0, n_prop, flags, st)) return rc;
   }
   if (obs_host) {
+    unsigned status = 0;
     WIG_CUDA(cudaMemcpyAsync(obs_host, h->obs, nobs * sizeof(double), cudaMemcpyDeviceToHost, st));
+    WIG_CUDA(cudaMemcpyAsync(&status, h->a.status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     WIG_CUDA(cudaStreamSynchronize(st));
+    if (status) {
+      WIG_CUDA(cudaMemsetAsync(h->a.status, 0, sizeof(unsigned), st));
+      return fail(WIG_ERR_TIMEOUT, "wigb_run: an x-pass wait for its staged rows gave up");
+    }
     return check_finite(obs_host, nobs, "wigb_run observables");
   }
   return WIG_OK;

@@ -3,6 +3,7 @@
 //   #define WIGB_WARPS <warps per CTA>   (the autotuned tile shape)
 //   #define WIGB_CASES(F) F(128) F(256) ...   (the size classes present)
 //   #define WIGB_PREC 0 | 1                      (FP32 / mixed precision, wig_batch.cuh)
+//   #define WIGB_XSTAGE 0 | 1                    (x-pass rows staged in shared memory)
 // Each kernel is persistent over its work list: the x- and p-pass draw items
 // from a ticket counter, the one-off reduce / scale kernels take items
 // b, b + gridDim.x, ...
@@ -27,18 +28,136 @@
 #else
 #define WIGB_CASE_INLINE __forceinline__
 #endif
-template <int N> __device__ WIGB_CASE_INLINE void wigb_x_case(const wig::BArgs& A, int inst, const wig::BInst& I, int row0) {
-  wig::batch_x_item<N>(A, inst, I, row0);
-}
 template <int N> __device__ WIGB_CASE_INLINE void wigb_p_case(const wig::BArgs& A, int inst, const wig::BInst& I, int col0,
                                                           int item, int sample) {
   wig::batch_p_item<N>(A, inst, I, col0, item, sample);
 }
-#define WIGB_X_CASE(N) case N: wigb_x_case<N>(A, it.x, sI, it.y); break;
 #define WIGB_P_CASE(N) case N: wigb_p_case<N>(A, it.x, sI, it.y, item, sample); break;
 #define WIGB_R_CASE(N) case N: wig::batch_reduce_item<N>(A, it.x, sI, it.y, item, mode, sample); break;
 #define WIGB_S_CASE(N) case N: wig::batch_scale_item<N>(A, it.x, sI, it.y); break;
 
+// ---------------------------------------------------------------- x-pass row staging
+// The x-pass is persistent over its work list, and each item's rows are one
+// contiguous block of W: while a CTA transforms an item, the next item's rows
+// are already on their way into a staging buffer in shared memory.  With
+// WIGB_BULK (the library's GPU build) the block arrives by a bulk asynchronous
+// copy (cp.async.bulk, completing on an mbarrier; no multicast); the wait is
+// bounded and, when it gives up, records 1 in A.status (the host reports
+// WIG_ERR_TIMEOUT).  Without it (host execution of this code) thread 0 copies
+// the block, ordered by the CTA's barriers.
+#define WIGB_XEXCH_F(N) m = m > wig::bx_exch(N, WIGB_WARPS, WIGB_PREC) ? m : wig::bx_exch(N, WIGB_WARPS, WIGB_PREC);
+#define WIGB_XSTAGE_F(N) m = m > wig::bx_stage(N, WIGB_WARPS) ? m : wig::bx_stage(N, WIGB_WARPS);
+__host__ __device__ constexpr int wigb_xexch_max() {
+  int m = 0;
+  WIGB_CASES(WIGB_XEXCH_F)
+  return m;
+}
+__host__ __device__ constexpr int wigb_xstage_max() {
+  int m = 0;
+  WIGB_CASES(WIGB_XSTAGE_F)
+  return m;
+}
+
+#ifdef WIGB_BULK
+__device__ __forceinline__ unsigned wigb_smem(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void wigb_stage_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(wigb_smem(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void wigb_stage_copy(float* dst, const float* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(wigb_smem(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   wigb_smem(dst)),
+               "l"(src), "r"(bytes), "r"(wigb_smem(bar))
+               : "memory");
+}
+__device__ __forceinline__ void wigb_stage_wait(unsigned long long* bar, unsigned phase, unsigned* status) {
+  unsigned done = 0;
+#pragma unroll 1
+  for (long it = 0; it < (1L << 24) && !done; ++it)
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(wigb_smem(bar)), "r"(phase)
+        : "memory");
+  if (!done && threadIdx.x == 0) atomicExch(status, 1u);
+}
+#else
+__device__ __forceinline__ void wigb_stage_init(unsigned long long*) {}
+__device__ __forceinline__ void wigb_stage_copy(float* dst, const float* src, unsigned bytes, unsigned long long*) {
+  memcpy(dst, src, bytes);
+}
+__device__ __forceinline__ void wigb_stage_wait(unsigned long long*, unsigned, unsigned*) {}
+#endif
+
+// WIGB_XSTAGE 1: the staged x-pass above; 0: each lane loads its rows from
+// global memory directly (no staging buffer: less shared memory a CTA, and
+// the loads are in flight only while the CTA waits on them).
+#ifndef WIGB_XSTAGE
+#define WIGB_XSTAGE 1
+#endif
+
+#if WIGB_XSTAGE
+#define WIGB_X_CASE(N) case N: wig::batch_x_item_t<wig::XC, N>(A, sIn[buf], sI[buf], sRow[buf], stage, after); break;
+
+// Shared memory: the exchange regions (wigb_xexch_max() float2), then the
+// staging buffer (wigb_xstage_max() floats).
+extern "C" __global__ void __launch_bounds__(WIGB_NT, WIGB_XMINB)
+wigb_xpass(wig::BArgs A, int n_items) {
+  extern __shared__ float2 smb[];
+  float* stage = reinterpret_cast<float*>(smb + wigb_xexch_max());
+  __shared__ wig::BInst sI[2];
+  __shared__ int sIn[2], sRow[2];
+  __shared__ __align__(8) unsigned long long bar;
+  int item = wig::next_item(&A.tickets[0], n_items);
+  int buf = 0;
+  unsigned phase = 0;
+  // the first item's rows
+  if (threadIdx.x == 0) {
+    wigb_stage_init(&bar);
+    if (item < n_items) {
+      const int2 it = A.xitems[item];
+      sI[0] = A.inst[it.x];
+      sIn[0] = it.x;
+      sRow[0] = it.y;
+      wigb_stage_copy(stage, A.W + sI[0].off + (size_t)it.y * sI[0].n_x,
+                      (unsigned)(wig::bx_stage(sI[0].n_x, WIGB_WARPS) * sizeof(float)), &bar);
+    }
+  }
+  __syncthreads();
+  while (item < n_items) {
+    wigb_stage_wait(&bar, phase, A.status);
+    int next = n_items;
+    // every lane holds its rows: draw the next item and start its rows' copy
+    auto after = [&]() {
+      __syncthreads();
+      next = wig::next_item(&A.tickets[0], n_items);
+      if (threadIdx.x == 0 && next < n_items) {
+        const int2 it = A.xitems[next];
+        sI[buf ^ 1] = A.inst[it.x];
+        sIn[buf ^ 1] = it.x;
+        sRow[buf ^ 1] = it.y;
+        wigb_stage_copy(stage, A.W + sI[buf ^ 1].off + (size_t)it.y * sI[buf ^ 1].n_x,
+                        (unsigned)(wig::bx_stage(sI[buf ^ 1].n_x, WIGB_WARPS) * sizeof(float)), &bar);
+      }
+    };
+    switch (sI[buf].n_x) {
+      WIGB_CASES(WIGB_X_CASE)
+      default: after(); break;
+    }
+    __syncthreads();   // the item's exchange reads are done; sI[buf ^ 1] is visible
+    item = next;
+    buf ^= 1;
+    phase ^= 1u;
+  }
+}
+#else
+#define WIGB_X_CASE(N)                                                                              \
+  case N:                                                                                           \
+    wig::batch_x_item_t<wig::XC, N>(A, it.x, sI, it.y, A.W + sI.off + (size_t)it.y * N, [] {}); \
+    break;
+
+// Shared memory: the exchange regions (wigb_xexch_max() float2).
 extern "C" __global__ void __launch_bounds__(WIGB_NT, WIGB_XMINB)
 wigb_xpass(wig::BArgs A, int n_items) {
   __shared__ wig::BInst sI;
@@ -51,6 +170,7 @@ wigb_xpass(wig::BArgs A, int n_items) {
     __syncthreads();
   }
 }
+#endif
 
 extern "C" __global__ void __launch_bounds__(WIGB_NT, WIGB_PMINB)
 wigb_ppass(wig::BArgs A, int n_items, int sample) {

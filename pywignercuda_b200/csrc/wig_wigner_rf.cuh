@@ -166,7 +166,7 @@ __device__ __forceinline__ void ppass_rf_body(const WigArgs& a, const Phys& ph, 
   extern __shared__ double2 sm[];
   __shared__ double red[NT / 32][NACC];
   __shared__ __align__(8) unsigned long long tbar;
-  double2* A = reinterpret_cast<double2*>((reinterpret_cast<uintptr_t>(sm) + 1023) & ~(uintptr_t)1023);
+  double2* A = reinterpret_cast<double2*>((reinterpret_cast<unsigned long long>(sm) + 1023ull) & ~1023ull);
   double2* B = A + C * NP;
   const int col0 = blockIdx.x * C;
 #ifdef WIG_TMA

@@ -125,16 +125,15 @@ int main(int argc, char** argv) {
   A.inst = inst.data(); A.xitems = xi.data(); A.pitems = pi.data();
   A.W = W.data(); A.tw = tw.data(); A.tw64 = tw64.data(); A.ft = ft.data(); A.fd = fd.data();
   A.partials = partials.data();
-  A.counters = counters.data(); A.tickets = tickets.data(); A.scale = scale.data();
+  unsigned status = 0;
+  A.counters = counters.data(); A.tickets = tickets.data(); A.scale = scale.data(); A.status = &status;
   A.obs = obs.data(); A.obs_stride = (int)(n_prop + 1);
   const int nxi = (int)xi.size(), npi = (int)pi.size();
 
   // dynamic shared memory of the passes (wigb_compile: the largest size class)
-  size_t smx = 0, smp = 0;
-  for (int n : cls) {
-    smx = std::max(smx, (size_t)wig::bx_smem(n, WIGB_WARPS) * sizeof(float2));
-    smp = std::max(smp, (size_t)wig::bp_smem(n, WIGB_WARPS) * sizeof(float2));
-  }
+  size_t smx = (size_t)wigb_xexch_max() * sizeof(float2) + (WIGB_XSTAGE ? (size_t)wigb_xstage_max() * sizeof(float) : 0),
+         smp = 0;
+  for (int n : cls) smp = std::max(smp, (size_t)wig::bp_smem(n, WIGB_WARPS) * sizeof(float2));
   // wigb_launch_run: reduce (normalisation, sample 0), then per step x-pass and p-pass, then scale
   emu_launch(grid, WIGB_NT, [&] { wigb_reduce(A, npi, 1, 0); });
   for (long n = 0; n < n_prop; ++n) {

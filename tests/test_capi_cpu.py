@@ -64,6 +64,25 @@ def test_wigner_jit_compiles(n):
     assert int(props.split(' bytes spill stores')[0].split()[-1]) <= 16, props
 
 
+@pytest.mark.parametrize('tma', ['1', '0'])
+@pytest.mark.parametrize('n', [64, 1024])
+def test_register_fft_passes_compile(monkeypatch, n, tma):
+    """The opt-in register-FFT passes (WIG_RF) compile under NVRTC, with the p-pass
+    tile loaded by TMA or by the threads.  At 1024 points the p-pass holds 32 FP64 complex
+    values a lane for each of its column pairs and spills a few hundred bytes (one reason
+    the path stays opt-in); below that it spills at most a few bytes."""
+    monkeypatch.setenv('WIG_RF', '1')
+    monkeypatch.setenv('WIG_TMA', tma)
+    rc, log = jit(wig_desc(n, n))
+    assert rc == 0, log
+    assert 'wig_xpass_rf' in log and 'wig_ppass_rf' in log
+    lines = log.splitlines()
+    for k in ('wig_xpass_rf', 'wig_ppass_rf'):
+        at = [i for i, l in enumerate(lines) if "Compiling entry function '%s'" % k in l]
+        props = ' '.join(lines[at[0] + 1:at[0] + 3])
+        assert int(props.split(' bytes spill stores')[0].split()[-1]) <= (64 if n < 1024 else 512), (k, props)
+
+
 def test_dirac_tiling_override_validated(monkeypatch):
     """WIG_DIRAC_TILING replaces the planner's tiles; a tile that does not divide
     the grid is refused on the host, before any compile."""

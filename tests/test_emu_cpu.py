@@ -262,16 +262,18 @@ BSHAPES = ((64, 128, 10., 8.), (128, 64, 8., 10.))
 BEXTRA = {1: dict(ff=1, f_eps=0.5, d_lambda=0.01, v1=0.3, v0=0.2), 4: dict(v1=-0.2)}
 
 
-@pytest.mark.parametrize('warps,grid,prec', [(4, 3, 0), (2, 5, 0), (4, 3, 1), (2, 5, 1)])
-def test_batch_device_code_matches_oracle(staged, warps, grid, prec):
+@pytest.mark.parametrize('warps,grid,prec,xstage', [(4, 3, 0, 0), (2, 5, 0, 1), (4, 3, 1, 1), (2, 5, 1, 0)])
+def test_batch_device_code_matches_oracle(staged, warps, grid, prec, xstage):
     """The real-storage passes (two rows / columns per complex transform, the
     Nyquist split), in FP32 (prec 0) and with the FP64 kinetic and Moyal pairs
     and their in-place mirror split (prec 1; the 64-point grids with the FP64
     dissipator, the 128-point ones with the FP32 one), the persistent work lists
     and the last-CTA normalisation, against the FP64 oracle, 2 steps (each
-    emulated step costs seconds of barrier traffic)."""
+    emulated step costs seconds of barrier traffic).  xstage 1: the x-pass rows arrive
+    through the shared-memory staging buffer, one item ahead."""
     exe = build(staged, 'batch_emu.cpp', {'WIGB_WARPS': warps, 'WIGB_XMINB': 1, 'WIGB_PMINB': 1, 'WIGB_PREC': prec,
-                                          'WIGB_DISS64_MAXN': 64, 'WIGB_CASES(F)': 'F(64) F(128)'})
+                                          'WIGB_XSTAGE': xstage, 'WIGB_DISS64_MAXN': 64,
+                                          'WIGB_CASES(F)': 'F(64) F(128)'})
     cases = random_batch(list(BSIZES) + [s[0] for s in BSHAPES], seed=11)
     cases[2]['gamma'] = 0.
     for c, (nx, npp, xa, pa) in zip(cases[len(BSIZES):], BSHAPES):

@@ -20,8 +20,8 @@ import test_emu_cpu as E
 from test_emu_cpu import staged  # noqa: F401  (the module-scoped staging fixture)
 
 CASES = [
-    ('test_batch_device_code_matches_oracle', dict(warps=4, grid=3, prec=0)),
-    ('test_batch_device_code_matches_oracle', dict(warps=2, grid=5, prec=1)),
+    ('test_batch_device_code_matches_oracle', dict(warps=4, grid=3, prec=0, xstage=0)),
+    ('test_batch_device_code_matches_oracle', dict(warps=2, grid=5, prec=1, xstage=1)),
     ('test_adjoint_device_code_matches_twin', dict(prec=0, gamma=0.)),
     ('test_adjoint_device_code_matches_twin', dict(prec=1, gamma=0.1)),
     ('test_wigner2d_device_code_matches_oracle', dict(xrows=32, xnt=256, pc=64, pnt=256, odm=0, kvn=0)),
