@@ -572,8 +572,8 @@ def run_batch(args, world, rank, local):
     val = validation(cases, states, dev) if rank == 0 and not args.profile_only else None
     head_p = precs[0]
     if val is not None:
-        ok = all(v['norm_max_abs'] <= 1e-6 and v['energy_rel_max'] <= 1e-6 for v in val['mixed'].values()
-                 if isinstance(v, dict))
+        ok = all(v['norm_max_abs'] <= 1e-6 and v['energy_rel_max'] <= 1e-6 and v['energy_rel_final'] <= 1e-6
+                 for v in val['mixed'].values() if isinstance(v, dict))
         head_p = 'mixed' if ok else 'f32'
         if head_p not in legs:
             head_p = precs[0]

@@ -272,7 +272,11 @@ int dirac3_jit_check(const dirac3_desc* desc, char* log, int64_t log_cap);
  * arithmetic, one per batch:
  *   WIGB_PREC_F32    FP32 transforms and factors throughout;
  *   WIGB_PREC_MIXED  the kinetic and Moyal transform pairs and their factors
- *                    in FP64, the three dissipator pairs in FP32.
+ *                    in FP64 (and the dissipator pairs, up to 256-point
+ *                    columns; FP32 above), each FP64 result rounded to the
+ *                    FP32 state stochastically: a function of the inputs and
+ *                    the step index t_index0 + n, so a run is reproducible
+ *                    (pass t_index0 on a continued run for fresh rounding).
  * Both form the phase arguments in FP64 and reduce them to one turn, and keep
  * the observables in FP64 (per-column moments, compensated per-instance sums).
  * Constants are exact (no '%f' rounding).  No counterpart in the reference,

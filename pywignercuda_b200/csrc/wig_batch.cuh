@@ -82,6 +82,7 @@ struct BArgs {
   unsigned* status;      // [1] set to 1 by a bounded wait that gave up (read and cleared by the host)
   double* obs;           // [n_inst][obs_stride][NOBS]
   int obs_stride;
+  unsigned step;         // the launch's step index (t_index0 + n): the stochastic-rounding key
 };
 
 // Shared memory of one item: the x-pass exchange regions and row staging buffer
@@ -132,6 +133,55 @@ __device__ __forceinline__ double2 turn_factor64(double t, double r) {
   sincospi(2. * f, &sn, &cs);
   return make_double2(r * cs, -r * sn);
 }
+
+// ---------------------------------------------------------- stochastic rounding
+// The mixed form (WIGB_PREC 1) computes each pass in FP64 and stores W in FP32.
+// Rounding to nearest there loses, at every point whose change over one pass is
+// below half an FP32 ulp (the slow rows and columns near the distribution's
+// peak, the late approach to a damped equilibrium), that change on every step,
+// so the slow part of the dynamics stalls and the energy error grows linearly
+// (stagnation: M. Croci and M. B. Giles, "Effects of round-to-nearest and
+// stochastic rounding in the numerical solution of the heat equation in low
+// precision", IMA J. Numer. Anal. 43 (2023)).  Stochastic rounding -- up with
+// probability equal to the remainder's fraction of the ulp -- keeps every change
+// in expectation.  Done in the integer domain: 29 random bits (the bits a double
+// carries below a float's mantissa) are added to the double's magnitude and the
+// result truncated to FP32.  Exact for |v| in the FP32 normal range; below it
+// (|v| < 2^-126, nothing there weighs in an observable) the rounding is biased
+// toward zero; NaN and infinities stay non-finite.
+//
+// The random words: each lane seeds a stream by hashing (step, pass, the index
+// of its first element), then takes one linear congruential step per element
+// (the top 29 bits of the 32-bit state are used).  A run is a function of its
+// inputs and t_index0: graph and non-graph runs agree bit for bit.
+// sr_mix: the "lowbias32" 32-bit integer hash (C. Wellons, hash-prospector).
+__host__ __device__ __forceinline__ unsigned sr_mix(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+// the key of one pass of one step (pass 0: x-pass, 1: p-pass)
+__device__ __forceinline__ unsigned sr_key(unsigned step, unsigned pass) { return sr_mix(2u * step + pass + 0x9e3779b9u); }
+// the random word of element e (index into the packed state): a stream's seed
+__device__ __forceinline__ unsigned sr_word(unsigned key, long long e) {
+  return sr_mix((unsigned)e ^ key ^ (0x85ebca6bu * (unsigned)(e >> 32)));
+}
+// a lane's stream of random words (LCG constants of Numerical Recipes, 2nd ed., 7.1)
+struct SrStream {
+  unsigned s;
+  __device__ __forceinline__ unsigned next() {
+    s = s * 1664525u + 1013904223u;
+    return s;
+  }
+};
+// v rounded to FP32: stochastically for double, unchanged for float
+__device__ __forceinline__ float store_round(double v, unsigned u) {
+  return __double2float_rz(__longlong_as_double(__double_as_longlong(v) + (long long)(u >> 3)));
+}
+__device__ __forceinline__ float store_round(float v, unsigned) { return v; }
 
 struct Kahan {
   double s = 0., c = 0.;
@@ -337,10 +387,11 @@ __device__ __forceinline__ void batch_x_item_t(const BArgs& A, int inst, const B
   F::invx(v, x, ti, g);
   float* Wa = A.W + I.off + (size_t)ra * N;
   float* Wb = Wa + N;
+  SrStream rs{sr_word(sr_key(A.step, 0), (long long)I.off + (long long)ra * N + g)};
 #pragma unroll
   for (int m = 0; m < E; ++m) {
-    Wa[g + G * m] = (float)v[m].x;
-    Wb[g + G * m] = (float)v[m].y;
+    Wa[g + G * m] = store_round(v[m].x, rs.next());
+    Wb[g + G * m] = store_round(v[m].y, rs.next());
   }
 }
 
@@ -481,8 +532,13 @@ __device__ __forceinline__ void batch_p_item(const BArgs& A, int inst, const BIn
         }
       }
     }
+    // rounded to FP32 stochastically (the lane's stream: seeded at its first point of column c1)
+    SrStream rs{sr_word(sr_key(A.step, 1), (long long)I.off + (long long)g * nx + col0 + c1)};
 #pragma unroll
-    for (int m = 0; m < E; ++m) w[m] = make_float2((float)z[m].x, (float)z[m].y);
+    for (int m = 0; m < E; ++m) {
+      const float a = store_round(z[m].x, rs.next());
+      w[m] = make_float2(a, store_round(z[m].y, rs.next()));
+    }
   }
   const int n_it_run = N <= WIGB_DISS64_MAXN ? 1 : n_it;
 #else

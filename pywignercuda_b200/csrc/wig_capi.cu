@@ -1483,14 +1483,14 @@ struct BVariant {
   int smem_x = 0, smem_p = 0, occ_x = 1, occ_p = 1;
 };
 
-// Whether the x-pass stages its rows in shared memory (WIGB_XSTAGE): on for the
-// mixed form, whose FP64 transforms leave the loads' latency exposed; off for the
-// FP32 form, which hides it with more resident warps.  Tuning override (read per
-// compile): WIG_BATCH_XSTAGE=0|1.
-int batch_xstage(int prec) {
+// Whether the x-pass stages its rows in shared memory (WIGB_XSTAGE).  On by
+// default: on the 64-instance mixed-grid batch (B200) it took the x-pass from 272
+// to 240 us in the mixed form and from 182 to 169 us in FP32.  Tuning override
+// (read per compile): WIG_BATCH_XSTAGE=0|1.
+int batch_xstage(int) {
   const char* e = getenv("WIG_BATCH_XSTAGE");
   if (e && *e) return atoi(e) ? 1 : 0;
-  return prec == WIGB_PREC_MIXED ? 1 : 0;
+  return 1;
 }
 
 // the x-pass's exchange regions and row staging buffer (wigb_xpass: the largest size class's each)
@@ -1793,6 +1793,7 @@ static int wigb_launch_run(wigb_handle* h, float* W, int64_t t_index0, int64_t n
   for (int64_t n = 0; n < n_prop; ++n) {
     if (flush) WIG_CUDA(cudaMemsetAsync(h->flush, (int)(n & 0x7f), h->flush_bytes, st));
     if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n], st));
+    a.step = (unsigned)(t_index0 + n);   // the launch copies its parameters
     void* xargs[] = {&a, &nxi};
     if (int rc = launch(v.fx, h->grid_x, nt, v.smem_x, st, xargs)) return rc;
     if (prof) WIG_CUDA(cudaEventRecord(h->ev[3 * n + 1], st));

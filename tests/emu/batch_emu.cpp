@@ -137,6 +137,7 @@ int main(int argc, char** argv) {
   // wigb_launch_run: reduce (normalisation, sample 0), then per step x-pass and p-pass, then scale
   emu_launch(grid, WIGB_NT, [&] { wigb_reduce(A, npi, 1, 0); });
   for (long n = 0; n < n_prop; ++n) {
+    A.step = (unsigned)n;
     emu_launch(grid, WIGB_NT, [&] { wigb_xpass(A, nxi); }, smx);
     const int sample = (int)(n + 1);
     emu_launch(grid, WIGB_NT, [&] { wigb_ppass(A, npi, sample); }, smp);

@@ -15,6 +15,7 @@
 #include <math.h>
 
 #include <atomic>
+#include <cmath>
 #include <cstdint>
 #include <barrier>
 #include <cstdio>
@@ -89,6 +90,23 @@ inline void sincospi(double x, double* s, double* c) {
   const long double a = 3.141592653589793238462643383279502884L * (long double)x;
   *s = (double)::sinl(a);
   *c = (double)::cosl(a);
+}
+
+// bit casts, and the double -> float conversion rounding toward zero
+inline long long __double_as_longlong(double v) {
+  long long b;
+  std::memcpy(&b, &v, sizeof b);
+  return b;
+}
+inline double __longlong_as_double(long long b) {
+  double v;
+  std::memcpy(&v, &b, sizeof v);
+  return v;
+}
+inline float __double2float_rz(double v) {
+  float f = (float)v;
+  if (std::isfinite(f) && std::fabs((double)f) > std::fabs(v)) f = std::nextafterf(f, 0.f);
+  return f;
 }
 
 // (grid_x, grid_y) x block threads; a block's threads run concurrently, blocks in turn.

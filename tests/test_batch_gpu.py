@@ -101,7 +101,10 @@ def test_1024_instances_of_the_batch_against_oracle(precision):
 
 def test_mixed_batch_2000_steps_within_1e6_of_complex128():
     """The whole 64-instance batch for its 2000 steps in the mixed form against the
-    complex128 drop-in path (pinned to the oracle): norm and energy within 1e-6."""
+    complex128 drop-in path (pinned to the oracle): norm within 1e-6, energy within
+    1e-6 of the trajectory's scale at every sample and of |E| at the last one.
+    The last is what stochastic rounding of the FP32 stores buys: with rounding to
+    nearest, the damped 128^2 instance 27 (E decaying to 0.04) ended 4.2e-6 off."""
     cases = config3_cases()
     steps = 2000
     _, obs, _ = run_batch(cases, steps, precision='mixed')
@@ -109,6 +112,8 @@ def test_mixed_batch_2000_steps_within_1e6_of_complex128():
     assert np.max(np.abs(obs[:, :, 0] - ref[:, :, 0])) < 1e-6
     er = energy_rel(obs, ref)
     assert np.max(er) < 1e-6, (np.argmax(er), np.max(er))
+    ef = np.abs(obs[:, -1, 9] - ref[:, -1, 9]) / np.abs(ref[:, -1, 9])
+    assert np.max(ef) < 1e-6, (np.argmax(ef), np.max(ef))
 
 
 def test_graph_and_tile_shapes_agree():

@@ -40,7 +40,8 @@ def stage(dst):
         src = EXTERN_SHARED.sub(lambda m: '%s* %s = reinterpret_cast<%s*>(emu_smem);'
                                 % (m.group(1), m.group(2), m.group(1)), src)
         open(os.path.join(dst, h), 'w').write(src)
-    for f in ('shim.h', 'dirac2d_emu.cpp', 'wigner2d_emu.cpp', 'dirac3d_emu.cpp', 'batch_emu.cpp', 'adjoint_emu.cpp'):
+    for f in ('shim.h', 'dirac2d_emu.cpp', 'wigner2d_emu.cpp', 'dirac3d_emu.cpp', 'batch_emu.cpp', 'adjoint_emu.cpp',
+              'round_emu.cpp'):
         shutil.copy(os.path.join(EMU, f), dst)
 
 
@@ -252,6 +253,55 @@ def _dirac3d_run(staged, dims, rows, yc, zc, xr, yr, zr, cap):
     assert rel_l2(got, ref) < 1e-12
     scale = np.maximum(np.abs(ref_obs).max(axis=0), 1e-3)
     assert np.all(np.abs(obs - ref_obs) / scale < 1e-10), (obs - ref_obs) / scale
+
+
+@pytest.mark.parametrize('mode', ['seeds', 'stream'])
+def test_stochastic_rounding_is_unbiased(staged, mode):
+    """The mixed form's FP64 -> FP32 store (store_round over a lane's SrStream
+    seeded by sr_word / sr_key): each result is one of the two FP32 values
+    bracketing v (v itself when it is one), rounds away from zero with
+    probability equal to v's fraction of the ulp -- so the mean over steps
+    converges to v -- and non-finite values stay non-finite.  The words are the
+    first word of each step's stream ('seeds': what one point sees over steps) or
+    the consecutive words of one stream ('stream': what one lane's points see in
+    one step).  Also: one value stored at many lanes' first points in one step
+    rounds up at the same rate (the seeds are uncorrelated across elements)."""
+    exe = build(staged, 'round_emu.cpp', {'WIGB_WARPS': 4, 'WIGB_PREC': 1, 'WIGB_CASES(F)': 'F(64)'})
+    rng = np.random.default_rng(3)
+    mags = np.exp(rng.uniform(np.log(1e-30), np.log(1e3), 200)) * rng.choice([-1., 1.], 200)
+    f32 = rng.standard_normal(20).astype(np.float32).astype(np.float64)          # already FP32
+    lo = np.float32(0.7).astype(np.float64)
+    ulp = np.nextafter(np.float32(0.7), np.float32(1.)).astype(np.float64) - lo
+    fracs = lo + ulp * np.array([0.5, 0.25, 0.75, 0.01, 0.99])                   # known fractions
+    vals = np.concatenate([mags, f32, fracs, -fracs, [0., -0., np.nan, np.inf, -np.inf]])
+    steps = 4000
+    fin, fout = os.path.join(staged, 'sr_in.bin'), os.path.join(staged, 'sr_out.bin')
+    vals.tofile(fin)
+    r = subprocess.run([exe, fin, fout, str(steps), '123456789', mode], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = np.fromfile(fout, dtype=np.float32).reshape(len(vals), steps).astype(np.float64)
+    for v, o in zip(vals, out):
+        if not np.isfinite(v):
+            assert not np.isfinite(o).any(), v
+            continue
+        a = np.float32(v)                                   # nearest
+        a = a.astype(np.float64)
+        if a == v:
+            assert np.all(o == v), v
+            continue
+        b = np.nextafter(np.float32(v), np.float32(np.inf if v > a else -np.inf)).astype(np.float64)
+        lo_v, hi_v = (a, b) if abs(a) < abs(b) else (b, a)  # toward / away from zero
+        assert np.all((o == lo_v) | (o == hi_v)), v
+        p = (abs(v) - abs(lo_v)) / abs(hi_v - lo_v)
+        up = np.mean(o == hi_v)
+        assert abs(up - p) <= 5. * np.sqrt(max(p * (1. - p), 1e-3) / steps) + 2. ** -29, (v, p, up)
+    # one step, one value at many elements
+    vals = np.full(20000, lo + 0.5 * ulp)
+    vals.tofile(fin)
+    r = subprocess.run([exe, fin, fout, '1', '0', 'seeds'], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = np.fromfile(fout, dtype=np.float32).astype(np.float64)
+    assert abs(np.mean(out > lo) - 0.5) < 5. * np.sqrt(0.25 / len(out))
 
 
 # instances of the batched FP32 form: mixed grids, two of them non-square with unequal amplitudes,

@@ -32,6 +32,19 @@ def test_partition_covers_every_instance_once(world):
         assert imbalance(inst, parts) < 1.10
 
 
+def test_cost_uses_the_measured_table():
+    from pywignercuda_b200.shard import MEASURED_NS
+    for d in _batch():
+        key = '%d%s' % (d['n_x'], 'd' if d['gamma'] else '')
+        assert key in MEASURED_NS
+        assert instance_cost(d) == pytest.approx(d['n_x'] * d['n_p'] * MEASURED_NS[key])
+    # a size class outside the table: the transform-count model, damped four times the undamped
+    und, dmp = dict(n_x=2048, n_p=64, gamma=0.), dict(n_x=2048, n_p=64, gamma=0.1)
+    assert instance_cost(dmp) == pytest.approx(4. * instance_cost(und))
+    # a caller's own table takes precedence
+    assert instance_cost(dict(n_x=128, n_p=128, gamma=0.), {'128': 2.}) == pytest.approx(2. * 128 * 128)
+
+
 def test_partition_is_deterministic():
     inst = _batch()
     assert partition(inst, 4) == partition(inst, 4)
