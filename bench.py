@@ -57,10 +57,12 @@ REPLICAS = 16
 PASS_BYTES = NX * NP * 16 * 2      # one fused pass reads and writes the c128 grid once
 # dram__bytes_read.sum + dram__bytes_write.sum per p-pass launch, from the ncu captures
 # summarised in profiles/wig_passes_c128_1024.md (one 1024^2 replica, whose state fits in
-# L2: the capture shows one read of it) and profiles/wigb_passes_batch64.md (the 64-instance
-# batch, 187 MB of state)
-NCU_TRAFFIC_PPASS = 16.94e6 + 0.04e6
-NCU_TRAFFIC_BATCH = None
+# L2: the capture shows one read of it, the write-back comes after the kernel) and
+# profiles/wigb_passes_batch128.md (the mixed p-pass on the 128-instance batch, 46.19 M points,
+# 187.18 MB read + 132.93 MB written; scaled here by points to the 64-instance batch's
+# 23.36 M, since each pass reads and writes every point once)
+NCU_TRAFFIC_PPASS = 16.94e6 + 0.005e6
+NCU_TRAFFIC_BATCH = (187.18e6 + 132.93e6) * 23363584 / 46186496
 
 
 def peaks():
@@ -280,6 +282,26 @@ def cpu_batch_sample(cases, max_seconds=15.0):
         if el >= max_seconds and steps >= 2:
             break
     return pts / el, steps, el, WORKERS, '%d rounds of one step of a 128/256/512/1024 instance' % steps
+
+
+def cpu_notebook_sample(steps=20, repeats=3, warmup=10):
+    """The reference notebook's own CPU propagator (real W, Strang V/2-K-V/2 with
+    real FFTs; ``CPU_GPU_Wigner2D.ipynb`` cells 6-10, pyFFTW restated by scipy.fft
+    on all cores) in its own configuration, 512^2: warm-up, then the median of
+    ``repeats`` timed runs of ``steps`` steps, as grid-pt-steps/s."""
+    from oracle.strang_notebook import StrangNotebook
+    from oracle.common import WORKERS
+    nb = StrangNotebook()
+    W = nb.run(nb.initial_state(), warmup)
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        W = nb.run(W, steps)
+        times.append(time.perf_counter() - t0)
+    t = sorted(times)[len(times) // 2]
+    return {'value': nb.n_x * nb.n_p * steps / t, 'unit': UNIT, 'cores': WORKERS, 'kind': 'port',
+            'sample': 'the notebook\'s CPU Strang path (real FFTs), 512^2, median of %d x %d steps after %d '
+                      'warm-up' % (repeats, steps, warmup)}
 
 
 def run_reference(args, world, rank):
@@ -657,7 +679,8 @@ def run_batch(args, world, rank, local):
     if rank == 0 and args.cpu_baseline:
         rate, n, el, cores, what = cpu_batch_sample(cases, max_seconds=15.0)
         line['cpu_baseline'] = {'value': rate, 'unit': UNIT, 'cores': cores, 'kind': 'port',
-                                'sample': what + ' (%.1f s)' % el}
+                                'sample': what + ' (%.1f s)' % el,
+                                'notebook_strang_512': cpu_notebook_sample()}
     if rank == 0:
         print(json.dumps(line))
 

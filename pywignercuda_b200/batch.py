@@ -8,8 +8,11 @@ spans all instances, the whole run captured once into a CUDA graph, the tile
 shape picked by ``autotune``.  The state is the real Wigner function in FP32
 (one float per grid point).  ``precision='f32'`` runs every transform and
 factor in FP32; ``'mixed'`` runs the kinetic and Moyal transform pairs and
-their factors in FP64 and the three dissipator pairs in FP32.  Phase
-arguments are formed and range-reduced in FP64; observables are FP64 (Kahan).
+their factors in FP64 (the three dissipator pairs too up to 256-point
+columns, in FP32 above) and rounds each FP64 result to the FP32 state
+stochastically, so changes smaller than half an FP32 ulp are kept in
+expectation instead of being lost every step.  Phase arguments are formed and
+range-reduced in FP64; observables are FP64 (Kahan).
 The step is the reference's Lie split (``GPU_Wigner2D_FFT.py:1884-1913``)
 with exact constants.
 """
@@ -98,6 +101,10 @@ class WignerBatch:
             profile=False, flush_l2=False):
         """Advance the packed state W in place; returns obs[count, n_prop+1, 11]
         (sample k before propagation k, the last after the final one).
+        t_index0: the index of the first step.  The mixed form rounds its FP64
+        results to the FP32 state stochastically, with random words drawn from
+        (step index, pass, point): a run is reproducible, and a continued run
+        should pass its first step's index to draw fresh words.
         profile=True (with graph=False) times every x-pass and p-pass launch
         (``profile()``); flush_l2=True then also writes a buffer twice the L2
         size before every step, outside the timed launches."""

@@ -151,7 +151,9 @@ class Propagator_Base:
     def Wigner_FromWavefunction(self, psi):
         """Wigner function of a wave-function callable psi(x), by the same discrete
         transform as ``Wigner_Half_HarmonicOscillator`` (psi(x - hbar theta/2)
-        psi*(x + hbar theta/2), IFFT over theta), shifted layout, normalised."""
+        psi*(x + hbar theta/2), IFFT over theta), shifted layout, normalised.
+        This package's helper: the reference has no counterpart (its classes take
+        W_init as an array)."""
         X_minus = self.X_range[np.newaxis, :] - 0.5 * self.hBar * self.Theta_range[:, np.newaxis]
         X_plus = self.X_range[np.newaxis, :] + 0.5 * self.hBar * self.Theta_range[:, np.newaxis]
         W = psi(X_minus) * np.conj(psi(X_plus))

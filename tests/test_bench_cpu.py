@@ -40,3 +40,11 @@ def test_reference_arm_other_ranks_exit_quietly():
     p = _run({'WORLD_SIZE': '2', 'RANK': '1', 'LOCAL_RANK': '1'}, timeout=120)
     assert p.returncode == 0, p.stderr[-2000:]
     assert not [ln for ln in p.stdout.splitlines() if ln.startswith('{')]
+
+
+def test_notebook_cpu_baseline_sample():
+    """The second CPU baseline: the notebook's own real-FFT Strang propagator at its
+    512^2 configuration (a short sample here)."""
+    import bench
+    r = bench.cpu_notebook_sample(steps=2, repeats=1, warmup=1)
+    assert r['value'] > 0 and r['unit'] == bench.UNIT and r['kind'] == 'port' and r['cores'] >= 1

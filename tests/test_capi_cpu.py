@@ -7,6 +7,7 @@ import re
 
 import pytest
 
+from conftest import full_only
 from pywignercuda_b200 import _lib
 from pywignercuda_b200._lib import WigDesc, DiracDesc
 
@@ -64,8 +65,7 @@ def test_wigner_jit_compiles(n):
     assert int(props.split(' bytes spill stores')[0].split()[-1]) <= 16, props
 
 
-@pytest.mark.parametrize('tma', ['1', '0'])
-@pytest.mark.parametrize('n', [64, 1024])
+@pytest.mark.parametrize('n,tma', [(1024, '1'), (64, '0'), full_only(1024, '0'), full_only(64, '1')])
 def test_register_fft_passes_compile(monkeypatch, n, tma):
     """The opt-in register-FFT passes (WIG_RF) compile under NVRTC, with the p-pass
     tile loaded by TMA or by the threads.  At 1024 points the p-pass holds 32 FP64 complex
@@ -207,8 +207,8 @@ def test_python_classes_fail_loudly_without_gpu():
         Inst()
 
 
-@pytest.mark.parametrize('warps', [8, 4, 2])
-@pytest.mark.parametrize('precision', [0, 1])
+@pytest.mark.parametrize('precision,warps', [(0, 4), (1, 2), full_only(0, 8), full_only(0, 2), full_only(1, 8),
+                                             full_only(1, 4)])
 def test_batch_jit_spills_bounded(warps, precision):
     """All size classes in one kernel.  The FP32 passes at 168 registers (3 / 6 CTAs of
     4 / 2 warps per SM) spill ~20 bytes in the 1024-point p-pass; the mixed form's FP64

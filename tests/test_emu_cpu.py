@@ -15,6 +15,7 @@ import subprocess
 import numpy as np
 import pytest
 
+from conftest import full_only
 from oracle.common import rel_l2
 from oracle.dirac2d import DiracOracle, DiracParams, spinor_particle_spin_up
 from oracle.dirac3d import Dirac3DOracle, Dirac3DParams, spinor_particle_spin_up_3d
@@ -74,7 +75,7 @@ def staged(tmp_path_factory):
 
 # (rows, row threads, columns, column threads) per CTA: the planner's rule at 32 x 16 (one CTA per
 # pass), several CTAs per pass, and one row / one column per CTA as at 512^2
-@pytest.mark.parametrize('rows,rnt,cc,cnt', [(16, 256, 32, 256), (4, 64, 8, 64), (1, 32, 1, 32)])
+@pytest.mark.parametrize('rows,rnt,cc,cnt', [(16, 256, 32, 256), full_only(4, 64, 8, 64), (1, 32, 1, 32)])
 def test_dirac2d_device_code_matches_oracle(staged, rows, rnt, cc, cnt):
     exe = build(staged, 'dirac2d_emu.cpp', dict(DIR_NX=NX, DIR_NY=NY, DIR_ROWS=rows, DIR_RNT=rnt, DIR_RMB=1,
                                                 DIR_C=cc, DIR_CNT=cnt, DIR_CMB=1, DIR_SNT=256))
@@ -141,7 +142,8 @@ def test_wigner2d_device_code_matches_oracle(staged, xrows, xnt, pc, pnt, odm, k
 
 # The register-FFT x- and p-pass of Lie plans (wig_wigner_rf.cuh) on a 128 x 64 grid: Caldeira-Leggett,
 # undamped, the Fokker-Planck (KvN) factor; one and several warps per CTA
-@pytest.mark.parametrize('xw,pw,kvn,gamma', [(4, 2, 0, WGAMMA), (1, 1, 0, WGAMMA), (2, 2, 0, 0.), (4, 1, 1, WGAMMA)])
+@pytest.mark.parametrize('xw,pw,kvn,gamma', [(4, 2, 0, WGAMMA), full_only(1, 1, 0, WGAMMA), full_only(2, 2, 0, 0.),
+                                              (4, 1, 1, WGAMMA)])
 def test_wigner2d_rf_device_code_matches_oracle(staged, xw, pw, kvn, gamma):
     nx, npp = 128, 64
     damp = int(gamma != 0.)
@@ -215,13 +217,13 @@ def d3_threads(n):
 
 # (rows, yc, zc, radix x / y / z, CTA cap): the planner's tiles at 32 x 16 x 16 (radix 16 on z),
 # small tiles with every pass grid-striding over 5 CTAs, and radix 16 on every axis over 3 CTAs
-@pytest.mark.parametrize('rows,yc,zc,xr,yr,zr,cap', [(16, 32, 32, 8, 8, 16, 2368), (2, 4, 2, 8, 8, 16, 5),
-                                                     (16, 32, 32, 16, 16, 16, 3)])
+@pytest.mark.parametrize('rows,yc,zc,xr,yr,zr,cap', [full_only(16, 32, 32, 8, 8, 16, 2368),
+                                                     full_only(2, 4, 2, 8, 8, 16, 5), (16, 32, 32, 16, 16, 16, 3)])
 def test_dirac3d_device_code_matches_oracle(staged, rows, yc, zc, xr, yr, zr, cap):
     _dirac3d_run(staged, D3, rows, yc, zc, xr, yr, zr, cap)
 
 
-@pytest.mark.parametrize('n', [16, 32])
+@pytest.mark.parametrize('n', [16, full_only(32)])
 def test_dirac3d_cubic_planner_tiles(staged, n):
     """Cubic grids with the planner's tiles (dirac3_plan: rows = 512 / n, yc = 2048 / n and
     zc = 1024 / n clamped to n, radix 16 on z): the shapes at which the z-pass's K mix read
@@ -312,7 +314,8 @@ BSHAPES = ((64, 128, 10., 8.), (128, 64, 8., 10.))
 BEXTRA = {1: dict(ff=1, f_eps=0.5, d_lambda=0.01, v1=0.3, v0=0.2), 4: dict(v1=-0.2)}
 
 
-@pytest.mark.parametrize('warps,grid,prec,xstage', [(4, 3, 0, 0), (2, 5, 0, 1), (4, 3, 1, 1), (2, 5, 1, 0)])
+@pytest.mark.parametrize('warps,grid,prec,xstage', [full_only(4, 3, 0, 0), (2, 5, 0, 1), (4, 3, 1, 1),
+                                                     full_only(2, 5, 1, 0)])
 def test_batch_device_code_matches_oracle(staged, warps, grid, prec, xstage):
     """The real-storage passes (two rows / columns per complex transform, the
     Nyquist split), in FP32 (prec 0) and with the FP64 kinetic and Moyal pairs

@@ -17,6 +17,7 @@ oracle / the twin as in test_emu_cpu.py."""
 import pytest
 
 import test_emu_cpu as E
+from conftest import FULL
 from test_emu_cpu import staged  # noqa: F401  (the module-scoped staging fixture)
 
 CASES = [
@@ -31,6 +32,10 @@ CASES = [
     ('test_dirac2d_device_code_matches_oracle', dict(rows=4, rnt=64, cc=8, cnt=64)),
     ('test_dirac3d_cubic_planner_tiles', dict(n=16)),
 ]
+# the default CPU suite: the race checker over the batched (mixed, staged x-pass), adjoint
+# (damped), complex128 Wigner (ODM) and Dirac2D passes, AddressSanitizer over the Dirac2D
+# passes; every pair with WIG_CPU_FULL=1 (run before a change to the kernels is committed)
+DEFAULT = {('thread', 1), ('thread', 3), ('thread', 5), ('thread', 8), ('address', 8)}
 
 
 def _ids(case):
@@ -42,9 +47,8 @@ def _ids(case):
 @pytest.mark.parametrize('sanitize', ['thread', 'address'])
 @pytest.mark.parametrize('case', CASES, ids=[_ids(c) for c in CASES])
 def test_device_code_under_sanitizer(staged, monkeypatch, sanitize, case):  # noqa: F811
-    if sanitize == 'address' and case[0] in ('test_bloch_device_code_matches_oracle',
-                                              'test_strang_gp_device_code_matches_oracle'):
-        pytest.skip('covered by the thread-sanitizer run (the CPU suite keeps to a few minutes)')
+    if (sanitize, CASES.index(case)) not in DEFAULT and not FULL:
+        pytest.skip('WIG_CPU_FULL=1 runs it (the default CPU suite keeps to a few minutes)')
     build = E.build
     monkeypatch.setattr(E, 'build', lambda dst, source, macros: build(dst, source, macros, sanitize=sanitize))
     name, kw = case
