@@ -275,3 +275,59 @@ def test_dirac3d_descriptor_validated():
     assert rc == 1 and 'expression' in log
     rc, log = jit(d3_desc(a0=b'unknown_name(x)'), 'dirac3_jit_check')
     assert rc != 0
+
+
+def _wigb(n_x=128, n_p=128, **kw):
+    d = _lib.WigbInstance()
+    d.n_x, d.n_p = n_x, n_p
+    d.x_amplitude = d.p_amplitude = 10.
+    d.hbar = d.mass = 1.
+    d.dt = 0.005
+    for k, v in kw.items():
+        setattr(d, k, v)
+    return d
+
+
+@pytest.mark.parametrize('bad,msg', [
+    (dict(count=0), 'empty batch'),
+    (dict(n_x=32), 'powers of two in [64, 1024]'),
+    (dict(n_p=2048), 'powers of two in [64, 1024]'),
+    (dict(n_x=96), 'powers of two in [64, 1024]'),
+    (dict(x_amplitude=0.), 'amplitudes > 0'),
+    (dict(mass=0.), 'hbar and mass nonzero'),
+    (dict(dt=float('nan')), 'dt finite'),
+    (dict(damping_f=2), 'damping_f'),
+    (dict(warps=3), 'warps must be'),
+    (dict(precision=5), 'precision must be'),
+])
+def test_batch_descriptors_validated_on_host(bad, msg):
+    """wigb_create refuses an empty batch, grids outside the batched range (powers
+    of two in [64, 1024], ragged n_x != n_p allowed), degenerate constants, an
+    unknown damping function, tile shape or precision with WIG_ERR_ARG and a
+    message, before touching the GPU; the second instance of a batch is checked
+    like the first."""
+    bad = dict(bad)
+    count, warps, precision = bad.pop('count', 2), bad.pop('warps', 0), bad.pop('precision', 0)
+    second = dict(n_x=256, n_p=64)
+    second.update(bad)
+    arr = (_lib.WigbInstance * 2)(_wigb(), _wigb(**second))
+    h = ctypes.c_void_p()
+    rc = _lib.load().wigb_create(ctypes.cast(arr, ctypes.c_void_p), count, warps, precision, ctypes.byref(h))
+    assert rc == 1 and not h.value
+    assert msg in _lib.load().wig_last_error().decode(), _lib.load().wig_last_error()
+
+
+@pytest.mark.parametrize('field,value', [('n_x', 48), ('n_p', 4096), ('precision', 2), ('abi_version', 3),
+                                         ('x_amplitude', -1.), ('gamma', float('inf')), ('f_eps', -1.)])
+def test_adjoint_descriptor_validated_on_host(field, value):
+    d = _lib.WigaDesc()
+    d.abi_version = _lib.ABI_VERSION
+    d.n_x = d.n_p = 128
+    d.precision = _lib.WIGA_PREC_C128
+    d.x_amplitude = d.p_amplitude = 10.
+    d.hbar = d.mass = 1.
+    d.dt = 0.005
+    setattr(d, field, value)
+    h = ctypes.c_void_p()
+    assert _lib.load().wiga_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    assert not h.value
