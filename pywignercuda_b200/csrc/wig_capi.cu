@@ -1543,6 +1543,16 @@ static std::string wigb_source(const std::vector<int>& classes, int warps, int p
   // lane is 128 registers)
   char head[256];
   const int minb = warps == 8 ? 1 : (precision == WIGB_PREC_MIXED ? 8 : 12) / warps;
+  // tuning override (read per compile): WIG_BATCH_WPS=x,p sets the x- and p-pass register
+  // caps by the warps per SM they must allow (e.g. 12,8); 0 keeps the default
+  int xminb = minb, pminb = minb;
+  if (const char* e = getenv("WIG_BATCH_WPS")) {
+    int xw = 0, pw = 0;
+    if (sscanf(e, "%d,%d", &xw, &pw) == 2) {
+      if (xw > 0) xminb = std::max(1, xw / warps);
+      if (pw > 0) pminb = std::max(1, pw / warps);
+    }
+  }
   // tuning override (read per compile): WIG_BATCH_NOINLINE=1 compiles each size class's
   // pass body as its own function
   const char* ni = getenv("WIG_BATCH_NOINLINE");
@@ -1550,7 +1560,7 @@ static std::string wigb_source(const std::vector<int>& classes, int warps, int p
   snprintf(head, sizeof(head),
            "#define WIGB_WARPS %d\n#define WIGB_PREC %d\n#define WIGB_XMINB %d\n#define WIGB_PMINB %d\n"
            "#define WIGB_NOINLINE %d\n#define WIGB_XSTAGE %d\n#define WIGB_BULK 1\n#define WIGB_CASES(F)", warps,
-           precision, minb, minb, noinline, xstage);
+           precision, xminb, pminb, noinline, xstage);
   std::string src = head;
   for (int n : classes) src += " F(" + std::to_string(n) + ")";
   src += "\n";
