@@ -1483,14 +1483,19 @@ struct BVariant {
   int smem_x = 0, smem_p = 0, occ_x = 1, occ_p = 1;
 };
 
-// Whether the x-pass stages its rows in shared memory (WIGB_XSTAGE).  On by
-// default: on the 64-instance mixed-grid batch (B200) it took the x-pass from 272
-// to 240 us in the mixed form and from 182 to 169 us in FP32.  Tuning override
-// (read per compile): WIG_BATCH_XSTAGE=0|1.
+// Whether the x-pass stages its rows in shared memory (WIGB_XSTAGE).  Off by
+// default.  At the register caps below, the staging buffer is what limits the
+// x-pass's resident warps (a 2-warp mixed CTA: 33 KB of exchange + 16 KB of
+// staging, 4 CTAs per SM); without it the x-pass runs 12 (mixed) or 16 (FP32)
+// warps per SM.  On the 64-instance mixed-grid batch (B200, CUDA events): mixed
+// x-pass 253 us staged at 8 warps per SM, 220 us direct at 12; FP32 173 us staged
+// at 12, 164 us direct at 16.  (At the earlier 8 / 12-warp caps staging had been
+// the faster one: 272 -> 240 and 182 -> 169 us.)  Tuning override (read per
+// compile): WIG_BATCH_XSTAGE=0|1.
 int batch_xstage(int) {
   const char* e = getenv("WIG_BATCH_XSTAGE");
   if (e && *e) return atoi(e) ? 1 : 0;
-  return 1;
+  return 0;
 }
 
 // the x-pass's exchange regions and row staging buffer (wigb_xpass: the largest size class's each)
@@ -1537,15 +1542,20 @@ struct wigb_handle {
 };
 
 static std::string wigb_source(const std::vector<int>& classes, int warps, int precision, int xstage) {
-  // register cap: 8-warp tiles run one CTA per SM (255 registers); smaller FP32
-  // tiles three 4-warp / six 2-warp CTAs (168 registers), mixed-precision ones
-  // two 4-warp / four 2-warp CTAs (255: an FP64 sequence of 32 elements per
-  // lane is 128 registers)
+  // Register caps, as the warps per SM each pass must allow (8-warp tiles run one
+  // CTA per SM, 255 registers).  Measured on the 64-instance batch (B200, CUDA events):
+  //   mixed x-pass 12 (168 registers, the same 72 B of spill as at 255): 253 -> 220 us
+  //     against 8 warps per SM;
+  //   mixed p-pass 12 (168 registers, ~1 KB of spill to L1-cached local memory; the
+  //     1024-point FP64 Moyal pair holds 32 double2 per lane): 535 -> 487 us against 8;
+  //   FP32 x-pass 16 (128 registers, no spill): 173 -> 164 us against 12;
+  //   FP32 p-pass 12 (168 registers): 16 measured slower (347 -> 379 us).
   char head[256];
-  const int minb = warps == 8 ? 1 : (precision == WIGB_PREC_MIXED ? 8 : 12) / warps;
+  const bool mixed = precision == WIGB_PREC_MIXED;
+  const int xwps = mixed ? 12 : 16, pwps = 12;
+  int xminb = warps == 8 ? 1 : std::max(1, xwps / warps), pminb = warps == 8 ? 1 : std::max(1, pwps / warps);
   // tuning override (read per compile): WIG_BATCH_WPS=x,p sets the x- and p-pass register
   // caps by the warps per SM they must allow (e.g. 12,8); 0 keeps the default
-  int xminb = minb, pminb = minb;
   if (const char* e = getenv("WIG_BATCH_WPS")) {
     int xw = 0, pw = 0;
     if (sscanf(e, "%d,%d", &xw, &pw) == 2) {

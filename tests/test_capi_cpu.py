@@ -210,10 +210,11 @@ def test_python_classes_fail_loudly_without_gpu():
 @pytest.mark.parametrize('precision,warps', [(0, 4), (1, 2), full_only(0, 8), full_only(0, 2), full_only(1, 8),
                                              full_only(1, 4)])
 def test_batch_jit_spills_bounded(warps, precision):
-    """All size classes in one kernel.  The FP32 passes at 168 registers (3 / 6 CTAs of
-    4 / 2 warps per SM) spill ~20 bytes in the 1024-point p-pass; the mixed form's FP64
-    Moyal pair holds 32 double2 per lane and spills up to ~270 bytes at 255 registers
-    (each size class alone: at most 40)."""
+    """All size classes in one kernel, at the default register caps (warps per SM:
+    FP32 x-pass 16, p-pass 12; mixed 12 and 12; 8-warp tiles one CTA per SM).  The
+    FP32 passes spill at most a few dozen bytes; the mixed p-pass at 168 registers
+    spills ~1.1 KB (its 1024-point FP64 Moyal pair holds 32 double2 per lane), the
+    trade that measured faster than 255 registers at 8 warps per SM."""
     sizes = (ctypes.c_int32 * 5)(64, 128, 256, 512, 1024)
     buf = ctypes.create_string_buffer(1 << 17)
     rc = _lib.load().wigb_jit_check(sizes, 5, warps, precision, buf, len(buf))
@@ -225,7 +226,7 @@ def test_batch_jit_spills_bounded(warps, precision):
         assert at, k
         props = ' '.join(lines[at[0] + 1:at[0] + 3])
         spill = int(props.split(' bytes spill stores')[0].split()[-1])
-        assert spill <= (32 if precision == 0 else 320), (k, props)
+        assert spill <= (32 if precision == 0 else 1536), (k, props)
 
 
 def test_batch_precision_validated():

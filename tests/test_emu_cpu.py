@@ -314,8 +314,8 @@ BSHAPES = ((64, 128, 10., 8.), (128, 64, 8., 10.))
 BEXTRA = {1: dict(ff=1, f_eps=0.5, d_lambda=0.01, v1=0.3, v0=0.2), 4: dict(v1=-0.2)}
 
 
-@pytest.mark.parametrize('warps,grid,prec,xstage', [full_only(4, 3, 0, 0), (2, 5, 0, 1), (4, 3, 1, 1),
-                                                     full_only(2, 5, 1, 0)])
+@pytest.mark.parametrize('warps,grid,prec,xstage', [full_only(4, 3, 0, 0), (2, 5, 0, 1), (4, 3, 1, 0),
+                                                     full_only(2, 5, 1, 1)])
 def test_batch_device_code_matches_oracle(staged, warps, grid, prec, xstage):
     """The real-storage passes (two rows / columns per complex transform, the
     Nyquist split), in FP32 (prec 0) and with the FP64 kinetic and Moyal pairs

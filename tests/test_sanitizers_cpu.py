@@ -21,8 +21,8 @@ from conftest import FULL
 from test_emu_cpu import staged  # noqa: F401  (the module-scoped staging fixture)
 
 CASES = [
-    ('test_batch_device_code_matches_oracle', dict(warps=4, grid=3, prec=0, xstage=0)),
-    ('test_batch_device_code_matches_oracle', dict(warps=2, grid=5, prec=1, xstage=1)),
+    ('test_batch_device_code_matches_oracle', dict(warps=4, grid=3, prec=0, xstage=1)),
+    ('test_batch_device_code_matches_oracle', dict(warps=2, grid=5, prec=1, xstage=0)),
     ('test_adjoint_device_code_matches_twin', dict(prec=0, gamma=0.)),
     ('test_adjoint_device_code_matches_twin', dict(prec=1, gamma=0.1)),
     ('test_wigner2d_device_code_matches_oracle', dict(xrows=32, xnt=256, pc=64, pnt=256, odm=0, kvn=0)),
@@ -32,7 +32,7 @@ CASES = [
     ('test_dirac2d_device_code_matches_oracle', dict(rows=4, rnt=64, cc=8, cnt=64)),
     ('test_dirac3d_cubic_planner_tiles', dict(n=16)),
 ]
-# the default CPU suite: the race checker over the batched (mixed, staged x-pass), adjoint
+# the default CPU suite: the race checker over the batched (mixed, direct x-pass loads), adjoint
 # (damped), complex128 Wigner (ODM) and Dirac2D passes, AddressSanitizer over the Dirac2D
 # passes; every pair with WIG_CPU_FULL=1 (run before a change to the kernels is committed)
 DEFAULT = {('thread', 1), ('thread', 3), ('thread', 5), ('thread', 8), ('address', 8)}
