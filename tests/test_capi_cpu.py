@@ -332,3 +332,26 @@ def test_adjoint_descriptor_validated_on_host(field, value):
     h = ctypes.c_void_p()
     assert _lib.load().wiga_create(ctypes.byref(d), ctypes.byref(h)) == 1
     assert not h.value
+
+
+def _batch_regs(precision, warps=2, sizes=(1024,)):
+    arr = (ctypes.c_int32 * len(sizes))(*sizes)
+    buf = ctypes.create_string_buffer(1 << 17)
+    assert _lib.load().wigb_jit_check(arr, len(sizes), warps, precision, buf, len(buf)) == 0, buf.value
+    lines = buf.value.decode().splitlines()
+    out = {}
+    for k in ('wigb_xpass', 'wigb_ppass'):
+        at = [i for i, l in enumerate(lines) if "Compiling entry function '%s'" % k in l][0]
+        out[k] = int(re.search(r'Used (\d+) registers', ' '.join(lines[at + 1:at + 4])).group(1))
+    return out
+
+
+def test_batch_register_caps_and_override(monkeypatch):
+    """The batched passes' default register caps (FP32 x-pass: 16 warps per SM, so at
+    most 128 registers a thread in a 2-warp tile; p-pass: 12, 168) and the
+    WIG_BATCH_WPS=x,p override, which recompiles them for other warps-per-SM targets."""
+    regs = _batch_regs(0)
+    assert regs['wigb_xpass'] <= 128 and regs['wigb_ppass'] <= 168, regs
+    monkeypatch.setenv('WIG_BATCH_WPS', '8,8')
+    regs = _batch_regs(0)
+    assert regs['wigb_xpass'] > 128 and regs['wigb_ppass'] > 168, regs
