@@ -59,10 +59,9 @@ PASS_BYTES = NX * NP * 16 * 2      # one fused pass reads and writes the c128 gr
 # summarised in profiles/wig_passes_c128_1024.md (one 1024^2 replica, whose state fits in
 # L2: the capture shows one read of it, the write-back comes after the kernel) and
 # profiles/wigb_passes_batch128.md (the mixed p-pass on the 128-instance batch, 46.19 M points,
-# 187.18 MB read + 132.93 MB written; scaled here by points to the 64-instance batch's
-# 23.36 M, since each pass reads and writes every point once)
-NCU_TRAFFIC_PPASS = 16.94e6 + 0.005e6
-NCU_TRAFFIC_BATCH = (187.18e6 + 132.93e6) * 23363584 / 46186496
+# 187.04 MB read + 200.93 MB written: the state once each way plus spilled local memory; scaled
+# here by points to the 64-instance batch's 23.36 M, since each pass reads and writes every point once)
+NCU_TRAFFIC_BATCH = (187.04e6 + 200.93e6) * 23363584 / 46186496
 
 
 def peaks():
@@ -471,12 +470,16 @@ def batch_leg(cases, states, precision, args, world, dev):
     same K steps replayed as one CUDA graph without flushing."""
     import torch
     from pywignercuda_b200.batch import WignerBatch, instance
+    fixed = getattr(args, 'warps', 0)
     batch = WignerBatch([instance(c['n'], x_amplitude=10., dt=DT, gamma=c['gamma'], d_theta=c['d_theta'],
-                                  v4=c['a'], v2=c['b']) for c in cases], precision=precision)
+                                  v4=c['a'], v2=c['b']) for c in cases], precision=precision, warps=fixed)
     stream = torch.cuda.current_stream(dev)
-    scratch = batch.pack(states)
-    warps, tune_ms = batch.autotune(scratch, probe_steps=3)
-    del scratch
+    if fixed:                                     # profiling runs: one tile shape, no autotuning
+        warps, tune_ms = fixed, {}
+    else:
+        scratch = batch.pack(states)
+        warps, tune_ms = batch.autotune(scratch, probe_steps=3)
+        del scratch
     K = args.steps
     W = batch.pack(states)
     batch.run(W, args.warmup)                                           # normalises
@@ -945,6 +948,8 @@ def main():
                     help='batch workload: only the timed section (for profiler launch lists)')
     ap.add_argument('--precision', default='both', choices=['both', 'mixed', 'f32'],
                     help='batch workload: the precisions timed (profiling runs)')
+    ap.add_argument('--warps', type=int, default=0, choices=[0, 2, 4, 8],
+                    help='batch workload: fixed tile shape (warps per CTA) instead of autotuning (profiling runs)')
     ap.add_argument('--instances', type=int, default=0,
                     help='batch workload: instances per rank (default 64; profiling runs)')
     args = ap.parse_args()
