@@ -61,6 +61,7 @@ PASS_BYTES = NX * NP * 16 * 2      # one fused pass reads and writes the c128 gr
 # profiles/wigb_passes_batch128.md (the mixed p-pass on the 128-instance batch, 46.19 M points,
 # 187.04 MB read + 200.93 MB written: the state once each way plus spilled local memory; scaled
 # here by points to the 64-instance batch's 23.36 M, since each pass reads and writes every point once)
+NCU_TRAFFIC_PPASS = 16.94e6 + 0.005e6
 NCU_TRAFFIC_BATCH = (187.04e6 + 200.93e6) * 23363584 / 46186496
 
 
@@ -401,6 +402,66 @@ def make_gp_instance(time_steps):
             GPU_Wigner2D_GPitaevskii.__init__(self, NX, NP, AMP, AMP, 1., 1., D_THETA, 0., GAMMA, POT, DPOT,
                                               '0.5*p*p')
     return MeanField()
+
+
+def run_adjoint(args, world, rank, local):
+    """The differentiable form on the control configuration: 512^2, V = a x^4 - b x^2
+    + eps(t) x (a = 0.05, b = 1), eps piecewise constant over 50 segments of 10 steps
+    (default_rng(1), N(0, 0.1)), coherent state at (-2, 0), loss dxdp sum W_T W_target
+    (target centre from default_rng(2)), 500 steps, a checkpoint every 50.  One
+    gradient = the checkpointed forward sweep + the backward sweep (segment
+    recomputation + adjoint steps) of WignerControl.propagate, giving dL/d(W0, eps, a, b).
+    Timed with CUDA events per gradient, in complex128 and complex64, undamped and
+    with Caldeira-Leggett damping (gamma = 0.1, D_theta = 0.1)."""
+    import torch
+    from pywignercuda_b200.adjoint import WignerControl
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    n, T, K = 512, 500, 50
+    eps0 = torch.tensor(np.random.default_rng(1).normal(0., 0.1, 50), dtype=torch.float64,
+                        device=dev).repeat_interleave(10).contiguous()
+    c = np.random.default_rng(2).uniform(-2., 2., 2)
+    d = 2. * 10. / n
+    target = torch.from_numpy(coherent_state(n, float(c[0]), float(c[1]))).to(dev)
+    reps = max(1, min(args.steps, 5))
+    out = {}
+    stream = torch.cuda.current_stream(dev)
+    for prec in ('c128', 'c64'):
+        for gamma in (0., 0.1):
+            prop = WignerControl(n, x_amplitude=10., dt=DT, v4=0.05, v2=-1., gamma=gamma, d_theta=gamma,
+                                 precision=prec)
+            W0 = torch.from_numpy(coherent_state(n, -2., 0.)).to(dev).to(prop.dtype)
+
+            def gradient():
+                W0r = W0.clone().requires_grad_(True)
+                eps = eps0.clone().requires_grad_(True)
+                coef = torch.tensor([0.05, -1.], dtype=torch.float64, device=dev, requires_grad=True)
+                WT = prop.propagate(W0r, eps, coef, checkpoint=K)
+                L = (WT.real.double() * target).sum() * d * d
+                L.backward()
+                return L
+            for _ in range(max(1, min(args.warmup, 2))):
+                gradient()
+            torch.cuda.synchronize()
+            times = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                gradient()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1))
+            ms = sorted(times)[len(times) // 2]
+            # a gradient advances the grid 2 T steps forward (sweep + recomputation) and T adjoint steps
+            out['%s_%s' % (prec, 'damped' if gamma else 'undamped')] = {
+                'ms_per_gradient': ms, 'grid_pt_steps_per_s': n * n * 3 * T / (ms / 1e3)}
+            del prop
+    if rank == 0:
+        print(json.dumps({'workload': 'adjoint', 'metric': 'gradient of the 500-step 512^2 control problem',
+                          'unit': 'ms per gradient (median of %d)' % reps, 'higher_is_better': False,
+                          'n_gpus': world, 'steps': T, 'checkpoint': K, 'forms': out,
+                          'note': 'grid_pt_steps_per_s counts the forward sweep, its recomputation and the '
+                                  'adjoint sweep (3 T steps of the 512^2 grid)'}))
 
 
 def run_gp(args, world, rank, local):
@@ -943,7 +1004,8 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--replicas', type=int, default=REPLICAS)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
-    ap.add_argument('--workload', default='batch', choices=['batch', 'c128', 'dirac', 'dirac3d', 'gp', 'shardcost'])
+    ap.add_argument('--workload', default='batch', choices=['batch', 'c128', 'dirac', 'dirac3d', 'gp', 'shardcost',
+                                                                'adjoint'])
     ap.add_argument('--profile-only', action='store_true',
                     help='batch workload: only the timed section (for profiler launch lists)')
     ap.add_argument('--precision', default='both', choices=['both', 'mixed', 'f32'],
@@ -970,6 +1032,8 @@ def main():
             run_dirac3d(args, world, rank, local)
         elif args.workload == 'shardcost':
             run_shardcost(args, world, rank, local)
+        elif args.workload == 'adjoint':
+            run_adjoint(args, world, rank, local)
         else:
             run_batch(args, world, rank, local)
     finally:

@@ -48,3 +48,21 @@ def test_notebook_cpu_baseline_sample():
     import bench
     r = bench.cpu_notebook_sample(steps=2, repeats=1, warmup=1)
     assert r['value'] > 0 and r['unit'] == bench.UNIT and r['kind'] == 'port' and r['cores'] >= 1
+
+
+def test_bench_names_are_defined():
+    """Every name bench.py reads is defined, imported, a parameter or a builtin: its GPU
+    legs only run on a GPU, so a missing module-level constant would otherwise surface
+    there first."""
+    import ast
+    import builtins
+    tree = ast.parse(open(os.path.join(ROOT, 'bench.py')).read())
+    defined = {n.id for n in ast.walk(tree) if isinstance(n, ast.Name) and isinstance(n.ctx, ast.Store)}
+    defined |= {n.name for n in ast.walk(tree) if isinstance(n, (ast.FunctionDef, ast.ClassDef))}
+    defined |= {n.arg for n in ast.walk(tree) if isinstance(n, ast.arg)}
+    for n in ast.walk(tree):
+        if isinstance(n, (ast.Import, ast.ImportFrom)):
+            defined |= {(a.asname or a.name).split('.')[0] for a in n.names}
+    used = {n.id for n in ast.walk(tree) if isinstance(n, ast.Name) and isinstance(n.ctx, ast.Load)}
+    missing = sorted(u for u in used - defined if not hasattr(builtins, u) and u != '__file__')
+    assert not missing, missing
