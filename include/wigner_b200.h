@@ -382,6 +382,14 @@ int wiga_forward(wiga_handle* h, void* W_dev, const double* eps_dev, int64_t ste
 int wig_step_adjoint(wiga_handle* h, void* lam_dev, const void* Y_dev, const void* U_dev, const void* s_dev,
                      const double* eps_dev, int64_t step, double* grad_dev, void* stream);
 
+/* The adjoint steps step0 + n_steps - 1 down to step0 in one call (the same
+ * launches as n_steps calls of wig_step_adjoint, with the arguments checked once):
+ * Y_dev and (damped) U_dev are that segment's records from wiga_forward
+ * ([n_steps][n_p][n_x], record k for step step0 + k).  No counterpart in the
+ * reference (it has no gradients).  Asynchronous on `stream`. */
+int wiga_adjoint_sweep(wiga_handle* h, void* lam_dev, const void* Y_dev, const void* U_dev, const void* s_dev,
+                       const double* eps_dev, int64_t step0, int64_t n_steps, double* grad_dev, void* stream);
+
 int wiga_destroy(wiga_handle* h);
 
 /* Compile-only check (no GPU) of the adjoint kernels for the descriptor's grid. */

@@ -157,6 +157,8 @@ SIGNATURES = [
                              c_void_p]),
     ('wig_step_adjoint', c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p,
                                  c_void_p]),
+    ('wiga_adjoint_sweep', c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int64,
+                                   c_void_p, c_void_p]),
     ('wiga_destroy', c_int, [c_void_p]),
     ('wiga_jit_check', c_int, [POINTER(WigaDesc), c_char_p, c_int64]),
     ('wig_observables_noalloc', c_int, [c_void_p, c_int32, c_int32, c_double, c_double, c_double, c_void_p,

@@ -122,6 +122,29 @@ class WignerControl:
                                            eps.data_ptr(), int(step), grad.data_ptr(), st.cuda_stream),
               'wig_step_adjoint')
 
+    def adjoint_sweep(self, lam, Y, eps, step0, grad, U=None, s=None, stream=None):
+        """The adjoint steps step0 + n - 1 down to step0 (n = Y.shape[0]) in one
+        call: lam (dL/dW_{step0+n}) becomes dL/dW_step0 in place and grad[step]
+        receives each step's terms, as n calls of adjoint_step would; Y (and,
+        damped, U and s) are the segment's records from forward_raw."""
+        torch = _torch()
+        n = int(Y.shape[0]) if Y.dim() == 3 else 0
+        self._check_plane(lam, 'lam')
+        self._check_plane(Y, 'Y', lead=n)
+        self._check_eps(eps, step0 + n)
+        if self.damped:
+            if U is None or s is None:
+                raise _lib.WignerArgumentError('a damped adjoint sweep needs U and s')
+            self._check_plane(U, 'U', lead=n)
+            self._check_s(s, step0 + n)
+        if grad.dtype != torch.float64 or not grad.is_cuda or not grad.is_contiguous() or grad.numel() < 3 * (step0 + n):
+            raise _lib.WignerArgumentError('grad must be a contiguous CUDA float64 (steps, 3) tensor')
+        st = stream if stream is not None else torch.cuda.current_stream(lam.device)
+        ptr = lambda T: T.data_ptr() if T is not None else None
+        check(_lib.load().wiga_adjoint_sweep(self._handle, lam.data_ptr(), Y.data_ptr(), ptr(U), ptr(s),
+                                             eps.data_ptr(), int(step0), n, grad.data_ptr(), st.cuda_stream),
+              'wiga_adjoint_sweep')
+
     def propagate(self, W0, eps, coef=None, checkpoint=50):
         """W_T after eps.numel() steps from W0, differentiable in W0, eps and
         (when given) coef = (v4, v2), a float64 tensor whose values replace the
@@ -170,8 +193,7 @@ def _make_fn():
                     U = torch.empty_like(Y) if prop.damped else None
                 W = ctx.ckpts[si].clone()
                 prop.forward_raw(W, eps, s0, n, Y, U, s)
-                for k in reversed(range(n)):
-                    prop.adjoint_step(lam, Y[k], eps, s0 + k, grad, U[k] if U is not None else None, s)
+                prop.adjoint_sweep(lam, Y, eps, s0, grad, U, s)
             ctx.ckpts = None
             g_coef = grad[:, 1:].sum(dim=0).to(ctx.coef_dtype) if ctx.has_coef else None
             gW0 = lam.to(ctx.W0_dtype) if ctx.W0_dtype.is_complex else lam.real.to(ctx.W0_dtype)

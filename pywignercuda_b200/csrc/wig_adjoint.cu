@@ -225,23 +225,11 @@ extern "C" int wiga_forward(wiga_handle* h, void* W_dev, const double* eps_dev, 
   return WIG_OK;
 }
 
-extern "C" int wig_step_adjoint(wiga_handle* h, void* lam_dev, const void* Y_dev, const void* U_dev,
-                                const void* s_dev, const double* eps_dev, int64_t step, double* grad_dev,
-                                void* stream) {
-  if (!h) return fail(WIG_ERR_ARG, "wig_step_adjoint: null handle");
-  if (int rc = check_ptr(lam_dev, "wig_step_adjoint lam")) return rc;
-  if (int rc = check_ptr(Y_dev, "wig_step_adjoint Y")) return rc;
-  if (int rc = check_ptr(eps_dev, "wig_step_adjoint eps")) return rc;
-  if (h->a.damped) {
-    if (int rc = check_ptr(U_dev, "wig_step_adjoint U")) return rc;
-    if (int rc = check_ptr(s_dev, "wig_step_adjoint s")) return rc;
-  }
-  if (!grad_dev || ((uintptr_t)grad_dev & 7) != 0) return fail(WIG_ERR_ARG, "wig_step_adjoint: bad grad pointer");
-  if (step < 0) return fail(WIG_ERR_ARG, "wig_step_adjoint: step must be >= 0");
-  if (int rc = check_device(h, "wig_step_adjoint")) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
-  char* lam = (char*)lam_dev;
-  long long s = (long long)step;
+namespace {
+
+// The launches of adjoint step `step` (arguments checked by the caller).
+int adjoint_step_launch(wiga_handle* h, char* lam, const void* Y_dev, const void* U_dev, const void* s_dev,
+                        const double* eps_dev, long long s, double* grad_dev, cudaStream_t st) {
   if (h->a.damped) {
     long long n = (long long)h->d.n_x * h->d.n_p;
     const char* lc = lam;
@@ -261,4 +249,47 @@ extern "C" int wig_step_adjoint(wiga_handle* h, void* lam_dev, const void* Y_dev
   int use_pend = 0;
   void* xa[] = {&h->a, (void*)&lc, &lam, &sgn, &use_pend};
   return launch(h->fx, h->grid_x, 32, h->smem_x, st, xa);
+}
+
+int check_adjoint_args(wiga_handle* h, void* lam_dev, const void* Y_dev, const void* U_dev, const void* s_dev,
+                       const double* eps_dev, int64_t step, double* grad_dev, const char* what) {
+  if (!h) return fail(WIG_ERR_ARG, "%s: null handle", what);
+  if (int rc = check_ptr(lam_dev, "adjoint lam")) return rc;
+  if (int rc = check_ptr(Y_dev, "adjoint Y")) return rc;
+  if (int rc = check_ptr(eps_dev, "adjoint eps")) return rc;
+  if (h->a.damped) {
+    if (int rc = check_ptr(U_dev, "adjoint U")) return rc;
+    if (int rc = check_ptr(s_dev, "adjoint s")) return rc;
+  }
+  if (!grad_dev || ((uintptr_t)grad_dev & 7) != 0) return fail(WIG_ERR_ARG, "%s: bad grad pointer", what);
+  if (step < 0) return fail(WIG_ERR_ARG, "%s: step must be >= 0", what);
+  return check_device(h, what);
+}
+
+}  // namespace
+
+extern "C" int wig_step_adjoint(wiga_handle* h, void* lam_dev, const void* Y_dev, const void* U_dev,
+                                const void* s_dev, const double* eps_dev, int64_t step, double* grad_dev,
+                                void* stream) {
+  if (int rc = check_adjoint_args(h, lam_dev, Y_dev, U_dev, s_dev, eps_dev, step, grad_dev, "wig_step_adjoint"))
+    return rc;
+  return adjoint_step_launch(h, (char*)lam_dev, Y_dev, U_dev, s_dev, eps_dev, (long long)step, grad_dev,
+                             (cudaStream_t)stream);
+}
+
+extern "C" int wiga_adjoint_sweep(wiga_handle* h, void* lam_dev, const void* Y_dev, const void* U_dev,
+                                  const void* s_dev, const double* eps_dev, int64_t step0, int64_t n_steps,
+                                  double* grad_dev, void* stream) {
+  if (n_steps < 1) return fail(WIG_ERR_ARG, "wiga_adjoint_sweep: n_steps must be >= 1");
+  if (int rc = check_adjoint_args(h, lam_dev, Y_dev, U_dev, s_dev, eps_dev, step0, grad_dev, "wiga_adjoint_sweep"))
+    return rc;
+  const size_t plane = (size_t)h->d.n_x * h->d.n_p * h->esize;
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int64_t k = n_steps - 1; k >= 0; --k) {
+    const char* Yk = (const char*)Y_dev + (size_t)k * plane;
+    const char* Uk = U_dev ? (const char*)U_dev + (size_t)k * plane : nullptr;
+    if (int rc = adjoint_step_launch(h, (char*)lam_dev, Yk, Uk, s_dev, eps_dev, (long long)(step0 + k), grad_dev, st))
+      return rc;
+  }
+  return WIG_OK;
 }

@@ -212,3 +212,29 @@ def test_complex64_control_gradients_against_twin():
     assert abs(L - Lr) < 1e-3 * abs(Lr) + 1e-6, (L, Lr)
     assert _rel(gt, gtr) < 5e-3, _rel(gt, gtr)
     assert _rel(gc, gcr) < 5e-3, (gc, gcr)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('precision,gamma', [('c128', 0.), ('c128', 0.1), ('c64', 0.1)])
+def test_adjoint_sweep_equals_steps(precision, gamma):
+    """wiga_adjoint_sweep (one call per checkpoint segment, as the autograd backward
+    uses it) launches exactly what the step-by-step wig_step_adjoint calls launch:
+    the same dL/dW_0 and gradient rows, bit for bit."""
+    prop, tw, dev = _setup(128, d_theta=0.02, gamma=gamma, precision=precision)
+    n = 12
+    eps = torch.tensor(np.random.default_rng(7).normal(0., 0.2, n), dtype=torch.float64, device=dev)
+    W = coherent(128, 10., -1.0, 0.5, device=dev).to(prop.dtype).contiguous()
+    Y = torch.empty((n, 128, 128), dtype=prop.dtype, device=dev)
+    U = torch.empty_like(Y) if gamma else None
+    s = torch.zeros(n, dtype=torch.complex128, device=dev) if gamma else None
+    prop.forward_raw(W, eps, 0, n, Y, U, s)
+    lam0 = coherent(128, 10., 1.0, -0.5, device=dev).to(prop.dtype).contiguous()
+    lam_a, lam_b = lam0.clone(), lam0.clone()
+    g_a = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    g_b = torch.zeros_like(g_a)
+    for k in reversed(range(n)):
+        prop.adjoint_step(lam_a, Y[k], eps, k, g_a, U[k] if U is not None else None, s)
+    prop.adjoint_sweep(lam_b, Y, eps, 0, g_b, U, s)
+    torch.cuda.synchronize()
+    assert torch.equal(lam_a, lam_b)
+    assert torch.equal(g_a, g_b)
