@@ -1550,7 +1550,7 @@ static std::string wigb_source(const std::vector<int>& classes, int warps, int p
   //     1024-point FP64 Moyal pair holds 32 double2 per lane): 535 -> 487 us against 8;
   //   FP32 x-pass 16 (128 registers, no spill): 173 -> 164 us against 12;
   //   FP32 p-pass 12 (168 registers): 16 measured slower (347 -> 379 us).
-  char head[256];
+  char head[512];
   const bool mixed = precision == WIGB_PREC_MIXED;
   const int xwps = mixed ? 12 : 16, pwps = 12;
   int xminb = warps == 8 ? 1 : std::max(1, xwps / warps), pminb = warps == 8 ? 1 : std::max(1, pwps / warps);
@@ -1567,10 +1567,16 @@ static std::string wigb_source(const std::vector<int>& classes, int warps, int p
   // pass body as its own function
   const char* ni = getenv("WIG_BATCH_NOINLINE");
   const int noinline = ni && atoi(ni) ? 1 : 0;
+  // failure-detection tests (read per compile): WIG_BATCH_TEST_STALL=1 builds the staged x-pass
+  // with its row copies announced but never issued and a wait limit of 4096 polls, so a run
+  // returns WIG_ERR_TIMEOUT quickly and leaves the context usable
+  const char* ts = getenv("WIG_BATCH_TEST_STALL");
+  const bool stall = ts && atoi(ts);
   snprintf(head, sizeof(head),
            "#define WIGB_WARPS %d\n#define WIGB_PREC %d\n#define WIGB_XMINB %d\n#define WIGB_PMINB %d\n"
-           "#define WIGB_NOINLINE %d\n#define WIGB_XSTAGE %d\n#define WIGB_BULK 1\n#define WIGB_CASES(F)", warps,
-           precision, xminb, pminb, noinline, xstage);
+           "#define WIGB_NOINLINE %d\n#define WIGB_XSTAGE %d\n#define WIGB_BULK 1\n%s#define WIGB_CASES(F)", warps,
+           precision, xminb, pminb, noinline, xstage,
+           stall ? "#define WIGB_TEST_STALL 1\n#define WIGB_WAIT_POLLS 4096L\n" : "");
   std::string src = head;
   for (int n : classes) src += " F(" + std::to_string(n) + ")";
   src += "\n";

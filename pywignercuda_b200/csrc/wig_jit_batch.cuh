@@ -58,36 +58,55 @@ __host__ __device__ constexpr int wigb_xstage_max() {
   return m;
 }
 
+// Polls of a staging wait before it gives up.
+#ifndef WIGB_WAIT_POLLS
+#define WIGB_WAIT_POLLS (1L << 24)
+#endif
+
 #ifdef WIGB_BULK
 __device__ __forceinline__ unsigned wigb_smem(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void wigb_stage_init(unsigned long long* bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(wigb_smem(bar)) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
+// WIGB_TEST_STALL (failure-detection tests only): the copy is announced to the
+// mbarrier but never issued, so every wait runs out -- nothing is in flight
+// when the kernel gives up and returns.
 __device__ __forceinline__ void wigb_stage_copy(float* dst, const float* src, unsigned bytes, unsigned long long* bar) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(wigb_smem(bar)), "r"(bytes) : "memory");
+#ifndef WIGB_TEST_STALL
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    wigb_smem(dst)),
                "l"(src), "r"(bytes), "r"(wigb_smem(bar))
                : "memory");
+#endif
 }
-__device__ __forceinline__ void wigb_stage_wait(unsigned long long* bar, unsigned phase, unsigned* status) {
+// Bounded wait for the staged rows: after WIGB_WAIT_POLLS polls it records 1 in
+// the status word (the host reports WIG_ERR_TIMEOUT) and sets the CTA's `stalled`
+// flag, after which this CTA's later waits return at once (the run is already
+// failed; the items are still drawn, so the work list ends in its usual state).
+__device__ __forceinline__ void wigb_stage_wait(unsigned long long* bar, unsigned phase, unsigned* status,
+                                                volatile int* stalled) {
+  if (*stalled) return;
   unsigned done = 0;
 #pragma unroll 1
-  for (long it = 0; it < (1L << 24) && !done; ++it)
+  for (long it = 0; it < WIGB_WAIT_POLLS && !done; ++it)
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
         : "=r"(done)
         : "r"(wigb_smem(bar)), "r"(phase)
         : "memory");
-  if (!done && threadIdx.x == 0) atomicExch(status, 1u);
+  if (!done) {
+    *stalled = 1;
+    if (threadIdx.x == 0) atomicExch(status, 1u);
+  }
 }
 #else
 __device__ __forceinline__ void wigb_stage_init(unsigned long long*) {}
 __device__ __forceinline__ void wigb_stage_copy(float* dst, const float* src, unsigned bytes, unsigned long long*) {
   memcpy(dst, src, bytes);
 }
-__device__ __forceinline__ void wigb_stage_wait(unsigned long long*, unsigned, unsigned*) {}
+__device__ __forceinline__ void wigb_stage_wait(unsigned long long*, unsigned, unsigned*, volatile int*) {}
 #endif
 
 // WIGB_XSTAGE 1: the staged x-pass above; 0: each lane loads its rows from
@@ -109,11 +128,13 @@ wigb_xpass(wig::BArgs A, int n_items) {
   __shared__ wig::BInst sI[2];
   __shared__ int sIn[2], sRow[2];
   __shared__ __align__(8) unsigned long long bar;
+  __shared__ int stalled;
   int item = wig::next_item(&A.tickets[0], n_items);
   int buf = 0;
   unsigned phase = 0;
   // the first item's rows
   if (threadIdx.x == 0) {
+    stalled = 0;
     wigb_stage_init(&bar);
     if (item < n_items) {
       const int2 it = A.xitems[item];
@@ -126,7 +147,7 @@ wigb_xpass(wig::BArgs A, int n_items) {
   }
   __syncthreads();
   while (item < n_items) {
-    wigb_stage_wait(&bar, phase, A.status);
+    wigb_stage_wait(&bar, phase, A.status, &stalled);
     int next = n_items;
     // every lane holds its rows: draw the next item and start its rows' copy
     auto after = [&]() {
