@@ -83,8 +83,9 @@ __device__ __forceinline__ void wigb_stage_copy(float* dst, const float* src, un
 }
 // Bounded wait for the staged rows: after WIGB_WAIT_POLLS polls it records 1 in
 // the status word (the host reports WIG_ERR_TIMEOUT) and sets the CTA's `stalled`
-// flag, after which this CTA's later waits return at once (the run is already
-// failed; the items are still drawn, so the work list ends in its usual state).
+// flag, after which the CTA issues no further copies and its later waits return
+// at once (the run is already failed; the items are still drawn, so the work list
+// ends in its usual state).
 __device__ __forceinline__ void wigb_stage_wait(unsigned long long* bar, unsigned phase, unsigned* status,
                                                 volatile int* stalled) {
   if (*stalled) return;
@@ -128,7 +129,7 @@ wigb_xpass(wig::BArgs A, int n_items) {
   __shared__ wig::BInst sI[2];
   __shared__ int sIn[2], sRow[2];
   __shared__ __align__(8) unsigned long long bar;
-  __shared__ int stalled;
+  __shared__ volatile int stalled;
   int item = wig::next_item(&A.tickets[0], n_items);
   int buf = 0;
   unsigned phase = 0;
@@ -158,8 +159,11 @@ wigb_xpass(wig::BArgs A, int n_items) {
         sI[buf ^ 1] = A.inst[it.x];
         sIn[buf ^ 1] = it.x;
         sRow[buf ^ 1] = it.y;
-        wigb_stage_copy(stage, A.W + sI[buf ^ 1].off + (size_t)it.y * sI[buf ^ 1].n_x,
-                        (unsigned)(wig::bx_stage(sI[buf ^ 1].n_x, WIGB_WARPS) * sizeof(float)), &bar);
+        // after a wait gave up, the barrier's phase never completes: no further arrival
+        // (it would arrive on a phase with no pending arrivals) and no further copy
+        if (!stalled)
+          wigb_stage_copy(stage, A.W + sI[buf ^ 1].off + (size_t)it.y * sI[buf ^ 1].n_x,
+                          (unsigned)(wig::bx_stage(sI[buf ^ 1].n_x, WIGB_WARPS) * sizeof(float)), &bar);
       }
     };
     switch (sI[buf].n_x) {
