@@ -634,6 +634,25 @@ def validation(cases, states, dev):
     return out
 
 
+def merge_validation(val, world):
+    """Every rank validates its own share of the batch: the batch leg's errors are
+    the worst over the ranks (the double-well leg is the same run on every rank).
+    Returns the merged figures on every rank, so that all ranks pick the same
+    headline form."""
+    if world == 1 or val is None:
+        return val
+    import torch.distributed as dist
+    vals = [None] * world
+    dist.all_gather_object(vals, val)
+    out = dict(vals[0])
+    for prec in ('mixed', 'f32'):
+        legs = dict(vals[0][prec])
+        legs['batch_2000'] = {k: (max(v[prec]['batch_2000'][k] for v in vals) if k != 'steps' else
+                                  vals[0][prec]['batch_2000'][k]) for k in vals[0][prec]['batch_2000']}
+        out[prec] = legs
+    return out
+
+
 def run_batch(args, world, rank, local):
     """Headline: the batched form on the 64-instance mixed-grid batch.  With N
     ranks the batch has 64 N instances (the same generator; N = 1 is the
@@ -655,7 +674,7 @@ def run_batch(args, world, rank, local):
     precs = ('mixed', 'f32') if args.precision == 'both' else (args.precision,)
     with ClockSampler(local) as clk:
         legs = {p: batch_leg(cases, states, p, args, world, dev) for p in precs}
-    val = validation(cases, states, dev) if rank == 0 and not args.profile_only else None
+    val = merge_validation(validation(cases, states, dev) if not args.profile_only else None, world)
     head_p = precs[0]
     if val is not None:
         ok = all(v['norm_max_abs'] <= 1e-6 and v['energy_rel_max'] <= 1e-6 and v['energy_rel_final'] <= 1e-6

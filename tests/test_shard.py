@@ -89,3 +89,50 @@ def test_gloo_two_ranks_gather_and_max(tmp_path):
     world = 2
     mp.spawn(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
     assert sorted(os.listdir(tmp_path)) == ['ok0', 'ok1']
+
+
+def _val(rank):
+    leg = lambda e: {'steps': 2000, 'norm_max_abs': 1e-16 * (rank + 1), 'energy_rel_max': e,
+                     'energy_rel_final': 2 * e, 'state_rel_l2_final': 3 * e}
+    dw = {'steps': 4000, 'norm_max_abs': 1e-16, 'energy_rel_max': 4e-9, 'energy_rel_final': 1e-9,
+          'state_rel_l2_final': 1e-7}
+    return {'mixed': {'batch_2000': leg(1e-7 * (rank + 1)), 'double_well_1024_4000': dict(dw)},
+            'f32': {'batch_2000': leg(1e-3 / (rank + 1)), 'double_well_1024_4000': dict(dw)},
+            'reference': 'text'}
+
+
+def _merge_main(rank, world, port, out_dir):
+    import json
+    import torch.distributed as dist
+    import bench
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        merged = bench.merge_validation(_val(rank), world)
+        open(os.path.join(out_dir, 'm%d.json' % rank), 'w').write(json.dumps(merged))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_validation_merged_on_every_rank(tmp_path):
+    """bench.merge_validation: each rank validates its own share of the batch; every
+    rank gets the worst batch figures over the ranks (so all ranks pick the same
+    headline form) and the double-well leg as run."""
+    import json
+    world = 2
+    mp.spawn(_merge_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    m0, m1 = (json.loads(open(os.path.join(tmp_path, 'm%d.json' % r)).read()) for r in range(world))
+    assert m0 == m1
+    assert m0['mixed']['batch_2000']['energy_rel_max'] == pytest.approx(2e-7)
+    assert m0['f32']['batch_2000']['energy_rel_max'] == pytest.approx(1e-3)
+    assert m0['mixed']['batch_2000']['steps'] == 2000
+    assert m0['mixed']['double_well_1024_4000']['energy_rel_max'] == pytest.approx(4e-9)
+    assert m0['reference'] == 'text'
+    assert bench_merge_single() is None
+
+
+def bench_merge_single():
+    import bench
+    assert bench.merge_validation({'a': 1}, 1) == {'a': 1}
+    return bench.merge_validation(None, 2)
