@@ -1572,10 +1572,17 @@ static std::string wigb_source(const std::vector<int>& classes, int warps, int p
   // returns WIG_ERR_TIMEOUT quickly and leaves the context usable
   const char* ts = getenv("WIG_BATCH_TEST_STALL");
   const bool stall = ts && atoi(ts);
+  // tuning override (read per compile): WIG_BATCH_DISS64=n runs the mixed form's dissipator in
+  // FP64 on columns of at most n points (default 256; 0: FP32 dissipator on every size)
+  int diss64 = 256;
+  if (const char* dv = getenv("WIG_BATCH_DISS64")) {
+    if (*dv) diss64 = std::max(0, atoi(dv));
+  }
   snprintf(head, sizeof(head),
            "#define WIGB_WARPS %d\n#define WIGB_PREC %d\n#define WIGB_XMINB %d\n#define WIGB_PMINB %d\n"
-           "#define WIGB_NOINLINE %d\n#define WIGB_XSTAGE %d\n#define WIGB_BULK 1\n%s#define WIGB_CASES(F)", warps,
-           precision, xminb, pminb, noinline, xstage,
+           "#define WIGB_NOINLINE %d\n#define WIGB_XSTAGE %d\n#define WIGB_DISS64_MAXN %d\n#define WIGB_BULK 1\n"
+           "%s#define WIGB_CASES(F)",
+           warps, precision, xminb, pminb, noinline, xstage, diss64,
            stall ? "#define WIGB_TEST_STALL 1\n#define WIGB_WAIT_POLLS 4096L\n" : "");
   std::string src = head;
   for (int n : classes) src += " F(" + std::to_string(n) + ")";
