@@ -355,3 +355,15 @@ def test_batch_register_caps_and_override(monkeypatch):
     monkeypatch.setenv('WIG_BATCH_WPS', '8,8')
     regs = _batch_regs(0)
     assert regs['wigb_xpass'] > 128 and regs['wigb_ppass'] > 168, regs
+
+
+def test_adjoint_sweep_arguments_validated_on_host():
+    """wiga_adjoint_sweep refuses an empty segment and a missing handle before any
+    launch (WIG_ERR_ARG)."""
+    lib = _lib.load()
+    buf = ctypes.create_string_buffer(64)
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    assert lib.wiga_adjoint_sweep(None, p, p, None, None, p, 0, 0, p, None) == 1
+    assert 'n_steps' in lib.wig_last_error().decode()
+    assert lib.wiga_adjoint_sweep(None, p, p, None, None, p, 0, 4, p, None) == 1
+    assert 'null handle' in lib.wig_last_error().decode()
