@@ -15,13 +15,13 @@ import math
 # device time per grid point per step (ns) of the mixed-precision batched form on one B200,
 # by square size class; 'd': damped (Caldeira-Leggett).  Measured with
 #   python bench.py --workload shardcost --steps 20 --warmup 3
-# (SM clock 1965 MHz, no throttle reason).  The cost per point is nearly flat in the size:
+# (SM clock 1965 MHz, default register caps).  The cost per point is nearly flat in the size:
 # the passes are bound by latency and issue, not by the transform's log factor.
 MEASURED_NS = {
-    '128': 0.02164, '128d': 0.02816,
-    '256': 0.02123, '256d': 0.02811,
-    '512': 0.02032, '512d': 0.02585,
-    '1024': 0.02236, '1024d': 0.02855,
+    '128': 0.01832, '128d': 0.02487,
+    '256': 0.01807, '256d': 0.02531,
+    '512': 0.01957, '512d': 0.02508,
+    '1024': 0.02102, '1024d': 0.02808,
 }
 
 
