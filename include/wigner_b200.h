@@ -308,7 +308,11 @@ int wigb_offsets(wigb_handle* h, int64_t* offsets);
 /* Normalise (unless flags & WIG_RUN_CONTINUE) and advance every instance of
  * the packed real FP32 state W (16-byte aligned) by n_prop propagations (t = t_index * dt).
  * obs_host (may be NULL): count x (n_prop + 1) x WIG_NOBS doubles, instance
- * major.  flags & WIG_RUN_GRAPH: the launch sequence is captured into a CUDA
+ * major; with it the call synchronises the stream and returns WIG_ERR_TIMEOUT
+ * (a bounded device-side wait gave up) or WIG_ERR_NONFINITE before returning
+ * numbers.  Without it the call is asynchronous and those checks wait for the
+ * next call that asks for observables (the timeout flag persists until read).
+ * flags & WIG_RUN_GRAPH: the launch sequence is captured into a CUDA
  * graph on first use (per W, t_index0, n_prop, flags, tile shape) and replayed. */
 int wigb_run(wigb_handle* h, void* W_dev, int64_t t_index0, int64_t n_prop, uint32_t flags,
              double* obs_host, void* stream);
