@@ -23,10 +23,10 @@ on the 1024^2 double well, 16 replicas), dirac3d (GPU_Dirac3D 256^3, a 1 GB
 spinor).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload batch|c128|dirac|dirac3d|gp]
+                  [--workload batch|c128|dirac|dirac3d|gp|adjoint|shardcost]
 
-N > 1 (torchrun): the batch has 64 N instances partitioned by cost across the
-ranks (weak scaling; no data-path collective, the observables are gathered to
+N > 1 (torchrun): the batch has 64 N instances (N copies of the configuration's)
+partitioned by cost across the ranks (weak scaling; no data-path collective, the observables are gathered to
 rank 0); the replica workloads run their replicas on every rank; time = max
 over ranks.  --impl reference times the oracle's CPU restatement of the reference
 propagator (complex128, numpy + scipy.fft, all host cores) on a sample of the
@@ -655,8 +655,8 @@ def merge_validation(val, world):
 
 def run_batch(args, world, rank, local):
     """Headline: the batched form on the 64-instance mixed-grid batch.  With N
-    ranks the batch has 64 N instances (the same generator; N = 1 is the
-    configuration itself) partitioned by cost across the ranks (weak scaling);
+    ranks the batch has 64 N instances, N copies of the configuration's (N = 1 is
+    the configuration itself), partitioned by cost across the ranks (weak scaling);
     each rank runs its share, the observables are gathered to rank 0.  Both
     precisions are timed; the headline is the one whose measured norm and energy
     errors at 2000 / 4000 steps are within 1e-6 (the mixed form), the other is
@@ -665,7 +665,10 @@ def run_batch(args, world, rank, local):
     from pywignercuda_b200.shard import gather_observables, partition
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
-    cases_all = batch_config(count=(args.instances or 64) * world)
+    # weak scaling: N copies of the configuration's batch (N = 1 is the configuration itself),
+    # partitioned by cost, so that every rank's work and accuracy profile stay the configuration's
+    base = batch_config(count=args.instances or 64)
+    cases_all = [dict(c) for _ in range(world) for c in base]
     parts = partition([dict(n_x=c['n'], n_p=c['n'], gamma=c['gamma']) for c in cases_all], world)
     cases = [cases_all[i] for i in parts[rank]]
     grand_total = sum(c['n'] * c['n'] for c in cases_all)
