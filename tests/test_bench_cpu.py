@@ -50,19 +50,28 @@ def test_notebook_cpu_baseline_sample():
     assert r['value'] > 0 and r['unit'] == bench.UNIT and r['kind'] == 'port' and r['cores'] >= 1
 
 
-def test_bench_names_are_defined():
-    """Every name bench.py reads is defined, imported, a parameter or a builtin: its GPU
-    legs only run on a GPU, so a missing module-level constant would otherwise surface
-    there first."""
+def _undefined_names(path):
     import ast
     import builtins
-    tree = ast.parse(open(os.path.join(ROOT, 'bench.py')).read())
+    tree = ast.parse(open(path).read())
     defined = {n.id for n in ast.walk(tree) if isinstance(n, ast.Name) and isinstance(n.ctx, ast.Store)}
     defined |= {n.name for n in ast.walk(tree) if isinstance(n, (ast.FunctionDef, ast.ClassDef))}
     defined |= {n.arg for n in ast.walk(tree) if isinstance(n, ast.arg)}
     for n in ast.walk(tree):
         if isinstance(n, (ast.Import, ast.ImportFrom)):
             defined |= {(a.asname or a.name).split('.')[0] for a in n.names}
+        if isinstance(n, ast.ExceptHandler) and n.name:
+            defined.add(n.name)
     used = {n.id for n in ast.walk(tree) if isinstance(n, ast.Name) and isinstance(n.ctx, ast.Load)}
-    missing = sorted(u for u in used - defined if not hasattr(builtins, u) and u != '__file__')
-    assert not missing, missing
+    return sorted(u for u in used - defined if not hasattr(builtins, u) and u != '__file__')
+
+
+def test_bench_and_package_names_are_defined():
+    """Every name bench.py and the package's modules read is defined, imported, a
+    parameter or a builtin: their GPU paths only run on a GPU, so a missing
+    module-level name would otherwise surface there first."""
+    paths = [os.path.join(ROOT, 'bench.py')]
+    pkg = os.path.join(ROOT, 'pywignercuda_b200')
+    paths += [os.path.join(pkg, f) for f in sorted(os.listdir(pkg)) if f.endswith('.py')]
+    for p in paths:
+        assert not _undefined_names(p), (p, _undefined_names(p))
